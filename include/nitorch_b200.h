@@ -1,0 +1,167 @@
+/*
+ * nitorch_b200 -- C ABI of the B200 spline push/pull library.
+ *
+ * Plain pointers, sizes and strides; no framework types.  Every entry point
+ * is asynchronous on the given CUDA stream (`void*` = cudaStream_t, NULL =
+ * legacy default stream), validates its arguments on the host and returns
+ * PP_OK (0) or a negative PP_ERR_* code; pp_last_error() then returns a
+ * message (thread-local).  Device faults are reported by the CUDA runtime
+ * at the next synchronising call, as for any kernel launch.
+ *
+ * Tensors are described by pp_tensor (sizes and strides in ELEMENTS, any
+ * non-negative strides).  Layouts follow nitorch's native backend:
+ *   image / volume : (N, C, X[, Y[, Z]])
+ *   grid           : (N, X[, Y[, Z]], D)  voxel coordinates, grid[..., 0] -> X
+ *   spatial grad   : (N, C, X[, Y[, Z]], D)
+ * The spatial dimensionality D (1, 2 or 3) is taken from the grid.
+ * Grids (and grid gradients) are float32 for float32 / bfloat16 / float16
+ * images and float64 for float64 images; all arithmetic is float32
+ * (float64 for float64 images).
+ *
+ * Ownership: inputs are borrowed read-only; outputs are caller-allocated
+ * and FULLY written by the call (push / count outputs are zero-filled by
+ * the library first, as the reference allocates them with zeros).
+ *
+ * Each entry point replaces the reference function named in its comment
+ * (nitorch/_C/src/pushpull.h:10-57, implemented in pushpull.cpp:76-327;
+ * prefilter: interpol.coeff, vendored as nitorch/_C/_ts/coeff.py:285-344).
+ */
+#ifndef NITORCH_B200_H
+#define NITORCH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PP_API __attribute__((visibility("default")))
+#else
+#define PP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PP_OK               0
+#define PP_ERR_ARG         -1   /* invalid shape / stride / option          */
+#define PP_ERR_DTYPE       -2   /* unsupported or mismatched dtype          */
+#define PP_ERR_CUDA        -3   /* CUDA launch / runtime error              */
+#define PP_ERR_UNSUPPORTED -4   /* valid request the library does not do    */
+#define PP_ERR_WORKSPACE   -5   /* workspace missing or too small           */
+#define PP_ERR_TIMEOUT     -6   /* a bounded device wait gave up            */
+
+/* Element types. */
+#define PP_FLOAT32  0
+#define PP_FLOAT64  1
+#define PP_BFLOAT16 2
+#define PP_FLOAT16  3
+
+/* Bound codes: same values as nitorch's BoundType (nitorch/_C/src/bounds.h). */
+#define PP_BOUND_REPLICATE 0
+#define PP_BOUND_DCT1      1
+#define PP_BOUND_DCT2      2
+#define PP_BOUND_DST1      3
+#define PP_BOUND_DST2      4
+#define PP_BOUND_DFT       5
+#define PP_BOUND_ZERO      7
+
+/* pp_options.flags */
+#define PP_DETERMINISTIC   1   /* push / count: order-independent exact
+                                  accumulation (bit-stable run to run)    */
+
+#define PP_MAX_DIM 8
+
+typedef struct pp_tensor {
+  void*   data;
+  int32_t dtype;                 /* PP_FLOAT32 ...                          */
+  int32_t ndim;
+  int64_t sizes[PP_MAX_DIM];
+  int64_t strides[PP_MAX_DIM];   /* in elements                             */
+} pp_tensor;
+
+typedef struct pp_options {
+  int32_t nbound;                /* 1..3 entries, padded with the last one  */
+  int32_t bound[3];              /* PP_BOUND_* per axis (X, Y, Z)           */
+  int32_t norder;                /* 1..3 entries, padded with the last one  */
+  int32_t order[3];              /* B-spline order 0..7 per axis            */
+  int32_t extrapolate;           /* bit 0: sample outside the field of view;
+                                    bit 1: half-voxel tolerance             */
+  int32_t flags;                 /* PP_DETERMINISTIC                        */
+} pp_options;
+
+/* Version of this ABI (major * 100 + minor). */
+PP_API int pp_abi_version(void);
+
+/* Message of the last error returned on this thread ("" if none). */
+PP_API const char* pp_last_error(void);
+
+/* Number of kernels this library has launched since it was loaded (all
+ * threads and devices); for auditing what ran on the GPU. */
+PP_API unsigned long long pp_kernel_launches(void);
+
+/* Workspace (device bytes, 256-byte aligned) that a push-type call with
+ * output `out` needs: 0 for float32 / float64 outputs without
+ * PP_DETERMINISTIC.  Pass it as `workspace` / `workspace_bytes`. */
+PP_API size_t pp_push_workspace_bytes(const pp_tensor* out, int32_t flags);
+
+/* ni::grid_pull (pushpull.h:10-13): out (N,C,*grid) = input sampled at grid. */
+PP_API int pp_grid_pull(const pp_tensor* input, const pp_tensor* grid,
+                 const pp_tensor* out, const pp_options* opt, void* stream);
+
+/* ni::grid_pull_backward (pushpull.h:15-18).  grad_input (N,C,*in) and/or
+ * grad_grid (N,*grid,D) may be NULL when not requested. */
+PP_API int pp_grid_pull_backward(const pp_tensor* grad, const pp_tensor* input,
+                          const pp_tensor* grid, const pp_tensor* grad_input,
+                          const pp_tensor* grad_grid, const pp_options* opt,
+                          void* stream, void* workspace, size_t workspace_bytes);
+
+/* ni::grid_push (pushpull.h:20-23): out (N,C,*shape) = adjoint of pull. */
+PP_API int pp_grid_push(const pp_tensor* input, const pp_tensor* grid,
+                 const pp_tensor* out, const pp_options* opt, void* stream,
+                 void* workspace, size_t workspace_bytes);
+
+/* ni::grid_push_backward (pushpull.h:25-28). */
+PP_API int pp_grid_push_backward(const pp_tensor* grad, const pp_tensor* input,
+                          const pp_tensor* grid, const pp_tensor* grad_input,
+                          const pp_tensor* grad_grid, const pp_options* opt,
+                          void* stream);
+
+/* ni::grid_count (pushpull.h:30-33): out (N,1,*shape), grid dtype. */
+PP_API int pp_grid_count(const pp_tensor* grid, const pp_tensor* out,
+                  const pp_options* opt, void* stream, void* workspace,
+                  size_t workspace_bytes);
+
+/* ni::grid_count_backward (pushpull.h:35-38): grad (N,1,*shape). */
+PP_API int pp_grid_count_backward(const pp_tensor* grad, const pp_tensor* grid,
+                           const pp_tensor* grad_grid, const pp_options* opt,
+                           void* stream);
+
+/* ni::grid_grad (pushpull.h:40-43): out (N,C,*grid,D). */
+PP_API int pp_grid_grad(const pp_tensor* input, const pp_tensor* grid,
+                 const pp_tensor* out, const pp_options* opt, void* stream);
+
+/* ni::grid_grad_backward (pushpull.h:45-48): grad (N,C,*grid,D). */
+PP_API int pp_grid_grad_backward(const pp_tensor* grad, const pp_tensor* input,
+                          const pp_tensor* grid, const pp_tensor* grad_input,
+                          const pp_tensor* grad_grid, const pp_options* opt,
+                          void* stream, void* workspace, size_t workspace_bytes);
+
+/* interpol.coeff.spline_coeff (vendored: _ts/coeff.py:285-310):
+ * interpolating B-spline coefficients along one axis of `input`, written to
+ * `out` (same sizes; may alias `input` for in-place).  `bound` uses the
+ * prefilter's integer codes (_ts/bounds.py:7-14): 0 zero, 1 replicate,
+ * 2 dct1, 3 dct2, 6 dft; other codes return PP_ERR_UNSUPPORTED, as the
+ * reference raises NotImplementedError. */
+PP_API int pp_spline_coeff(const pp_tensor* input, const pp_tensor* out,
+                    int32_t bound, int32_t order, int32_t axis, void* stream);
+
+/* interpol.coeff.spline_coeff_nd (_ts/coeff.py:314-344): the last `dim`
+ * axes, per-axis bound / order lists padded with their last entry. */
+PP_API int pp_spline_coeff_nd(const pp_tensor* input, const pp_tensor* out,
+                       int32_t nbound, const int32_t* bound, int32_t norder,
+                       const int32_t* order, int32_t dim, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NITORCH_B200_H */

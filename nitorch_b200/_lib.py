@@ -1,0 +1,157 @@
+"""ctypes binding of the C ABI in ``include/nitorch_b200.h``.
+
+The shared library ``nitorch_b200/_C/libnitorch_b200.so`` is built in-tree
+(``python -m nitorch_b200.build`` or ``make -C nitorch_b200/csrc``).  There
+is no CPU fallback: if the library is missing or no CUDA device is
+available, the first call raises.
+"""
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_C", "libnitorch_b200.so")
+
+PP_OK = 0
+PP_ERR_ARG = -1
+PP_ERR_DTYPE = -2
+PP_ERR_CUDA = -3
+PP_ERR_UNSUPPORTED = -4
+PP_ERR_WORKSPACE = -5
+PP_ERR_TIMEOUT = -6
+
+PP_FLOAT32, PP_FLOAT64, PP_BFLOAT16, PP_FLOAT16 = 0, 1, 2, 3
+PP_DETERMINISTIC = 1
+PP_MAX_DIM = 8
+
+_DTYPES = {
+    torch.float32: PP_FLOAT32,
+    torch.float64: PP_FLOAT64,
+    torch.bfloat16: PP_BFLOAT16,
+    torch.float16: PP_FLOAT16,
+}
+
+
+class PPTensor(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("dtype", ctypes.c_int32),
+        ("ndim", ctypes.c_int32),
+        ("sizes", ctypes.c_int64 * PP_MAX_DIM),
+        ("strides", ctypes.c_int64 * PP_MAX_DIM),
+    ]
+
+
+class PPOptions(ctypes.Structure):
+    _fields_ = [
+        ("nbound", ctypes.c_int32),
+        ("bound", ctypes.c_int32 * 3),
+        ("norder", ctypes.c_int32),
+        ("order", ctypes.c_int32 * 3),
+        ("extrapolate", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+    ]
+
+
+EXPORTS = (
+    "pp_abi_version", "pp_last_error", "pp_kernel_launches", "pp_push_workspace_bytes",
+    "pp_grid_pull", "pp_grid_pull_backward", "pp_grid_push",
+    "pp_grid_push_backward", "pp_grid_count", "pp_grid_count_backward",
+    "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
+    "pp_spline_coeff_nd",
+)
+
+_lib = None
+
+
+def _declare(L):
+    T = ctypes.POINTER(PPTensor)
+    O = ctypes.POINTER(PPOptions)
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    L.pp_abi_version.restype = ctypes.c_int
+    L.pp_last_error.restype = ctypes.c_char_p
+    L.pp_kernel_launches.restype = ctypes.c_ulonglong
+    L.pp_push_workspace_bytes.argtypes = [T, ctypes.c_int32]
+    L.pp_push_workspace_bytes.restype = sz
+    L.pp_grid_pull.argtypes = [T, T, T, O, vp]
+    L.pp_grid_pull_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
+    L.pp_grid_push.argtypes = [T, T, T, O, vp, vp, sz]
+    L.pp_grid_push_backward.argtypes = [T, T, T, T, T, O, vp]
+    L.pp_grid_count.argtypes = [T, T, O, vp, vp, sz]
+    L.pp_grid_count_backward.argtypes = [T, T, T, O, vp]
+    L.pp_grid_grad.argtypes = [T, T, T, O, vp]
+    L.pp_grid_grad_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
+    L.pp_spline_coeff.argtypes = [T, T, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp]
+    L.pp_spline_coeff_nd.argtypes = [T, T, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                     ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                     ctypes.c_int32, vp]
+    for name in EXPORTS:
+        if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches"):
+            getattr(L, name).restype = ctypes.c_int
+    return L
+
+
+def load():
+    """Load (once) and return the C library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"nitorch_b200: CUDA library not built ({LIB_PATH} missing); "
+                "run `python -m nitorch_b200.build`")
+        _lib = _declare(ctypes.CDLL(LIB_PATH))
+    return _lib
+
+
+def kernel_launches():
+    """Kernels launched by the library so far (process-wide counter)."""
+    return int(load().pp_kernel_launches())
+
+
+def check(rc):
+    if rc != PP_OK:
+        msg = load().pp_last_error().decode(errors="replace")
+        if rc == PP_ERR_UNSUPPORTED and "not implemented" in msg:
+            raise NotImplementedError(msg)
+        raise RuntimeError(msg)
+
+
+def desc(t):
+    """pp_tensor view of a torch tensor (borrowed: keep `t` alive)."""
+    if t is None:
+        return None
+    d = PPTensor()
+    d.data = t.data_ptr() if t.numel() else None
+    try:
+        d.dtype = _DTYPES[t.dtype]
+    except KeyError:
+        raise RuntimeError(f"(): unsupported dtype {t.dtype}") from None
+    nd = t.dim()
+    if nd > PP_MAX_DIM:
+        raise RuntimeError(f"(): too many dimensions ({nd})")
+    d.ndim = nd
+    d.sizes[:nd] = t.shape
+    d.strides[:nd] = t.stride()
+    return d
+
+
+def ref(d):
+    return None if d is None else ctypes.byref(d)
+
+
+def options(bound, order, extrapolate, flags=0):
+    o = PPOptions()
+    b = [int(x) for x in bound][:3]
+    i = [int(x) for x in order][:3]
+    o.nbound = len(b)
+    o.bound[:len(b)] = b
+    o.norder = len(i)
+    o.order[:len(i)] = i
+    o.extrapolate = int(extrapolate)
+    o.flags = int(flags)
+    return o
+
+
+def stream_of(t):
+    return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)

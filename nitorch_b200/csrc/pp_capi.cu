@@ -1,0 +1,547 @@
+// C ABI of the push/pull library: argument validation (the checks of
+// nitorch/_C/src/pushpull.cpp:19-72), output preparation (the zero-filled
+// allocations of pushpull_common.cpp:476-571), mode wiring (pushpull.cpp
+// flag table) and dispatch to the kernel family of pp_kernels.cuh.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/nitorch_b200.h"
+#include "pp_capi_internal.cuh"
+#include "pp_kernels.cuh"
+
+// Launchers compiled from pp_inst.cu, one per (dtype, dim, mode).
+cudaError_t pp_launch_f32_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f32_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f64_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_bf16_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
+cudaError_t pp_launch_f16_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+
+static const pp_launcher_t kLaunchers[4][3][7] = {
+  {
+    {pp_launch_f32_d1_m0, pp_launch_f32_d1_m1, pp_launch_f32_d1_m2, pp_launch_f32_d1_m3, pp_launch_f32_d1_m4, pp_launch_f32_d1_m5, pp_launch_f32_d1_m6},
+    {pp_launch_f32_d2_m0, pp_launch_f32_d2_m1, pp_launch_f32_d2_m2, pp_launch_f32_d2_m3, pp_launch_f32_d2_m4, pp_launch_f32_d2_m5, pp_launch_f32_d2_m6},
+    {pp_launch_f32_d3_m0, pp_launch_f32_d3_m1, pp_launch_f32_d3_m2, pp_launch_f32_d3_m3, pp_launch_f32_d3_m4, pp_launch_f32_d3_m5, pp_launch_f32_d3_m6},
+  },
+  {
+    {pp_launch_f64_d1_m0, pp_launch_f64_d1_m1, pp_launch_f64_d1_m2, pp_launch_f64_d1_m3, pp_launch_f64_d1_m4, pp_launch_f64_d1_m5, pp_launch_f64_d1_m6},
+    {pp_launch_f64_d2_m0, pp_launch_f64_d2_m1, pp_launch_f64_d2_m2, pp_launch_f64_d2_m3, pp_launch_f64_d2_m4, pp_launch_f64_d2_m5, pp_launch_f64_d2_m6},
+    {pp_launch_f64_d3_m0, pp_launch_f64_d3_m1, pp_launch_f64_d3_m2, pp_launch_f64_d3_m3, pp_launch_f64_d3_m4, pp_launch_f64_d3_m5, pp_launch_f64_d3_m6},
+  },
+  {
+    {pp_launch_bf16_d1_m0, pp_launch_bf16_d1_m1, pp_launch_bf16_d1_m2, pp_launch_bf16_d1_m3, pp_launch_bf16_d1_m4, pp_launch_bf16_d1_m5, pp_launch_bf16_d1_m6},
+    {pp_launch_bf16_d2_m0, pp_launch_bf16_d2_m1, pp_launch_bf16_d2_m2, pp_launch_bf16_d2_m3, pp_launch_bf16_d2_m4, pp_launch_bf16_d2_m5, pp_launch_bf16_d2_m6},
+    {pp_launch_bf16_d3_m0, pp_launch_bf16_d3_m1, pp_launch_bf16_d3_m2, pp_launch_bf16_d3_m3, pp_launch_bf16_d3_m4, pp_launch_bf16_d3_m5, pp_launch_bf16_d3_m6},
+  },
+  {
+    {pp_launch_f16_d1_m0, pp_launch_f16_d1_m1, pp_launch_f16_d1_m2, pp_launch_f16_d1_m3, pp_launch_f16_d1_m4, pp_launch_f16_d1_m5, pp_launch_f16_d1_m6},
+    {pp_launch_f16_d2_m0, pp_launch_f16_d2_m1, pp_launch_f16_d2_m2, pp_launch_f16_d2_m3, pp_launch_f16_d2_m4, pp_launch_f16_d2_m5, pp_launch_f16_d2_m6},
+    {pp_launch_f16_d3_m0, pp_launch_f16_d3_m1, pp_launch_f16_d3_m2, pp_launch_f16_d3_m3, pp_launch_f16_d3_m4, pp_launch_f16_d3_m5, pp_launch_f16_d3_m6},
+  },
+};
+
+namespace ppc {
+
+thread_local std::string g_err;
+std::atomic<unsigned long long> g_launches{0};
+
+// --- options ----------------------------------------------------------------
+int read_options(const pp_options* o, int D, int bound[3], int order[3]) {
+  if (!o) return fail(PP_ERR_ARG, "(): expected options not be undefined");
+  if (o->nbound < 1 || o->nbound > 3) return fail(PP_ERR_ARG, "(): expected non empty parameter bound_mode");
+  if (o->norder < 1 || o->norder > 3) return fail(PP_ERR_ARG, "(): expected non empty parameter interpolation_mode");
+  for (int a = 0; a < 3; ++a) {
+    bound[a] = o->bound[a < o->nbound ? a : o->nbound - 1];
+    order[a] = o->order[a < o->norder ? a : o->norder - 1];
+  }
+  for (int a = 0; a < D; ++a) {
+    const int b = bound[a];
+    if (!(b >= 0 && b <= 5) && b != PP_BOUND_ZERO)
+      return fail(PP_ERR_ARG, "(): unsupported bound code %d", b);
+    if (order[a] < 0 || order[a] > 7)
+      return fail(PP_ERR_ARG, "(): unsupported interpolation order %d", order[a]);
+  }
+  return PP_OK;
+}
+
+int iso_order(int D, const int order[3]) {
+  for (int a = 1; a < D; ++a)
+    if (order[a] != order[0]) return -1;
+  return order[0];
+}
+
+// --- tensor -> kernel argument helpers ----------------------------------------
+void set_image(const pp_tensor* t, int D, int64_t& sN, int64_t& sC, int64_t s[3]) {
+  sN = t->strides[0];
+  sC = t->strides[1];
+  for (int a = 0; a < 3; ++a) s[a] = a < D ? t->strides[2 + a] : 0;
+}
+
+void set_grid(const pp_tensor* t, int D, int64_t& sN, int64_t s[3], int64_t& sD) {
+  sN = t->strides[0];
+  for (int a = 0; a < 3; ++a) s[a] = a < D ? t->strides[1 + a] : 0;
+  sD = t->strides[1 + D];
+}
+
+bool fits32(int64_t v) { return v < (int64_t(1) << 31) - 1; }
+
+cudaError_t launch(int dtype, int D, int mode, int ord, bool wide, const ppk::PPArgs& a, cudaStream_t st) {
+  if (dtype < 0 || dtype > 3 || D < 1 || D > 3 || mode < 0 || mode >= ppk::K_NMODES) return cudaErrorInvalidValue;
+  count_launch();
+  return kLaunchers[dtype][D - 1][mode](ord, wide, a, st);
+}
+
+int grid_dtype_for(int image_dtype) { return image_dtype == PP_FLOAT64 ? PP_FLOAT64 : PP_FLOAT32; }
+
+// Common checks of grid (pushpull.cpp:19-72): 3-5 dims, last dim = ndim-2,
+// non-empty spatial dims.
+int check_grid(const pp_tensor* grid, int& D) {
+  int rc = check_tensor(grid, "grid");
+  if (rc) return rc;
+  if (grid->ndim < 3 || grid->ndim > 5)
+    return fail(PP_ERR_ARG, "(): expected 3D, 4D or 5D grid but got input with %d dimensions", grid->ndim);
+  D = grid->ndim - 2;
+  if (grid->sizes[grid->ndim - 1] != D)
+    return fail(PP_ERR_ARG, "(): expected grid to have size %d in last dimension, but got %lld", D,
+                (long long)grid->sizes[grid->ndim - 1]);
+  for (int i = 1; i < grid->ndim - 1; ++i)
+    if (grid->sizes[i] <= 0)
+      return fail(PP_ERR_ARG, "(): expected grid to have non-empty spatial dimensions, but dimension %d is empty", i);
+  if (grid->dtype != PP_FLOAT32 && grid->dtype != PP_FLOAT64)
+    return fail(PP_ERR_DTYPE, "(): expected grid to be float32 or float64");
+  return PP_OK;
+}
+
+int check_image(const pp_tensor* t, const char* name, int D, int grid_dtype) {
+  int rc = check_tensor(t, name);
+  if (rc) return rc;
+  if (t->ndim != D + 2)
+    return fail(PP_ERR_ARG, "(): expected %s to have %d dimensions, but it has %d", name, D + 2, t->ndim);
+  for (int i = 2; i < t->ndim; ++i)
+    if (t->sizes[i] <= 0)
+      return fail(PP_ERR_ARG, "(): expected %s to have non-empty spatial dimensions, but dimension %d is empty", name, i);
+  if (grid_dtype_for(t->dtype) != grid_dtype)
+    return fail(PP_ERR_DTYPE, "(): expected %s and grid to have the same dtype (or a 16-bit %s with a float32 grid)", name, name);
+  return PP_OK;
+}
+
+int check_same_sizes(const pp_tensor* t, const int64_t* sizes, int nd, const char* name) {
+  if (t->ndim != nd) return fail(PP_ERR_ARG, "(): %s has %d dimensions, expected %d", name, t->ndim, nd);
+  for (int i = 0; i < nd; ++i)
+    if (t->sizes[i] != sizes[i])
+      return fail(PP_ERR_ARG, "(): %s has size %lld in dimension %d, expected %lld", name,
+                  (long long)t->sizes[i], i, (long long)sizes[i]);
+  return PP_OK;
+}
+
+}  // namespace ppc
+
+using namespace ppc;
+
+namespace {
+
+// Core dispatcher shared by the entry points.
+struct Call {
+  int D = 0;
+  int bound[3] = {0, 0, 0}, order[3] = {1, 1, 1};
+  int dtype = PP_FLOAT32;  // image storage dtype
+  ppk::PPArgs a;
+  Call() { std::memset(&a, 0, sizeof(a)); }
+};
+
+int prepare(Call& k, const pp_tensor* grid, const pp_options* opt) {
+  int rc = check_grid(grid, k.D);
+  if (rc) return rc;
+  rc = read_options(opt, k.D, k.bound, k.order);
+  if (rc) return rc;
+  for (int a = 0; a < 3; ++a) { k.a.bound[a] = k.bound[a]; k.a.order[a] = k.order[a]; }
+  k.a.extrapolate = opt->extrapolate;
+  k.a.grid = grid->data;
+  set_grid(grid, k.D, k.a.grid_sN, k.a.grid_s, k.a.grid_sD);
+  k.a.N = grid->sizes[0];
+  int64_t nv = grid->sizes[0];
+  for (int a = 0; a < 3; ++a) {
+    k.a.trgt_size[a] = a < k.D ? grid->sizes[1 + a] : 1;
+    nv *= k.a.trgt_size[a];
+  }
+  k.a.nvox = nv;
+  return PP_OK;
+}
+
+bool need_wide(const Call& k, std::initializer_list<const pp_tensor*> spatial) {
+  if (!fits32(k.a.nvox)) return true;
+  for (const pp_tensor* t : spatial)
+    if (t && !fits32(max_offset(t, 2))) return true;
+  return false;
+}
+
+int run(Call& k, int mode, bool wide, cudaStream_t st) {
+  const int ord = iso_order(k.D, k.order);
+  if (k.a.nvox == 0) return PP_OK;
+  return cuda_check(launch(k.dtype, k.D, mode, ord, wide, k.a, st), "push/pull kernel launch");
+}
+
+// 16-bit outputs of scatter modes accumulate into a float workspace.
+size_t scatter_ws_bytes(const pp_tensor* out, int flags) {
+  if (!out) return 0;
+  size_t b = 0;
+  const int64_t n = numel(out);
+  if (out->dtype == PP_BFLOAT16 || out->dtype == PP_FLOAT16) b += ((n * 4 + 255) / 256) * 256;
+  (void)flags;
+  return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pp_abi_version(void) { return 100; }
+
+const char* pp_last_error(void) { return g_err.c_str(); }
+
+unsigned long long pp_kernel_launches(void) { return g_launches.load(); }
+
+size_t pp_push_workspace_bytes(const pp_tensor* out, int32_t flags) {
+  return scatter_ws_bytes(out, flags);
+}
+
+int pp_grid_pull(const pp_tensor* input, const pp_tensor* grid, const pp_tensor* out,
+                 const pp_options* opt, void* stream) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if (input->sizes[0] != grid->sizes[0])
+    return fail(PP_ERR_ARG, "(): expected input and grid to have the same batch size");
+  if ((rc = check_tensor(out, "output"))) return rc;
+  int64_t osz[5] = {grid->sizes[0], input->sizes[1], 1, 1, 1};
+  for (int a = 0; a < k.D; ++a) osz[2 + a] = grid->sizes[1 + a];
+  if ((rc = check_same_sizes(out, osz, k.D + 2, "output"))) return rc;
+  if (out->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match input");
+  k.dtype = input->dtype;
+  k.a.src = input->data;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.out = out->data;
+  set_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  return run(k, ppk::K_PULL, need_wide(k, {input, out}), static_cast<cudaStream_t>(stream));
+}
+
+int pp_grid_grad(const pp_tensor* input, const pp_tensor* grid, const pp_tensor* out,
+                 const pp_options* opt, void* stream) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if (input->sizes[0] != grid->sizes[0])
+    return fail(PP_ERR_ARG, "(): expected input and grid to have the same batch size");
+  if ((rc = check_tensor(out, "output"))) return rc;
+  int64_t osz[6] = {grid->sizes[0], input->sizes[1], 1, 1, 1, 1};
+  for (int a = 0; a < k.D; ++a) osz[2 + a] = grid->sizes[1 + a];
+  osz[2 + k.D] = k.D;
+  if ((rc = check_same_sizes(out, osz, k.D + 3, "output"))) return rc;
+  if (out->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match input");
+  k.dtype = input->dtype;
+  k.a.src = input->data;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.out = out->data;
+  set_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  k.a.out_sK = out->strides[2 + k.D];
+  return run(k, ppk::K_SGRAD, need_wide(k, {input, out}), static_cast<cudaStream_t>(stream));
+}
+
+// Scatter helper: push `trgt` (N,C,*grid[,K]) into `out` (N,C,*shape) with
+// `mode`, optionally fused with a grid gradient of `src`.
+static int scatter_into(Call& k, int mode, const pp_tensor* out, bool wide,
+                        void* ws, size_t ws_bytes, cudaStream_t st) {
+  int rc;
+  const bool half = out->dtype == PP_BFLOAT16 || out->dtype == PP_FLOAT16;
+  float* acc = nullptr;
+  if (half) {
+    const size_t need = scatter_ws_bytes(out, 0);
+    if (!ws || ws_bytes < need)
+      return fail(PP_ERR_WORKSPACE, "(): 16-bit push output needs %zu bytes of workspace", need);
+    acc = static_cast<float*>(ws);
+    if ((rc = cuda_check(cudaMemsetAsync(acc, 0, numel(out) * 4, st), "workspace clear"))) return rc;
+    // dense (contiguous) float accumulator with the output's sizes
+    k.a.out = acc;
+    int64_t s = 1;
+    int64_t cs[PP_MAX_DIM];
+    for (int i = out->ndim - 1; i >= 0; --i) { cs[i] = s; s *= out->sizes[i]; }
+    k.a.out_sN = cs[0];
+    k.a.out_sC = cs[1];
+    for (int a = 0; a < 3; ++a) k.a.out_s[a] = a < k.D ? cs[2 + a] : 0;
+  } else {
+    if ((rc = zero_fill(out, st))) return rc;
+    k.a.out = out->data;
+    set_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  }
+  if ((rc = run(k, mode, wide, st))) return rc;
+  if (half) return store_f32(acc, out, st);
+  return PP_OK;
+}
+
+int pp_grid_push(const pp_tensor* input, const pp_tensor* grid, const pp_tensor* out,
+                 const pp_options* opt, void* stream, void* workspace, size_t workspace_bytes) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  // pushpull.cpp:131-150: input spatial size must match the grid's
+  for (int a = 0; a < k.D; ++a)
+    if (input->sizes[2 + a] != grid->sizes[1 + a] || input->sizes[0] != grid->sizes[0])
+      return fail(PP_ERR_ARG, "(): expected input and grid to have same batch, width, height and (optionally) depth sizes");
+  if ((rc = check_tensor(out, "output"))) return rc;
+  if (out->ndim != k.D + 2 || out->sizes[0] != grid->sizes[0] || out->sizes[1] != input->sizes[1])
+    return fail(PP_ERR_ARG, "(): output must be (N, C, *shape)");
+  for (int i = 2; i < out->ndim; ++i)
+    if (out->sizes[i] <= 0) return fail(PP_ERR_ARG, "(): expected non-empty output shape");
+  if (out->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match input");
+  k.dtype = input->dtype;
+  k.a.trgt = input->data;
+  k.a.C = input->sizes[1];
+  set_image(input, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? out->sizes[2 + a] : 1;
+  return scatter_into(k, ppk::K_PUSH, out, need_wide(k, {input, out}), workspace, workspace_bytes,
+                      static_cast<cudaStream_t>(stream));
+}
+
+int pp_grid_count(const pp_tensor* grid, const pp_tensor* out, const pp_options* opt, void* stream,
+                  void* workspace, size_t workspace_bytes) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_tensor(out, "output"))) return rc;
+  if (out->ndim != k.D + 2 || out->sizes[0] != grid->sizes[0] || out->sizes[1] != 1)
+    return fail(PP_ERR_ARG, "(): output must be (N, 1, *shape)");
+  for (int i = 2; i < out->ndim; ++i)
+    if (out->sizes[i] <= 0) return fail(PP_ERR_ARG, "(): expected non-empty output shape");
+  if (out->dtype != grid->dtype) return fail(PP_ERR_DTYPE, "(): count output must have the grid dtype");
+  k.dtype = grid->dtype;
+  k.a.C = 1;
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? out->sizes[2 + a] : 1;
+  return scatter_into(k, ppk::K_COUNT, out, need_wide(k, {out}), workspace, workspace_bytes,
+                      static_cast<cudaStream_t>(stream));
+}
+
+static int check_ggrad(const pp_tensor* gg, const pp_tensor* grid) {
+  int rc = check_tensor(gg, "grad_grid");
+  if (rc) return rc;
+  if ((rc = check_same_sizes(gg, grid->sizes, grid->ndim, "grad_grid"))) return rc;
+  if (gg->dtype != grid->dtype) return fail(PP_ERR_DTYPE, "(): grad_grid must have the grid dtype");
+  return PP_OK;
+}
+
+int pp_grid_pull_backward(const pp_tensor* grad, const pp_tensor* input, const pp_tensor* grid,
+                          const pp_tensor* grad_input, const pp_tensor* grad_grid,
+                          const pp_options* opt, void* stream, void* workspace, size_t workspace_bytes) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if ((rc = check_tensor(grad, "grad"))) return rc;
+  int64_t gsz[5] = {grid->sizes[0], input->sizes[1], 1, 1, 1};
+  for (int a = 0; a < k.D; ++a) gsz[2 + a] = grid->sizes[1 + a];
+  if ((rc = check_same_sizes(grad, gsz, k.D + 2, "grad"))) return rc;
+  if (grad->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad dtype must match input");
+  if (grad_input && (rc = check_same_sizes(grad_input, input->sizes, input->ndim, "grad_input"))) return rc;
+  if (grad_input && grad_input->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad_input dtype must match input");
+  if (grad_grid && (rc = check_ggrad(grad_grid, grid))) return rc;
+  if (!grad_input && !grad_grid) return PP_OK;
+  k.dtype = input->dtype;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  k.a.src = input->data;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.trgt = grad->data;
+  set_image(grad, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  const bool wide = need_wide(k, {input, grad, grad_input});
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (grad_grid) {
+    k.a.gg = grad_grid->data;
+    set_grid(grad_grid, k.D, k.a.gg_sN, k.a.gg_s, k.a.gg_sD);
+    k.a.flags = ppk::F_GRAD | (grad_input ? ppk::F_A : 0);
+    if (!grad_input) return run(k, ppk::K_PUSHGRAD, wide, st);
+    return scatter_into(k, ppk::K_PUSHGRAD, grad_input, wide, workspace, workspace_bytes, st);
+  }
+  return scatter_into(k, ppk::K_PUSH, grad_input, wide, workspace, workspace_bytes, st);
+}
+
+int pp_grid_push_backward(const pp_tensor* grad, const pp_tensor* input, const pp_tensor* grid,
+                          const pp_tensor* grad_input, const pp_tensor* grad_grid,
+                          const pp_options* opt, void* stream) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if ((rc = check_image(grad, "grad", k.D, grid->dtype))) return rc;
+  if (grad->sizes[0] != grid->sizes[0] || grad->sizes[1] != input->sizes[1])
+    return fail(PP_ERR_ARG, "(): grad must be (N, C, *shape)");
+  if (grad->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad dtype must match input");
+  if (grad_input && (rc = check_same_sizes(grad_input, input->sizes, input->ndim, "grad_input"))) return rc;
+  if (grad_input && grad_input->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad_input dtype must match input");
+  if (grad_grid && (rc = check_ggrad(grad_grid, grid))) return rc;
+  if (!grad_input && !grad_grid) return PP_OK;
+  k.dtype = input->dtype;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? grad->sizes[2 + a] : 1;
+  k.a.src = grad->data;
+  set_image(grad, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.trgt = input->data;
+  set_image(input, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (grad_input) {
+    k.a.out = grad_input->data;
+    set_image(grad_input, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  }
+  const bool wide = need_wide(k, {grad, input, grad_input});
+  if (grad_grid) {
+    k.a.gg = grad_grid->data;
+    set_grid(grad_grid, k.D, k.a.gg_sN, k.a.gg_s, k.a.gg_sD);
+    k.a.flags = ppk::F_GRAD | (grad_input ? ppk::F_A : 0);
+    return run(k, ppk::K_PULLGRAD, wide, st);
+  }
+  return run(k, ppk::K_PULL, wide, st);
+}
+
+int pp_grid_count_backward(const pp_tensor* grad, const pp_tensor* grid, const pp_tensor* grad_grid,
+                           const pp_options* opt, void* stream) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(grad, "grad", k.D, grid->dtype))) return rc;
+  if (grad->sizes[0] != grid->sizes[0] || grad->sizes[1] != 1)
+    return fail(PP_ERR_ARG, "(): grad must be (N, 1, *shape)");
+  if (grad->dtype != grid->dtype) return fail(PP_ERR_DTYPE, "(): grad must have the grid dtype");
+  if ((rc = check_ggrad(grad_grid, grid))) return rc;
+  k.dtype = grid->dtype;
+  k.a.C = 1;
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? grad->sizes[2 + a] : 1;
+  k.a.src = grad->data;
+  set_image(grad, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.gg = grad_grid->data;
+  set_grid(grad_grid, k.D, k.a.gg_sN, k.a.gg_s, k.a.gg_sD);
+  k.a.flags = ppk::F_GRAD | ppk::F_NOTRGT;
+  return run(k, ppk::K_PUSHGRAD, need_wide(k, {grad}), static_cast<cudaStream_t>(stream));
+}
+
+int pp_grid_grad_backward(const pp_tensor* grad, const pp_tensor* input, const pp_tensor* grid,
+                          const pp_tensor* grad_input, const pp_tensor* grad_grid,
+                          const pp_options* opt, void* stream, void* workspace, size_t workspace_bytes) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if ((rc = check_tensor(grad, "grad"))) return rc;
+  int64_t gsz[6] = {grid->sizes[0], input->sizes[1], 1, 1, 1, 1};
+  for (int a = 0; a < k.D; ++a) gsz[2 + a] = grid->sizes[1 + a];
+  gsz[2 + k.D] = k.D;
+  if ((rc = check_same_sizes(grad, gsz, k.D + 3, "grad"))) return rc;
+  if (grad->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad dtype must match input");
+  if (grad_input && (rc = check_same_sizes(grad_input, input->sizes, input->ndim, "grad_input"))) return rc;
+  if (grad_input && grad_input->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad_input dtype must match input");
+  if (grad_grid && (rc = check_ggrad(grad_grid, grid))) return rc;
+  if (!grad_input && !grad_grid) return PP_OK;
+  k.dtype = input->dtype;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  k.a.src = input->data;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.trgt = grad->data;
+  set_image(grad, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  k.a.trgt_sK = grad->strides[2 + k.D];
+  const bool wide = need_wide(k, {input, grad, grad_input});
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k.a.flags = (grad_grid ? ppk::F_GRAD : 0) | (grad_input ? ppk::F_A : 0);
+  if (grad_grid) {
+    k.a.gg = grad_grid->data;
+    set_grid(grad_grid, k.D, k.a.gg_sN, k.a.gg_s, k.a.gg_sD);
+  }
+  if (!grad_input) return run(k, ppk::K_KD, wide, st);
+  return scatter_into(k, ppk::K_KD, grad_input, wide, workspace, workspace_bytes, st);
+}
+
+}  // extern "C"

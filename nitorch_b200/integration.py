@@ -1,0 +1,56 @@
+"""Route an installed nitorch through this backend.
+
+nitorch selects its compiled backend in ``nitorch/_C/grid.py:9-79`` by
+importing ``grid_pull ... BoundType`` from the module ``nitorch._C.spatial``
+(``NI_COMPILED_BACKEND=C``), and imports its prefilter from ``interpol``
+(``grid.py:4-7``).  ``install()`` registers this package's modules under
+those names *before* nitorch is imported, so ``nitorch.spatial.grid_*`` run
+on the B200 kernels unmodified.
+"""
+import os
+import sys
+import types
+
+
+def install(set_env=True):
+    """Register ``nitorch._C.spatial`` (and ``interpol.coeff``) aliases.
+
+    Must run before ``import nitorch``.  Returns the spatial module.
+    """
+    from . import coeff, spatial
+    if set_env:
+        os.environ["NI_COMPILED_BACKEND"] = "C"
+    sys.modules["nitorch._C.spatial"] = spatial
+    if "interpol" not in sys.modules:
+        # Minimal interpol stand-in: the prefilter plus the names grid.py
+        # imports from it (grid.py:4-7).
+        from .enums import BoundType
+        pkg = types.ModuleType("interpol")
+        pkg.__path__ = []
+        mcoeff = types.ModuleType("interpol.coeff")
+        mcoeff.spline_coeff = coeff.spline_coeff
+        mcoeff.spline_coeff_nd = coeff.spline_coeff_nd
+        mpush = types.ModuleType("interpol.pushpull")
+        mpush.grid_push = spatial.grid_push
+        mbounds = types.ModuleType("interpol.bounds")
+        import enum
+
+        class _TSBoundType(enum.Enum):
+            zero = zeros = 0
+            replicate = nearest = 1
+            dct1 = mirror = 2
+            dct2 = reflect = 3
+            dst1 = antimirror = 4
+            dst2 = antireflect = 5
+            dft = wrap = 6
+        mbounds.BoundType = _TSBoundType
+        msplines = types.ModuleType("interpol.splines")
+        from .enums import InterpolationType
+        msplines.InterpolationType = InterpolationType
+        for name, m in (("coeff", mcoeff), ("pushpull", mpush), ("bounds", mbounds),
+                        ("splines", msplines)):
+            setattr(pkg, name, m)
+            sys.modules[f"interpol.{name}"] = m
+        sys.modules["interpol"] = pkg
+        del BoundType
+    return spatial

@@ -1,0 +1,300 @@
+"""Python front-end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module.  The product (``nitorch_b200``) never does.
+
+It wraps ``pushpull_oracle.c`` (a plain-C restatement of the reference's
+push/pull and prefilter arithmetic, compiled by ``oracle/Makefile``) with
+numpy-based functions that mirror the reference's native front-end
+(``nitorch/_C/src/pushpull.cpp:76-327``): same argument meaning, same
+output shapes, same mode wiring (``pushpull.cpp`` flag table).
+
+Bounds and orders are given as lists of compiled-backend codes
+(``nitorch/_C/src/bounds.h``: replicate 0, dct1 1, dct2 2, dst1 3, dst2 4,
+dft 5, zero 7; orders 0-7), padded with the last entry as the reference's
+allocator does (``pushpull_common.cpp:91-120``).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+
+PULL, PUSH, COUNT, GRAD, SGRAD = 1, 2, 4, 8, 16
+QUIRK_D1, QUIRK_D3 = 1, 4
+
+_LIBS = {}
+
+
+def build():
+    """Compile the oracle libraries (gcc only; seconds)."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def lib(real="f64"):
+    if real not in _LIBS:
+        path = os.path.join(BUILD, f"liboracle_{real}.so")
+        if not os.path.exists(path):
+            build()
+        _LIBS[real] = _declare(ctypes.CDLL(path), real)
+    return _LIBS[real]
+
+
+def _ctype(real):
+    return ctypes.c_double if real == "f64" else ctypes.c_float
+
+
+def _declare(L, real):
+    R = _ctype(real)
+    i64 = ctypes.c_int64
+    P = ctypes.c_void_p
+
+    class Params(ctypes.Structure):
+        _fields_ = [
+            ("dim", ctypes.c_int), ("bound", ctypes.c_int * 3),
+            ("order", ctypes.c_int * 3), ("extrapolate", ctypes.c_int),
+            ("mode", ctypes.c_int), ("quirks", ctypes.c_int),
+            ("N", i64), ("C", i64), ("src_size", i64 * 3),
+            ("trgt_size", i64 * 3), ("trgt_K", i64),
+            ("src", P), ("src_s", i64 * 5),
+            ("trgt", P), ("trgt_s", i64 * 6),
+            ("grid", P), ("grid_s", i64 * 5),
+            ("out", P), ("out_s", i64 * 6),
+            ("ggrad", P), ("ggrad_s", i64 * 5),
+        ]
+
+    L.Params = Params
+    assert ctypes.sizeof(Params) == L.or_params_size(), "oracle ABI mismatch"
+    L.or_pushpull.argtypes = [ctypes.POINTER(Params)]
+    L.or_pushpull.restype = ctypes.c_int
+    L.or_bound_index.argtypes = [ctypes.c_int, i64, i64]
+    L.or_bound_index.restype = i64
+    L.or_bound_sign.argtypes = [ctypes.c_int, i64, i64]
+    L.or_bound_sign.restype = ctypes.c_int
+    for name in ("or_weight", "or_fastweight", "or_fastgrad"):
+        getattr(L, name).argtypes = [ctypes.c_int, R]
+        getattr(L, name).restype = R
+    L.or_fasthess.argtypes = [ctypes.c_int, R, ctypes.c_int]
+    L.or_fasthess.restype = R
+    L.or_support_low.argtypes = [ctypes.c_int, R]
+    L.or_support_low.restype = i64
+    L.or_coeff_axis.argtypes = [P, ctypes.c_int, ctypes.POINTER(i64),
+                                ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.or_coeff_axis.restype = ctypes.c_int
+    return L
+
+
+def _pad(v, n):
+    v = list(v) if isinstance(v, (list, tuple)) else [v]
+    v = v + v[-1:] * max(0, n - len(v))
+    return [int(x) for x in v[:n]] + [0] * (3 - n)
+
+
+def _strides(a):
+    return [s // a.itemsize for s in a.strides]
+
+
+def _np(real):
+    return np.float64 if real == "f64" else np.float32
+
+
+def _run(real, dim, bound, order, extrapolate, mode, *, src=None, src_size,
+         trgt=None, grid, out=None, ggrad=None, trgt_K=0, quirks=0):
+    L = lib(real)
+    p = L.Params()
+    p.dim = dim
+    p.bound[:] = _pad(bound, dim)
+    p.order[:] = _pad(order, dim)
+    p.extrapolate = int(extrapolate)
+    p.mode = mode
+    p.quirks = quirks
+    p.N = grid.shape[0]
+    p.C = (src.shape[1] if src is not None else
+           trgt.shape[1] if trgt is not None else 1)
+    p.src_size[:] = list(src_size) + [1] * (3 - dim)
+    p.trgt_size[:] = list(grid.shape[1:1 + dim]) + [1] * (3 - dim)
+    p.trgt_K = trgt_K
+
+    def put(name, arr, nstride):
+        if arr is None:
+            setattr(p, name, None)
+            return
+        s = _strides(arr)
+        full = [0] * nstride
+        setattr(p, name, arr.ctypes.data)
+        return s, full
+
+    if src is not None:
+        s = _strides(src)
+        p.src = src.ctypes.data
+        p.src_s[:] = s[:2] + s[2:2 + dim] + [0] * (3 - dim)
+    if trgt is not None:
+        s = _strides(trgt)
+        p.trgt = trgt.ctypes.data
+        sk = s[2 + dim] if trgt.ndim == dim + 3 else 0
+        p.trgt_s[:] = s[:2] + s[2:2 + dim] + [0] * (3 - dim) + [sk]
+    s = _strides(grid)
+    p.grid = grid.ctypes.data
+    p.grid_s[:] = [s[0]] + s[1:1 + dim] + [0] * (3 - dim) + [s[1 + dim]]
+    if out is not None:
+        s = _strides(out)
+        p.out = out.ctypes.data
+        sk = s[2 + dim] if out.ndim == dim + 3 else 0
+        p.out_s[:] = s[:2] + s[2:2 + dim] + [0] * (3 - dim) + [sk]
+    if ggrad is not None:
+        s = _strides(ggrad)
+        p.ggrad = ggrad.ctypes.data
+        p.ggrad_s[:] = [s[0]] + s[1:1 + dim] + [0] * (3 - dim) + [s[1 + dim]]
+    rc = L.or_pushpull(ctypes.byref(p))
+    if rc != 0:
+        raise RuntimeError(f"oracle failed with {rc}")
+
+
+def _prep(real, *arrays):
+    dt = _np(real)
+    return [None if a is None else np.asarray(a, dtype=dt) for a in arrays]
+
+
+# --------------------------------------------------------------------- #
+# The eight reference operations (pushpull.cpp:76-327)                  #
+# --------------------------------------------------------------------- #
+
+def grid_pull(inp, grid, bound, order, extrapolate, real="f64", quirks=0):
+    inp, grid = _prep(real, inp, grid)
+    dim = grid.shape[-1]
+    out = np.zeros(inp.shape[:2] + grid.shape[1:1 + dim], dtype=inp.dtype)
+    _run(real, dim, bound, order, extrapolate, PULL, src=inp,
+         src_size=inp.shape[2:], grid=grid, out=out, quirks=quirks)
+    return out
+
+
+def grid_pull_backward(grad, inp, grid, bound, order, extrapolate,
+                       need_input=True, need_grid=True, real="f64", quirks=0):
+    grad, inp, grid = _prep(real, grad, inp, grid)
+    dim = grid.shape[-1]
+    res = []
+    gi = np.zeros(inp.shape, inp.dtype) if need_input else None
+    gg = np.zeros(grid.shape, grid.dtype) if need_grid else None
+    mode = (PUSH if need_input else 0) | (GRAD if need_grid else 0)
+    if mode:
+        _run(real, dim, bound, order, extrapolate, mode, src=inp,
+             src_size=inp.shape[2:], trgt=grad, grid=grid, out=gi, ggrad=gg,
+             quirks=quirks)
+    if need_input:
+        res.append(gi)
+    if need_grid:
+        res.append(gg)
+    return res
+
+
+def grid_push(inp, grid, shape, bound, order, extrapolate, real="f64", quirks=0):
+    inp, grid = _prep(real, inp, grid)
+    dim = grid.shape[-1]
+    shape = tuple(shape) if shape else tuple(inp.shape[2:])
+    out = np.zeros(inp.shape[:2] + shape, dtype=inp.dtype)
+    _run(real, dim, bound, order, extrapolate, PUSH, src_size=shape,
+         trgt=inp, grid=grid, out=out, quirks=quirks)
+    return out
+
+
+def grid_push_backward(grad, inp, grid, bound, order, extrapolate,
+                       need_input=True, need_grid=True, real="f64", quirks=0):
+    grad, inp, grid = _prep(real, grad, inp, grid)
+    dim = grid.shape[-1]
+    res = []
+    gi = np.zeros(inp.shape, inp.dtype) if need_input else None
+    gg = np.zeros(grid.shape, grid.dtype) if need_grid else None
+    mode = (PULL if need_input else 0) | (GRAD if need_grid else 0)
+    if mode:
+        _run(real, dim, bound, order, extrapolate, mode, src=grad,
+             src_size=grad.shape[2:], trgt=inp, grid=grid, out=gi, ggrad=gg,
+             quirks=quirks)
+    if need_input:
+        res.append(gi)
+    if need_grid:
+        res.append(gg)
+    return res
+
+
+def grid_count(grid, shape, bound, order, extrapolate, real="f64", quirks=0):
+    (grid,) = _prep(real, grid)
+    dim = grid.shape[-1]
+    shape = tuple(shape) if shape else tuple(grid.shape[1:1 + dim])
+    out = np.zeros((grid.shape[0], 1) + shape, dtype=grid.dtype)
+    _run(real, dim, bound, order, extrapolate, COUNT, src_size=shape,
+         grid=grid, out=out, quirks=quirks)
+    return out
+
+
+def grid_count_backward(grad, grid, bound, order, extrapolate, real="f64",
+                        quirks=0):
+    grad, grid = _prep(real, grad, grid)
+    dim = grid.shape[-1]
+    gg = np.zeros(grid.shape, grid.dtype)
+    _run(real, dim, bound, order, extrapolate, GRAD, src=grad,
+         src_size=grad.shape[2:], grid=grid, ggrad=gg, quirks=quirks)
+    return gg
+
+
+def grid_grad(inp, grid, bound, order, extrapolate, real="f64", quirks=0):
+    inp, grid = _prep(real, inp, grid)
+    dim = grid.shape[-1]
+    out = np.zeros(inp.shape[:2] + grid.shape[1:1 + dim] + (dim,), inp.dtype)
+    _run(real, dim, bound, order, extrapolate, SGRAD, src=inp,
+         src_size=inp.shape[2:], grid=grid, out=out, quirks=quirks)
+    return out
+
+
+def grid_grad_backward(grad, inp, grid, bound, order, extrapolate,
+                       need_input=True, need_grid=True, real="f64", quirks=0):
+    grad, inp, grid = _prep(real, grad, inp, grid)
+    dim = grid.shape[-1]
+    res = []
+    gi = np.zeros(inp.shape, inp.dtype) if need_input else None
+    gg = np.zeros(grid.shape, grid.dtype) if need_grid else None
+    mode = (PUSH if need_input else 0) | (GRAD if need_grid else 0)
+    if mode:
+        _run(real, dim, bound, order, extrapolate, mode, src=inp,
+             src_size=inp.shape[2:], trgt=grad, grid=grid, out=gi, ggrad=gg,
+             trgt_K=dim, quirks=quirks)
+    if need_input:
+        res.append(gi)
+    if need_grid:
+        res.append(gg)
+    return res
+
+
+# --------------------------------------------------------------------- #
+# Prefilter (_ts/coeff.py:285-344), FP64                                #
+# --------------------------------------------------------------------- #
+
+def spline_coeff(inp, bound_ts, order, dim=-1):
+    """One axis.  ``bound_ts`` uses the prefilter's integer codes
+    (_ts/bounds.py:7-14): zero 0, replicate 1, dct1 2, dct2 3, dft 6."""
+    a = np.ascontiguousarray(np.asarray(inp, dtype=np.float64)).copy()
+    axis = dim % a.ndim
+    shape = (ctypes.c_int64 * a.ndim)(*a.shape)
+    rc = lib("f64").or_coeff_axis(a.ctypes.data, a.ndim, shape, axis,
+                                  int(bound_ts), int(order))
+    if rc == -2:
+        raise NotImplementedError("prefilter bound not implemented")
+    if rc:
+        raise ValueError(f"prefilter failed with {rc}")
+    return a
+
+
+def spline_coeff_nd(inp, bound_ts, order, dim=None):
+    a = np.asarray(inp, dtype=np.float64)
+    dim = a.ndim if dim is None else dim
+    b = _pad(bound_ts, dim)[:dim]
+    o = _pad(order, dim)[:dim]
+    for d in range(dim):
+        a = spline_coeff(a, b[d], o[d], dim=-dim + d)
+    return a
+
+
+# compiled-backend bound code -> prefilter code (grid.py:133 via _TSBoundType)
+BOUND_TO_TS = {0: 1, 1: 2, 2: 3, 3: 4, 4: 5, 5: 6, 7: 0}

@@ -1,0 +1,53 @@
+"""Loaders for the reference implementation itself -- TEST INFRASTRUCTURE.
+
+* ``load_compiled()``: the reference's own C++ CPU backend, compiled from the
+  reference sources by ``oracle/build_ref.py`` into ``oracle/_ref/``
+  (the module ``nitorch._C.spatial``).  Returns None when not built.
+* ``load_ts_coeff()``: the reference's vendored prefilter
+  ``nitorch/_C/_ts/coeff.py`` imported from the reference tree, when that
+  tree is present (only in the development container, never on a GPU box).
+
+Only the tests, the golden-fixture generator and the CPU-baseline leg of the
+benchmark use these.
+"""
+import importlib.util
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "spatial.so")
+REFERENCE_ROOT = os.environ.get("NITORCH_REFERENCE", "/root/reference")
+
+_compiled = None
+_ts = None
+
+
+def load_compiled():
+    """The compiled reference module (``nitorch._C.spatial``) or None."""
+    global _compiled
+    if _compiled is None and os.path.exists(REF_SO):
+        import torch  # noqa: F401  (the extension links against libtorch)
+        spec = importlib.util.spec_from_file_location("spatial", REF_SO)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _compiled = mod
+    return _compiled
+
+
+def load_ts_coeff():
+    """The reference's vendored prefilter module, or None if the reference
+    tree is absent.  Its package uses relative imports, so it is loaded as a
+    package named ``_ref_interpol`` rooted at ``nitorch/_C/_ts``."""
+    global _ts
+    if _ts is None:
+        root = os.path.join(REFERENCE_ROOT, "nitorch", "_C", "_ts")
+        if not os.path.isdir(root):
+            return None
+        spec = importlib.util.spec_from_file_location(
+            "_ref_interpol", os.path.join(root, "__init__.py"),
+            submodule_search_locations=[root])
+        pkg = importlib.util.module_from_spec(spec)
+        sys.modules["_ref_interpol"] = pkg
+        spec.loader.exec_module(pkg)
+        _ts = sys.modules["_ref_interpol.coeff"]
+    return _ts

@@ -1,0 +1,161 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a checkout where the reference is available:
+    python oracle/build_ref.py            # compiles nitorch/_C into oracle/_ref
+    python tests/golden/make_golden.py
+
+Writes
+  pushpull_golden.npz : seeded small inputs and the compiled reference's
+                        outputs of its eight push/pull functions, float64,
+                        1/2/3-D, seven bounds, orders 0-7; float32 order-0
+                        cases for the bit-exact checks.
+  coeff_golden.npz    : outputs of the reference's vendored prefilter
+                        (nitorch/_C/_ts/coeff.py) for orders 2-7, bounds
+                        dct1 / dct2 / dft, several line lengths, plus 3-D
+                        spline_coeff_nd volumes.
+  config1_golden.npz  : checksums of the reference's pull / push on the
+                        seeded config-1 workload (1x1x64^3, order 1, dct2).
+
+Reference defects are handled as in tests/test_oracle_vs_reference.py: the
+grid_grad_backward target is laid out with a last-dimension stride > 1 (D2),
+and 1-D grid_grad is generated with extrapolation on (D6).  Orders 5-7 of
+grid_grad_backward carry defect D3 (zero second derivatives); those grid
+gradients are stored under a "_d3" key.
+"""
+import os
+import sys
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import reference as R  # noqa: E402
+from tests._cases import BOUND_CODES, ORDERS, make_case, config1_inputs  # noqa: E402
+
+
+def _t(a, rg=False):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return t.requires_grad_(rg) if rg else t
+
+
+def _strided_last(a):
+    n, c, k = a.shape[0], a.shape[1], a.shape[-1]
+    sp = a.shape[2:-1]
+    p = int(np.prod(sp))
+    st, acc = [], 1
+    for s in reversed(sp):
+        st.insert(0, acc)
+        acc *= s
+    t = torch.empty_strided(a.shape, [c * k * p, k * p] + st + [p], dtype=torch.float64)
+    t.copy_(torch.from_numpy(a))
+    return t
+
+
+def pushpull(ref):
+    B = {v.value: v for v in ref.BoundType.__members__.values()}
+    I = {v.value: v for v in ref.InterpolationType.__members__.values()}
+    out = {}
+    for dim in (1, 2, 3):
+        for bound in BOUND_CODES:
+            for order in ORDERS:
+                key = f"d{dim}_b{bound}_o{order}"
+                vol, grid = make_case(dim, seed=7000 + 100 * dim + 10 * bound + order,
+                                      in_size=5 if dim < 3 else 4, out_size=4 if dim < 3 else 3)
+                g = np.random.default_rng(8000 + 100 * dim + 10 * bound + order)
+                tgt = g.standard_normal((1, vol.shape[1]) + grid.shape[1:-1])
+                gpush = g.standard_normal(vol.shape)
+                gcount = g.standard_normal((1, 1) + vol.shape[2:])
+                ggrad = g.standard_normal((1, vol.shape[1]) + grid.shape[1:-1] + (dim,))
+                b, o = [B[bound]], [I[order]]
+                ex = 1
+                out[key + "_vol"] = vol
+                out[key + "_grid"] = grid
+                out[key + "_tgt"] = tgt
+                out[key + "_gpush"] = gpush
+                out[key + "_gcount"] = gcount
+                out[key + "_ggrad"] = ggrad
+                out[key + "_pull"] = ref.grid_pull(_t(vol), _t(grid), b, o, ex).numpy()
+                out[key + "_sgrad"] = ref.grid_grad(_t(vol), _t(grid), b, o, ex).numpy()
+                out[key + "_push"] = ref.grid_push(_t(tgt), _t(grid), list(vol.shape[2:]), b, o, ex).numpy()
+                out[key + "_count"] = ref.grid_count(_t(grid), list(vol.shape[2:]), b, o, ex).numpy()
+                r = ref.grid_pull_backward(_t(tgt), _t(vol, True), _t(grid, True), b, o, ex)
+                out[key + "_pullbwd_in"] = r[0].detach().numpy()
+                out[key + "_pullbwd_grid"] = r[1].detach().numpy()
+                r = ref.grid_push_backward(_t(gpush), _t(tgt, True), _t(grid, True), b, o, ex)
+                out[key + "_pushbwd_in"] = r[0].detach().numpy()
+                out[key + "_pushbwd_grid"] = r[1].detach().numpy()
+                r = ref.grid_count_backward(_t(gcount), _t(grid, True), b, o, ex)
+                out[key + "_countbwd_grid"] = r.detach().numpy()
+                r = ref.grid_grad_backward(_strided_last(ggrad), _t(vol, True), _t(grid, True), b, o, ex)
+                out[key + "_gradbwd_in"] = r[0].detach().numpy()
+                out[key + ("_gradbwd_grid_d3" if order >= 5 else "_gradbwd_grid")] = r[1].detach().numpy()
+    # float32 order-0 cases, no extrapolation (OOB mask) and both tolerances
+    for dim in (1, 2, 3):
+        for bound in BOUND_CODES:
+            vol, grid = make_case(dim, seed=9000 + 10 * dim + bound, spread=3.0)
+            vol = vol.astype(np.float32)
+            grid = grid.astype(np.float32)
+            key = f"f32_d{dim}_b{bound}"
+            out[key + "_vol"] = vol
+            out[key + "_grid"] = grid
+            for ex in (0, 1, 2):
+                out[key + f"_pull_ex{ex}"] = ref.grid_pull(_t(vol), _t(grid), [B[bound]], [I[0]], ex).numpy()
+    return out
+
+
+def coeff(ts):
+    out = {}
+    r = np.random.default_rng(4242)
+    for order in range(2, 8):
+        for bound in (2, 3, 6):
+            for n in (2, 3, 7, 40):
+                x = r.standard_normal((3, n))
+                y = ts.spline_coeff(torch.from_numpy(x.copy()), bound, order, dim=-1).numpy()
+                out[f"o{order}_b{bound}_n{n}_x"] = x
+                out[f"o{order}_b{bound}_n{n}_y"] = y
+    for order in (2, 3, 5, 7):
+        x = r.standard_normal((2, 6, 5, 7))
+        y = ts.spline_coeff_nd(torch.from_numpy(x.copy()), [3], [order], dim=3).numpy()
+        out[f"nd_o{order}_x"] = x
+        out[f"nd_o{order}_y"] = y
+    return out
+
+
+def config1(ref):
+    x, grid, y = config1_inputs()
+    B, I = ref.BoundType.dct2, ref.InterpolationType.linear
+    tx, tg, ty = (torch.from_numpy(a) for a in (x, grid, y))
+    out = {}
+    p = ref.grid_pull(tx, tg, [B], [I], 0)
+    q = ref.grid_push(ty, tg, list(x.shape[2:]), [B], [I], 0)
+    out["pull_sum"] = p.sum().item()
+    out["pull_sumsq"] = (p * p).sum().item()
+    out["push_sum"] = q.sum().item()
+    out["push_sumsq"] = (q * q).sum().item()
+    out["inner_pull_y"] = (p * ty).sum().item()
+    out["inner_x_push"] = (tx * q).sum().item()
+    out["pull_slice"] = p[0, 0, 32].numpy()
+    out["push_slice"] = q[0, 0, 32].numpy()
+    return {k: np.asarray(v) for k, v in out.items()}
+
+
+def main():
+    ref = R.load_compiled()
+    if ref is None:
+        raise SystemExit("build the reference first: python oracle/build_ref.py")
+    torch.set_num_threads(1)
+    np.savez_compressed(os.path.join(HERE, "pushpull_golden.npz"), **pushpull(ref))
+    ts = R.load_ts_coeff()
+    if ts is None:
+        raise SystemExit("reference tree not found (NITORCH_REFERENCE)")
+    np.savez_compressed(os.path.join(HERE, "coeff_golden.npz"), **coeff(ts))
+    np.savez_compressed(os.path.join(HERE, "config1_golden.npz"), **config1(ref))
+    for f in ("pushpull_golden.npz", "coeff_golden.npz", "config1_golden.npz"):
+        print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()
