@@ -7,9 +7,9 @@
 //   spline polynomials : nitorch/_C/src/impl/interpolation_common.h:57-815
 //   support (low node) : interpolation_common.h bounds0..7 (round for
 //                        order 0, floor of x - (p-1)/2 otherwise)
-// The B-spline pieces are the standard centred B-spline polynomials; second
-// derivatives for orders >= 5 use  B''_p(x) = B_{p-2}(x+1) - 2 B_{p-2}(x)
-// + B_{p-2}(x-1)  (the reference leaves them at zero).
+// Weights and derivatives come from the Cox-de Boor recurrence
+// (bspline_stencil); second derivatives are exact at every order (the
+// reference leaves them at zero for orders 5-7).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -107,118 +107,69 @@ __device__ __forceinline__ int bound_sign(int b, I i, I n) {
 }
 
 // ---------------------------------------------------------------------
-// B-spline pieces. x is the signed distance node - sample, |x| inside the
-// support (the callers only evaluate nodes of the support).
+// B-spline stencil of one axis.
+//
+// The p+1 non-zero weights of a sample are values of the cardinal B-spline
+// M_p (support [0, p+1]; B_p(x) = M_p(x + (p+1)/2)) at f + i, i = 0..p,
+// where f in [0,1) is the sample's offset from its support.  They are
+// evaluated together by the Cox-de Boor recurrence
+//     M_k(s) = ( s M_{k-1}(s) + (k+1-s) M_{k-1}(s-1) ) / k,
+// whose terms are all non-negative (accurate to a few ulps at every order,
+// where Horner forms of the order-7 pieces lose ~4 digits in float32).
+// Derivatives use  M_p' (s) = M_{p-1}(s) - M_{p-1}(s-1)  and
+// M_p''(s) = M_{p-2}(s) - 2 M_{p-2}(s-1) + M_{p-2}(s-2), i.e. the rows of
+// the same recurrence at k = p-1 and k = p-2.
+// Tap j sits on node low + j at signed distance dx_j = x - (low + j); its
+// weight is B_p(dx_j) = M_p(f + p - j), i.e. row[p - j].
+// NT: compile-time max taps (>= p+1); p may be a run-time value.
 // ---------------------------------------------------------------------
-template <class T>
-__device__ __forceinline__ T bs_weight(int order, T x) {
-  x = fabs(x);
-  switch (order) {
-    case 0: return T(1);
-    case 1: return T(1) - x;
-    case 2:
-      if (x < T(0.5)) return T(0.75) - x * x;
-      x = T(1.5) - x; return T(0.5) * x * x;
-    case 3:
-      if (x < T(1)) return (x * x * (x - T(2)) * T(3) + T(4)) * T(1.0 / 6.0);
-      x = T(2) - x; return x * x * x * T(1.0 / 6.0);
-    case 4:
-      if (x < T(0.5)) { x *= x; return x * (x * T(0.25) - T(0.625)) + T(115.0 / 192.0); }
-      if (x < T(1.5)) return x * (x * (x * (T(5) - x) * T(1.0 / 6.0) - T(1.25)) + T(5.0 / 24.0)) + T(55.0 / 96.0);
-      x -= T(2.5); x *= x; return x * x * T(1.0 / 24.0);
-    case 5:
-      if (x < T(1)) { T f = x * x; return f * (f * (T(0.25) - x * T(1.0 / 12.0)) - T(0.5)) + T(0.55); }
-      if (x < T(2)) return x * (x * (x * (x * (x * T(1.0 / 24.0) - T(0.375)) + T(1.25)) - T(1.75)) + T(0.625)) + T(0.425);
-      { T f = T(3) - x; x = f * f; return f * x * x * T(1.0 / 120.0); }
-    case 6:
-      if (x < T(0.5)) { x *= x;
-        return x * (x * (T(7.0 / 48.0) - x * T(1.0 / 36.0)) - T(77.0 / 192.0)) + T(5887.0 / 11520.0); }
-      if (x < T(1.5))
-        return x * (x * (x * (x * (x * (x * T(1.0 / 48.0) - T(7.0 / 48.0)) + T(0.328125))
-               - T(35.0 / 288.0)) - T(91.0 / 256.0)) - T(7.0 / 768.0)) + T(7861.0 / 15360.0);
-      if (x < T(2.5))
-        return x * (x * (x * (x * (x * (T(7.0 / 60.0) - x * T(1.0 / 120.0)) - T(0.65625))
-               + T(133.0 / 72.0)) - T(2.5703125)) + T(1267.0 / 960.0)) + T(1379.0 / 7680.0);
-      x -= T(3.5); x *= x * x; return x * x * T(1.0 / 720.0);
-    default:  // 7
-      if (x < T(1)) { T f = x * x;
-        return f * (f * (f * (x * T(1.0 / 144.0) - T(1.0 / 36.0)) + T(1.0 / 9.0)) - T(1.0 / 3.0)) + T(151.0 / 315.0); }
-      if (x < T(2))
-        return x * (x * (x * (x * (x * (x * (T(0.05) - x * T(1.0 / 240.0)) - T(7.0 / 30.0))
-               + T(0.5)) - T(7.0 / 18.0)) - T(0.1)) - T(7.0 / 90.0)) + T(103.0 / 210.0);
-      if (x < T(3))
-        return x * (x * (x * (x * (x * (x * (x * T(1.0 / 720.0) - T(1.0 / 36.0)) + T(7.0 / 30.0))
-               - T(19.0 / 18.0)) + T(49.0 / 18.0)) - T(23.0 / 6.0)) + T(217.0 / 90.0)) - T(139.0 / 630.0);
-      { T f = T(4) - x; x = f * f * f; return x * x * f * T(1.0 / 5040.0); }
+template <int NT, bool NEED_G, bool NEED_H, class T>
+__device__ __forceinline__ void bspline_stencil(int p, T f, T (&w)[NT], T (&g)[NT], T (&h)[NT]) {
+  T b[NT + 1], c[NT + 1], d[NT + 1];
+#pragma unroll
+  for (int i = 0; i <= NT; ++i) { b[i] = i == 0 ? T(1) : T(0); c[i] = b[i]; d[i] = b[i]; }
+#pragma unroll
+  for (int k = 1; k < NT; ++k) {
+    if (k <= p) {
+      if (NEED_H && k == p - 1) {
+#pragma unroll
+        for (int i = 0; i <= NT; ++i) d[i] = b[i];
+      }
+      if (NEED_G && k == p) {
+#pragma unroll
+        for (int i = 0; i <= NT; ++i) c[i] = b[i];
+      }
+      const T ik = T(1) / T(k);
+#pragma unroll
+      for (int i = k; i >= 0; --i) {
+        const T lo = i > 0 ? b[i - 1] : T(0);
+        b[i] = ((f + T(i)) * b[i] + (T(k + 1 - i) - f) * lo) * ik;
+      }
+    }
   }
-}
-
-// Weight with support test (0 outside), used for derivative identities.
-template <class T>
-__device__ __forceinline__ T bs_weight_full(int order, T x) {
-  T a = fabs(x);
-  if (a >= T(0.5) * T(order + 1)) return T(0);
-  return bs_weight(order, x);
-}
-
-template <class T>
-__device__ __forceinline__ T bs_grad(int order, T x) {
-  bool neg = x < T(0);
-  if (neg) x = -x;
-  T r;
-  switch (order) {
-    case 0: return T(0);
-    case 1: return neg ? T(1) : T(-1);
-    case 2: r = x < T(0.5) ? T(-2) * x : x - T(1.5); break;
-    case 3:
-      if (x < T(1)) r = x * (x * T(1.5) - T(2));
-      else { T t = T(2) - x; r = -(t * t) * T(0.5); }
-      break;
-    case 4:
-      if (x < T(0.5)) r = x * (x * x - T(1.25));
-      else if (x < T(1.5)) r = x * (x * (x * T(-2.0 / 3.0) + T(2.5)) - T(2.5)) + T(5.0 / 24.0);
-      else { T t = x * T(2) - T(5); r = t * t * t * T(1.0 / 48.0); }
-      break;
-    case 5:
-      if (x < T(1)) r = x * (x * (x * (x * T(-5.0 / 12.0) + T(1))) - T(1));
-      else if (x < T(2)) r = x * (x * (x * (x * T(5.0 / 24.0) - T(1.5)) + T(3.75)) - T(3.5)) + T(0.625);
-      else { T t = x - T(3); t *= t; r = -(t * t) * T(1.0 / 24.0); }
-      break;
-    case 6:
-      if (x < T(0.5)) { T x2 = x * x; r = x * (x2 * T(7.0 / 12.0) - x2 * x2 * T(1.0 / 6.0) - T(77.0 / 96.0)); }
-      else if (x < T(1.5))
-        r = x * (x * (x * (x * (x * T(0.125) - T(35.0 / 48.0)) + T(1.3125)) - T(35.0 / 96.0)) - T(0.7109375)) - T(7.0 / 768.0);
-      else if (x < T(2.5))
-        r = x * (x * (x * (x * (x * T(-1.0 / 20.0) + T(7.0 / 12.0)) - T(2.625)) + T(133.0 / 24.0)) - T(5.140625)) + T(1267.0 / 960.0);
-      else { T t = x * T(2) - T(7); T t2 = t * t; r = t2 * t2 * t * T(1.0 / 3840.0); }
-      break;
-    default:  // 7
-      if (x < T(1)) { T x2 = x * x;
-        r = x * (x2 * (x2 * (x * T(7.0 / 144.0) - T(1.0 / 6.0)) + T(4.0 / 9.0)) - T(2.0 / 3.0)); }
-      else if (x < T(2))
-        r = x * (x * (x * (x * (x * (x * T(-7.0 / 240.0) + T(3.0 / 10.0)) - T(7.0 / 6.0)) + T(2)) - T(7.0 / 6.0)) - T(1.0 / 5.0)) - T(7.0 / 90.0);
-      else if (x < T(3))
-        r = x * (x * (x * (x * (x * (x * T(7.0 / 720.0) - T(1.0 / 6.0)) + T(7.0 / 6.0)) - T(38.0 / 9.0)) + T(49.0 / 6.0)) - T(23.0 / 3.0)) + T(217.0 / 90.0);
-      else { T t = x - T(4); T t3 = t * t * t; r = -(t3 * t3) * T(1.0 / 720.0); }
-      break;
+  if (NEED_H && p <= 1) {
+#pragma unroll
+    for (int i = 0; i <= NT; ++i) d[i] = T(0);
   }
-  return neg ? -r : r;
-}
-
-template <class T>
-__device__ __forceinline__ T bs_hess(int order, T x) {
-  T a = fabs(x);
-  switch (order) {
-    case 0: case 1: return T(0);
-    case 2: return a < T(0.5) ? T(-2) : T(1);
-    case 3: return a < T(1) ? a * T(3) - T(2) : T(2) - a;
-    case 4:
-      if (a < T(0.5)) return a * a * T(3) - T(1.25);
-      if (a < T(1.5)) return a * (a * T(-2) + T(5)) - T(2.5);
-      { T t = a * T(2) - T(5); return t * t * T(0.125); }
-    default:
-      return bs_weight_full(order - 2, x + T(1)) - T(2) * bs_weight_full(order - 2, x)
-           + bs_weight_full(order - 2, x - T(1));
+#pragma unroll
+  for (int j = 0; j < NT; ++j) {
+    const int r = p - j;          // row index of tap j
+    w[j] = (r >= 0) ? b[r < 0 ? 0 : r] : T(0);
+    if (NEED_G) {
+      const T c0 = (r >= 0 && r <= NT) ? c[r < 0 ? 0 : (r > NT ? NT : r)] : T(0);
+      const T c1 = (r - 1 >= 0) ? c[r - 1 < 0 ? 0 : r - 1] : T(0);
+      g[j] = p == 0 ? T(0) : c0 - c1;
+    } else {
+      g[j] = T(0);
+    }
+    if (NEED_H) {
+      const T d0 = (r >= 0) ? d[r < 0 ? 0 : r] : T(0);
+      const T d1 = (r - 1 >= 0) ? d[r - 1 < 0 ? 0 : r - 1] : T(0);
+      const T d2 = (r - 2 >= 0) ? d[r - 2 < 0 ? 0 : r - 2] : T(0);
+      h[j] = p <= 1 ? T(0) : d0 - T(2) * d1 + d2;
+    } else {
+      h[j] = T(0);
+    }
   }
 }
 

@@ -52,7 +52,7 @@ struct PPArgs {
 template <int ORD> struct Taps { static constexpr int value = ORD < 0 ? 8 : (ORD == 0 ? 1 : ORD + 1); };
 // Unroll factor of the outermost (z) tap loop: full up to cubic, rolled for
 // higher and runtime orders (keeps code size and compile time bounded).
-template <int ORD, int NZ> struct OuterUnroll { static constexpr int value = (ORD >= 0 && ORD <= 3) ? NZ : 1; };
+template <int ORD, int NZ> struct OuterUnroll { static constexpr int value = 1; };
 
 // Per-axis stencil.  NT = max taps; unused axes have one tap of weight 1.
 template <int NT, class T, class I>
@@ -73,23 +73,20 @@ __device__ __forceinline__ void build_axis(Axis<NT, T, I>& ax, int ORDc, int bnd
   // Keep the node arithmetic defined for absurd or non-finite coordinates
   // (only reachable with extrapolation on): |x| <= 2^30, NaN -> -2^30.
   x = fmin(fmax(x, T(-1073741824.0)), T(1073741824.0));
-  I low = support_low<I, T>(ord, x);
+  const I low = support_low<I, T>(ord, x);
   const bool inside = low >= 0 && low + nt - 1 < n;
+  const T f = (x - static_cast<T>(low)) - T(0.5) * static_cast<T>(ord - 1);
+  bspline_stencil<NT, NEED_G, NEED_H, T>(ord, ord == 0 ? T(0) : f, ax.w, ax.g, ax.h);
   ax.mask = 0;
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     if (t < nt) {
-      I b = low + t;
-      T dx = x - static_cast<T>(b);
-      T w = bs_weight<T>(ord, dx);
-      T g = NEED_G ? bs_grad<T>(ord, dx) : T(0);
-      T h = NEED_H ? bs_hess<T>(ord, dx) : T(0);
+      const I b = low + t;
       int s = 1;
       I idx = b;
       if (!inside) { s = bound_sign<I>(bnd, b, n); idx = bound_index<I>(bnd, b, n); }
-      if (s == 0) { idx = 0; w = g = h = T(0); }
-      else { ax.mask |= 1u << t; if (s < 0) { w = -w; g = -g; h = -h; } }
-      ax.w[t] = w; ax.g[t] = g; ax.h[t] = h;
+      if (s == 0) { idx = 0; ax.w[t] = ax.g[t] = ax.h[t] = T(0); }
+      else { ax.mask |= 1u << t; if (s < 0) { ax.w[t] = -ax.w[t]; ax.g[t] = -ax.g[t]; ax.h[t] = -ax.h[t]; } }
       if (NEED_OS) ax.os[t] = idx * sts;
       if (NEED_OO) ax.oo[t] = idx * sto;
     } else {
@@ -107,8 +104,16 @@ __device__ __forceinline__ void unit_axis(Axis<NT, T, I>& ax) {
   for (int t = 0; t < NT; ++t) { ax.w[t] = t == 0 ? T(1) : T(0); ax.g[t] = T(0); ax.h[t] = T(0); ax.os[t] = 0; ax.oo[t] = 0; }
 }
 
-template <int D, int ORD, class S, int MODE, class I>
-__global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
+// CTA tile: 32 (last spatial axis) x 8 (second-to-last axis) sampling
+// points; blockIdx.x enumerates (outer index, tile along the last axis),
+// blockIdx.y tiles the second-to-last axis.  Neighbouring lanes and warps
+// then share most of their support, which the L1 serves.
+constexpr int TILE_IN = 32, TILE_MID = 8, PP_THREADS = TILE_IN * TILE_MID;
+
+template <int MODE> struct MinBlocks { static constexpr int value = (MODE == K_PUSH || MODE == K_COUNT) ? 3 : 2; };
+
+template <int D, int ORD, int CB, class S, int MODE, class I>
+__global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(const PPArgs a) {
   using T = typename Acc<S>::type;
   constexpr int NT = Taps<ORD>::value;
   constexpr int NX = NT, NY = D > 1 ? NT : 1, NZ = D > 2 ? NT : 1;
@@ -117,18 +122,24 @@ __global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
   constexpr bool GATHER = MODE == K_PULL || MODE == K_SGRAD || MODE == K_PULLGRAD || MODE == K_PUSHGRAD || MODE == K_KD;
   constexpr bool SCATTER = MODE == K_PUSH || MODE == K_COUNT || MODE == K_PUSHGRAD || MODE == K_KD;
 
-  const int64_t vid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (vid >= a.nvox) return;
-
-  // ---- decode sampling point (n, x, y, z), Z fastest -------------------
+  // ---- sampling point (n, x, y, z) from the 2-D tile mapping -----------
+  const I inner = static_cast<I>(a.trgt_size[D - 1]);
+  const I mid = D > 1 ? static_cast<I>(a.trgt_size[D - 2]) : I(1);
+  const I ntile = (inner + TILE_IN - 1) / TILE_IN;
+  const I outer_idx = static_cast<I>(blockIdx.x) / ntile;
+  const I ii = (static_cast<I>(blockIdx.x) - outer_idx * ntile) * TILE_IN + static_cast<I>(threadIdx.x);
+  const I mm = static_cast<I>(blockIdx.y) * TILE_MID + static_cast<I>(threadIdx.y);
+  if (ii >= inner || mm >= mid) return;
   I sub[3] = {0, 0, 0};
   I n;
-  {
-    I v = static_cast<I>(vid);
-    if (D > 2) { sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]); }
-    if (D > 1) { sub[1] = v % static_cast<I>(a.trgt_size[1]); v /= static_cast<I>(a.trgt_size[1]); }
-    sub[0] = v % static_cast<I>(a.trgt_size[0]);
-    n = v / static_cast<I>(a.trgt_size[0]);
+  if (D == 3) {
+    sub[2] = ii; sub[1] = mm;
+    sub[0] = outer_idx % static_cast<I>(a.trgt_size[0]);
+    n = outer_idx / static_cast<I>(a.trgt_size[0]);
+  } else if (D == 2) {
+    sub[1] = ii; sub[0] = mm; n = outer_idx;
+  } else {
+    sub[0] = ii; n = outer_idx;
   }
 
   // ---- coordinates ------------------------------------------------------
@@ -220,76 +231,123 @@ __global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
 
 #define PP_TAP_VALID(i, j, k) (full || ((((ax.mask >> (i)) & (ay.mask >> (j)) & (az.mask >> (k))) & 1u) != 0u))
 
+  // Channels are processed in groups of CB (compile-time): per tap, one
+  // offset and one weight feed CB loads / atomics, and the accumulators of
+  // the group live in registers.
+#define PP_CB for (int cb = 0; cb < CB; ++cb)
+  const int64_t C = MODE == K_COUNT ? 1 : a.C;
+
   // ======================= gather-only modes ================================
   if constexpr (MODE == K_PULL) {
     S* op = static_cast<S*>(a.out) + ovox;
-    for (int64_t c = 0; c < a.C; ++c) {
-      const S* sp = src_n + c * a.src_sC;
-      T acc = T(0);
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      const S* sp = src_n + c0 * a.src_sC;
+      T acc[CB];
+#pragma unroll
+      PP_CB acc[cb] = T(0);
 #pragma unroll (OuterUnroll<ORD, NZ>::value)
       for (int k = 0; k < NZ; ++k) {
         if (k < tz) {
-          T accy = T(0);
+          T accy[CB];
+#pragma unroll
+          PP_CB accy[cb] = T(0);
 #pragma unroll
           for (int j = 0; j < NY; ++j) {
             if (j < ty) {
               const I oyz = ay.os[j] + az.os[k];
-              T accx = T(0);
+              T accx[CB];
+#pragma unroll
+              PP_CB accx[cb] = T(0);
 #pragma unroll
               for (int i = 0; i < NX; ++i) {
                 if (i < tx) {
-                  T v = ldg_acc(sp + (ax.os[i] + oyz));
-                  if (!PP_TAP_VALID(i, j, k)) v = T(0);
-                  accx = fma(ax.w[i], v, accx);
+                  const I off = ax.os[i] + oyz;
+                  const bool valid = PP_TAP_VALID(i, j, k);
+#pragma unroll
+                  PP_CB {
+                    if (CB == 1 || cb < nc) {
+                      T v = ldg_acc(sp + (cb * a.src_sC + off));
+                      if (!valid) v = T(0);
+                      accx[cb] = fma(ax.w[i], v, accx[cb]);
+                    }
+                  }
                 }
               }
-              accy = fma(ay.w[j], accx, accy);
+#pragma unroll
+              PP_CB accy[cb] = fma(ay.w[j], accx[cb], accy[cb]);
             }
           }
-          acc = fma(az.w[k], accy, acc);
+#pragma unroll
+          PP_CB acc[cb] = fma(az.w[k], accy[cb], acc[cb]);
         }
       }
-      op[c * a.out_sC] = from_acc<S>(acc);
+#pragma unroll
+      PP_CB if (CB == 1 || cb < nc) op[(c0 + cb) * a.out_sC] = from_acc<S>(acc[cb]);
     }
+  }
+
+  // Spatial-gradient accumulation shared by SGRAD and PULLGRAD: per channel
+  // of the group, the interpolant (w) and its x/y/z derivatives.
+#define PP_GRAD_GATHER(EXTRA_ROW, EXTRA_PLANE)                                   \
+  T gx[CB], gy[CB], gz[CB], gw[CB];                                              \
+  _Pragma("unroll") PP_CB { gx[cb] = gy[cb] = gz[cb] = gw[cb] = T(0); }          \
+  _Pragma("unroll (OuterUnroll<ORD, NZ>::value)") for (int k = 0; k < NZ; ++k) {  \
+    if (k < tz) {                                                                \
+      T yw[CB], ygx[CB], ygy[CB];                                                \
+      _Pragma("unroll") PP_CB { yw[cb] = ygx[cb] = ygy[cb] = T(0); }             \
+      _Pragma("unroll") for (int j = 0; j < NY; ++j) {                           \
+        if (j < ty) {                                                            \
+          const I oyz = ay.os[j] + az.os[k];                                     \
+          T sx[CB], dx[CB];                                                      \
+          _Pragma("unroll") PP_CB { sx[cb] = dx[cb] = T(0); }                    \
+          _Pragma("unroll") for (int i = 0; i < NX; ++i) {                       \
+            if (i < tx) {                                                        \
+              const I off = ax.os[i] + oyz;                                      \
+              const bool valid = PP_TAP_VALID(i, j, k);                          \
+              _Pragma("unroll") PP_CB {                                          \
+                if (CB == 1 || cb < nc) {                                        \
+                  T v = ldg_acc(sp + (cb * a.src_sC + off));                     \
+                  if (!valid) v = T(0);                                          \
+                  sx[cb] = fma(ax.w[i], v, sx[cb]);                              \
+                  dx[cb] = fma(ax.g[i], v, dx[cb]);                              \
+                }                                                                \
+              }                                                                  \
+              EXTRA_ROW                                                          \
+            }                                                                    \
+          }                                                                      \
+          _Pragma("unroll") PP_CB {                                              \
+            yw[cb] = fma(ay.w[j], sx[cb], yw[cb]);                               \
+            ygx[cb] = fma(ay.w[j], dx[cb], ygx[cb]);                             \
+            ygy[cb] = fma(ay.g[j], sx[cb], ygy[cb]);                             \
+          }                                                                      \
+        }                                                                        \
+      }                                                                          \
+      _Pragma("unroll") PP_CB {                                                  \
+        gx[cb] = fma(az.w[k], ygx[cb], gx[cb]);                                  \
+        gy[cb] = fma(az.w[k], ygy[cb], gy[cb]);                                  \
+        gz[cb] = fma(az.g[k], yw[cb], gz[cb]);                                   \
+        gw[cb] = fma(az.w[k], yw[cb], gw[cb]);                                   \
+      }                                                                          \
+      EXTRA_PLANE                                                                \
+    }                                                                            \
   }
 
   if constexpr (MODE == K_SGRAD) {
     S* op = static_cast<S*>(a.out) + ovox;
-    for (int64_t c = 0; c < a.C; ++c) {
-      const S* sp = src_n + c * a.src_sC;
-      T gx = T(0), gy = T(0), gz = T(0);
-#pragma unroll (OuterUnroll<ORD, NZ>::value)
-      for (int k = 0; k < NZ; ++k) {
-        if (k < tz) {
-          T yw = T(0), ygx = T(0), ygy = T(0);
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      const S* sp = src_n + c0 * a.src_sC;
+      PP_GRAD_GATHER(, )
 #pragma unroll
-          for (int j = 0; j < NY; ++j) {
-            if (j < ty) {
-              const I oyz = ay.os[j] + az.os[k];
-              T sx = T(0), dx = T(0);
-#pragma unroll
-              for (int i = 0; i < NX; ++i) {
-                if (i < tx) {
-                  T v = ldg_acc(sp + (ax.os[i] + oyz));
-                  if (!PP_TAP_VALID(i, j, k)) v = T(0);
-                  sx = fma(ax.w[i], v, sx);
-                  dx = fma(ax.g[i], v, dx);
-                }
-              }
-              yw = fma(ay.w[j], sx, yw);
-              ygx = fma(ay.w[j], dx, ygx);
-              ygy = fma(ay.g[j], sx, ygy);
-            }
-          }
-          gx = fma(az.w[k], ygx, gx);
-          gy = fma(az.w[k], ygy, gy);
-          gz = fma(az.g[k], yw, gz);
+      PP_CB {
+        if (CB == 1 || cb < nc) {
+          S* oc = op + (c0 + cb) * a.out_sC;
+          oc[0] = from_acc<S>(gx[cb]);
+          if (D > 1) oc[a.out_sK] = from_acc<S>(gy[cb]);
+          if (D > 2) oc[2 * a.out_sK] = from_acc<S>(gz[cb]);
         }
       }
-      S* oc = op + c * a.out_sC;
-      oc[0] = from_acc<S>(gx);
-      if (D > 1) oc[a.out_sK] = from_acc<S>(gy);
-      if (D > 2) oc[2 * a.out_sK] = from_acc<S>(gz);
     }
   }
 
@@ -297,41 +355,18 @@ __global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
     // push backward: src = incoming gradient, trgt = pushed values.
     S* op = static_cast<S*>(a.out) + ovox;
     T og0 = T(0), og1 = T(0), og2 = T(0);
-    for (int64_t c = 0; c < a.C; ++c) {
-      const S* sp = src_n + c * a.src_sC;
-      T acc = T(0), gx = T(0), gy = T(0), gz = T(0);
-#pragma unroll (OuterUnroll<ORD, NZ>::value)
-      for (int k = 0; k < NZ; ++k) {
-        if (k < tz) {
-          T yw = T(0), ygx = T(0), ygy = T(0);
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      const S* sp = src_n + c0 * a.src_sC;
+      PP_GRAD_GATHER(, )
 #pragma unroll
-          for (int j = 0; j < NY; ++j) {
-            if (j < ty) {
-              const I oyz = ay.os[j] + az.os[k];
-              T sx = T(0), dx = T(0);
-#pragma unroll
-              for (int i = 0; i < NX; ++i) {
-                if (i < tx) {
-                  T v = ldg_acc(sp + (ax.os[i] + oyz));
-                  if (!PP_TAP_VALID(i, j, k)) v = T(0);
-                  sx = fma(ax.w[i], v, sx);
-                  dx = fma(ax.g[i], v, dx);
-                }
-              }
-              yw = fma(ay.w[j], sx, yw);
-              ygx = fma(ay.w[j], dx, ygx);
-              ygy = fma(ay.g[j], sx, ygy);
-            }
-          }
-          acc = fma(az.w[k], yw, acc);
-          gx = fma(az.w[k], ygx, gx);
-          gy = fma(az.w[k], ygy, gy);
-          gz = fma(az.g[k], yw, gz);
+      PP_CB {
+        if (CB == 1 || cb < nc) {
+          if (do_a) op[(c0 + cb) * a.out_sC] = from_acc<S>(gw[cb]);
+          const T t = ldg_acc(trg_v + (c0 + cb) * a.trgt_sC);
+          og0 = fma(t, gx[cb], og0); og1 = fma(t, gy[cb], og1); og2 = fma(t, gz[cb], og2);
         }
       }
-      if (do_a) op[c * a.out_sC] = from_acc<S>(acc);
-      const T t = ldg_acc(trg_v + c * a.trgt_sC);
-      og0 = fma(t, gx, og0); og1 = fma(t, gy, og1); og2 = fma(t, gz, og2);
     }
     if (do_grad) {
       T* g = static_cast<T*>(a.gg) + gvox;
@@ -343,24 +378,32 @@ __global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
 
   // ======================= scatter modes ====================================
   if constexpr (MODE == K_PUSH || MODE == K_COUNT) {
-    const int64_t C = MODE == K_COUNT ? 1 : a.C;
-    for (int64_t c = 0; c < C; ++c) {
-      const T t = MODE == K_COUNT ? T(1) : ldg_acc(trg_v + c * a.trgt_sC);
-      T* opc = outs_n + c * a.out_sC;
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      T* opc = outs_n + c0 * a.out_sC;
+      T t[CB];
+#pragma unroll
+      PP_CB t[cb] = (MODE == K_COUNT) ? T(1) : ((CB == 1 || cb < nc) ? ldg_acc(trg_v + (c0 + cb) * a.trgt_sC) : T(0));
 #pragma unroll (OuterUnroll<ORD, NZ>::value)
       for (int k = 0; k < NZ; ++k) {
         if (k < tz) {
-          const T tz_ = az.w[k] * t;
 #pragma unroll
           for (int j = 0; j < NY; ++j) {
             if (j < ty) {
-              const T tyz = ay.w[j] * tz_;
+              const T wyz = ay.w[j] * az.w[k];
               const I oyz = ay.oo[j] + az.oo[k];
 #pragma unroll
               for (int i = 0; i < NX; ++i) {
-                if (i < tx) {
-                  const T v = ax.w[i] * tyz;
-                  if (PP_TAP_VALID(i, j, k) && v != T(0)) atomic_acc(opc + (ax.oo[i] + oyz), v);
+                if (i < tx && PP_TAP_VALID(i, j, k)) {
+                  const T wt = ax.w[i] * wyz;
+                  const I off = ax.oo[i] + oyz;
+#pragma unroll
+                  PP_CB {
+                    if (CB == 1 || cb < nc) {
+                      const T v = wt * t[cb];
+                      if (v != T(0)) atomic_acc(opc + (cb * a.out_sC + off), v);
+                    }
+                  }
                 }
               }
             }
@@ -375,50 +418,78 @@ __global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
     // count backward: F_NOTRGT, t = 1, no push.
     const bool has_t = (a.flags & F_NOTRGT) == 0;
     T og0 = T(0), og1 = T(0), og2 = T(0);
-    for (int64_t c = 0; c < a.C; ++c) {
-      const S* sp = src_n + c * a.src_sC;
-      T* opc = do_a ? outs_n + c * a.out_sC : nullptr;
-      const T t = has_t ? ldg_acc(trg_v + c * a.trgt_sC) : T(1);
-      T gx = T(0), gy = T(0), gz = T(0);
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      const S* sp = src_n + c0 * a.src_sC;
+      T* opc = do_a ? outs_n + c0 * a.out_sC : nullptr;
+      T t[CB];
+#pragma unroll
+      PP_CB t[cb] = (CB == 1 || cb < nc) ? (has_t ? ldg_acc(trg_v + (c0 + cb) * a.trgt_sC) : T(1)) : T(0);
+      T gx[CB], gy[CB], gz[CB];
+#pragma unroll
+      PP_CB { gx[cb] = gy[cb] = gz[cb] = T(0); }
 #pragma unroll (OuterUnroll<ORD, NZ>::value)
       for (int k = 0; k < NZ; ++k) {
         if (k < tz) {
-          T yw = T(0), ygx = T(0), ygy = T(0);
-          const T tz_ = az.w[k] * t;
+          T yw[CB], ygx[CB], ygy[CB];
+#pragma unroll
+          PP_CB { yw[cb] = ygx[cb] = ygy[cb] = T(0); }
 #pragma unroll
           for (int j = 0; j < NY; ++j) {
             if (j < ty) {
               const I oyz = ay.os[j] + az.os[k];
               const I ooyz = ay.oo[j] + az.oo[k];
-              const T tyz = ay.w[j] * tz_;
-              T sx = T(0), dx = T(0);
+              const T wyz = ay.w[j] * az.w[k];
+              T sx[CB], dx[CB];
+#pragma unroll
+              PP_CB { sx[cb] = dx[cb] = T(0); }
 #pragma unroll
               for (int i = 0; i < NX; ++i) {
                 if (i < tx) {
                   const bool valid = PP_TAP_VALID(i, j, k);
                   if (do_grad) {
-                    T v = ldg_acc(sp + (ax.os[i] + oyz));
-                    if (!valid) v = T(0);
-                    sx = fma(ax.w[i], v, sx);
-                    dx = fma(ax.g[i], v, dx);
+                    const I off = ax.os[i] + oyz;
+#pragma unroll
+                    PP_CB {
+                      if (CB == 1 || cb < nc) {
+                        T v = ldg_acc(sp + (cb * a.src_sC + off));
+                        if (!valid) v = T(0);
+                        sx[cb] = fma(ax.w[i], v, sx[cb]);
+                        dx[cb] = fma(ax.g[i], v, dx[cb]);
+                      }
+                    }
                   }
-                  if (do_a) {
-                    const T pv = ax.w[i] * tyz;
-                    if (valid && pv != T(0)) atomic_acc(opc + (ax.oo[i] + ooyz), pv);
+                  if (do_a && valid) {
+                    const T wt = ax.w[i] * wyz;
+                    const I off = ax.oo[i] + ooyz;
+#pragma unroll
+                    PP_CB {
+                      if (CB == 1 || cb < nc) {
+                        const T pv = wt * t[cb];
+                        if (pv != T(0)) atomic_acc(opc + (cb * a.out_sC + off), pv);
+                      }
+                    }
                   }
                 }
               }
-              yw = fma(ay.w[j], sx, yw);
-              ygx = fma(ay.w[j], dx, ygx);
-              ygy = fma(ay.g[j], sx, ygy);
+#pragma unroll
+              PP_CB {
+                yw[cb] = fma(ay.w[j], sx[cb], yw[cb]);
+                ygx[cb] = fma(ay.w[j], dx[cb], ygx[cb]);
+                ygy[cb] = fma(ay.g[j], sx[cb], ygy[cb]);
+              }
             }
           }
-          gx = fma(az.w[k], ygx, gx);
-          gy = fma(az.w[k], ygy, gy);
-          gz = fma(az.g[k], yw, gz);
+#pragma unroll
+          PP_CB {
+            gx[cb] = fma(az.w[k], ygx[cb], gx[cb]);
+            gy[cb] = fma(az.w[k], ygy[cb], gy[cb]);
+            gz[cb] = fma(az.g[k], yw[cb], gz[cb]);
+          }
         }
       }
-      og0 = fma(t, gx, og0); og1 = fma(t, gy, og1); og2 = fma(t, gz, og2);
+#pragma unroll
+      PP_CB { og0 = fma(t[cb], gx[cb], og0); og1 = fma(t[cb], gy[cb], og1); og2 = fma(t[cb], gz[cb], og2); }
     }
     if (do_grad) {
       T* g = static_cast<T*>(a.gg) + gvox;
@@ -431,64 +502,96 @@ __global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
   if constexpr (MODE == K_KD) {
     // grid_grad backward: trgt = incoming gradient (N, C, *grid, D).
     T og0 = T(0), og1 = T(0), og2 = T(0);
-    for (int64_t c = 0; c < a.C; ++c) {
-      const S* sp = src_n + c * a.src_sC;
-      T* opc = do_a ? outs_n + c * a.out_sC : nullptr;
-      const S* tp = trg_v + c * a.trgt_sC;
-      const T t0 = ldg_acc(tp);
-      const T t1 = D > 1 ? ldg_acc(tp + a.trgt_sK) : T(0);
-      const T t2 = D > 2 ? ldg_acc(tp + 2 * a.trgt_sK) : T(0);
-      // Hessian accumulators of the interpolant of channel c.
-      T hxx = T(0), hxy = T(0), hxz = T(0), hyy = T(0), hyz = T(0), hzz = T(0);
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      const S* sp = src_n + c0 * a.src_sC;
+      T* opc = do_a ? outs_n + c0 * a.out_sC : nullptr;
+      T t0[CB], t1[CB], t2[CB];
+#pragma unroll
+      PP_CB {
+        const bool on = CB == 1 || cb < nc;
+        const S* tp = trg_v + (c0 + cb) * a.trgt_sC;
+        t0[cb] = on ? ldg_acc(tp) : T(0);
+        t1[cb] = (on && D > 1) ? ldg_acc(tp + a.trgt_sK) : T(0);
+        t2[cb] = (on && D > 2) ? ldg_acc(tp + 2 * a.trgt_sK) : T(0);
+      }
+      T hxx[CB], hxy[CB], hxz[CB], hyy[CB], hyz[CB], hzz[CB];
+#pragma unroll
+      PP_CB { hxx[cb] = hxy[cb] = hxz[cb] = hyy[cb] = hyz[cb] = hzz[cb] = T(0); }
 #pragma unroll (OuterUnroll<ORD, NZ>::value)
       for (int k = 0; k < NZ; ++k) {
         if (k < tz) {
-          T yw = T(0), ygx = T(0), ygy = T(0), yhx = T(0), ygxy = T(0), yhy = T(0);
+          T yw[CB], ygx[CB], ygy[CB], yhx[CB], ygxy[CB], yhy[CB];
+#pragma unroll
+          PP_CB { yw[cb] = ygx[cb] = ygy[cb] = yhx[cb] = ygxy[cb] = yhy[cb] = T(0); }
 #pragma unroll
           for (int j = 0; j < NY; ++j) {
             if (j < ty) {
               const I oyz = ay.os[j] + az.os[k];
               const I ooyz = ay.oo[j] + az.oo[k];
-              // push value of tap (i,j,k): gx_i*(wy wz t0) + wx_i*(gy wz t1 + wy gz t2)
-              const T pa = ay.w[j] * az.w[k] * t0;
-              const T pb = ay.g[j] * az.w[k] * t1 + ay.w[j] * az.g[k] * t2;
-              T sx = T(0), dx = T(0), hx = T(0);
+              T sx[CB], dx[CB], hx[CB];
+#pragma unroll
+              PP_CB { sx[cb] = dx[cb] = hx[cb] = T(0); }
 #pragma unroll
               for (int i = 0; i < NX; ++i) {
                 if (i < tx) {
                   const bool valid = PP_TAP_VALID(i, j, k);
                   if (do_grad) {
-                    T v = ldg_acc(sp + (ax.os[i] + oyz));
-                    if (!valid) v = T(0);
-                    sx = fma(ax.w[i], v, sx);
-                    dx = fma(ax.g[i], v, dx);
-                    hx = fma(ax.h[i], v, hx);
+                    const I off = ax.os[i] + oyz;
+#pragma unroll
+                    PP_CB {
+                      if (CB == 1 || cb < nc) {
+                        T v = ldg_acc(sp + (cb * a.src_sC + off));
+                        if (!valid) v = T(0);
+                        sx[cb] = fma(ax.w[i], v, sx[cb]);
+                        dx[cb] = fma(ax.g[i], v, dx[cb]);
+                        hx[cb] = fma(ax.h[i], v, hx[cb]);
+                      }
+                    }
                   }
-                  if (do_a) {
-                    const T pv = ax.g[i] * pa + ax.w[i] * pb;
-                    if (valid && pv != T(0)) atomic_acc(opc + (ax.oo[i] + ooyz), pv);
+                  if (do_a && valid) {
+                    const I off = ax.oo[i] + ooyz;
+#pragma unroll
+                    PP_CB {
+                      if (CB == 1 || cb < nc) {
+                        // push value: gx wy wz t0 + wx (gy wz t1 + wy gz t2)
+                        const T pa = ay.w[j] * az.w[k] * t0[cb];
+                        const T pb = ay.g[j] * az.w[k] * t1[cb] + ay.w[j] * az.g[k] * t2[cb];
+                        const T pv = ax.g[i] * pa + ax.w[i] * pb;
+                        if (pv != T(0)) atomic_acc(opc + (cb * a.out_sC + off), pv);
+                      }
+                    }
                   }
                 }
               }
-              yw = fma(ay.w[j], sx, yw);
-              ygx = fma(ay.w[j], dx, ygx);
-              ygy = fma(ay.g[j], sx, ygy);
-              yhx = fma(ay.w[j], hx, yhx);
-              ygxy = fma(ay.g[j], dx, ygxy);
-              yhy = fma(ay.h[j], sx, yhy);
+#pragma unroll
+              PP_CB {
+                yw[cb] = fma(ay.w[j], sx[cb], yw[cb]);
+                ygx[cb] = fma(ay.w[j], dx[cb], ygx[cb]);
+                ygy[cb] = fma(ay.g[j], sx[cb], ygy[cb]);
+                yhx[cb] = fma(ay.w[j], hx[cb], yhx[cb]);
+                ygxy[cb] = fma(ay.g[j], dx[cb], ygxy[cb]);
+                yhy[cb] = fma(ay.h[j], sx[cb], yhy[cb]);
+              }
             }
           }
-          hxx = fma(az.w[k], yhx, hxx);
-          hxy = fma(az.w[k], ygxy, hxy);
-          hyy = fma(az.w[k], yhy, hyy);
-          hxz = fma(az.g[k], ygx, hxz);
-          hyz = fma(az.g[k], ygy, hyz);
-          hzz = fma(az.h[k], yw, hzz);
+#pragma unroll
+          PP_CB {
+            hxx[cb] = fma(az.w[k], yhx[cb], hxx[cb]);
+            hxy[cb] = fma(az.w[k], ygxy[cb], hxy[cb]);
+            hyy[cb] = fma(az.w[k], yhy[cb], hyy[cb]);
+            hxz[cb] = fma(az.g[k], ygx[cb], hxz[cb]);
+            hyz[cb] = fma(az.g[k], ygy[cb], hyz[cb]);
+            hzz[cb] = fma(az.h[k], yw[cb], hzz[cb]);
+          }
         }
       }
-      og0 += hxx * t0 + hxy * t1 + hxz * t2;
-      og1 += hxy * t0 + hyy * t1 + hyz * t2;
-      og2 += hxz * t0 + hyz * t1 + hzz * t2;
+#pragma unroll
+      PP_CB {
+        og0 += hxx[cb] * t0[cb] + hxy[cb] * t1[cb] + hxz[cb] * t2[cb];
+        og1 += hxy[cb] * t0[cb] + hyy[cb] * t1[cb] + hyz[cb] * t2[cb];
+        og2 += hxz[cb] * t0[cb] + hyz[cb] * t1[cb] + hzz[cb] * t2[cb];
+      }
     }
     if (do_grad) {
       T* g = static_cast<T*>(a.gg) + gvox;
@@ -497,7 +600,41 @@ __global__ void __launch_bounds__(256) pp_kernel(const PPArgs a) {
       if (D > 2) g[2 * a.gg_sD] = og2;
     }
   }
+#undef PP_GRAD_GATHER
+#undef PP_CB
 #undef PP_TAP_VALID
+}
+
+template <int D, int ORD, int CB, class S, int MODE, class I>
+inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
+  if (a.nvox == 0) return cudaSuccess;
+  const int64_t inner = a.trgt_size[D - 1];
+  const int64_t mid = D > 1 ? a.trgt_size[D - 2] : 1;
+  const int64_t outer = a.N * (D == 3 ? a.trgt_size[0] : 1);
+  const int64_t gx = outer * ((inner + TILE_IN - 1) / TILE_IN);
+  const int64_t gy = (mid + TILE_MID - 1) / TILE_MID;
+  if (gx > 0x7fffffffLL || gy > 65535) return cudaErrorInvalidConfiguration;
+  dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(gy), 1);
+  dim3 block(TILE_IN, TILE_MID, 1);
+  pp_kernel<D, ORD, CB, S, MODE, I><<<grid, block, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Channel block: the whole channel set when C <= 4, else groups of 4.
+// Only the specialised orders up to cubic get CB > 1.
+template <int D, int ORD, class S, int MODE, class I>
+inline cudaError_t launch_cb(const PPArgs& a, cudaStream_t st) {
+  const int64_t C = MODE == K_COUNT ? 1 : a.C;
+  if constexpr (ORD >= 0 && ORD <= 3) {
+    switch (C >= 4 ? 4 : static_cast<int>(C)) {
+      case 2: return launch_one<D, ORD, 2, S, MODE, I>(a, st);
+      case 3: return launch_one<D, ORD, 3, S, MODE, I>(a, st);
+      case 4: return launch_one<D, ORD, 4, S, MODE, I>(a, st);
+      default: return launch_one<D, ORD, 1, S, MODE, I>(a, st);
+    }
+  } else {
+    return launch_one<D, ORD, 1, S, MODE, I>(a, st);
+  }
 }
 
 // Orders that get a compile-time specialisation for a storage type; every
@@ -507,27 +644,18 @@ template <class S> struct Specialised { static constexpr unsigned mask = 0; };
 template <> struct Specialised<float> { static constexpr unsigned mask = 0xFFu; };
 template <> struct Specialised<__nv_bfloat16> { static constexpr unsigned mask = (1u << 1) | (1u << 3); };
 
-template <int D, int ORD, class S, int MODE, class I>
-inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
-  const int threads = 256;
-  const int64_t blocks = (a.nvox + threads - 1) / threads;
-  if (blocks == 0) return cudaSuccess;
-  pp_kernel<D, ORD, S, MODE, I><<<static_cast<unsigned>(blocks), threads, 0, st>>>(a);
-  return cudaGetLastError();
-}
-
 template <int D, class S, int MODE>
 inline cudaError_t launch_ord(int ord, bool wide, const PPArgs& a, cudaStream_t st) {
   constexpr unsigned m = (D == 1) ? 0u : Specialised<S>::mask;
   if (!wide && ord >= 0) {
     switch (ord) {
-#define PP_CASE(O) case O: if constexpr ((m >> O) & 1u) return launch_one<D, O, S, MODE, int32_t>(a, st); break;
+#define PP_CASE(O) case O: if constexpr ((m >> O) & 1u) return launch_cb<D, O, S, MODE, int32_t>(a, st); break;
       PP_CASE(0) PP_CASE(1) PP_CASE(2) PP_CASE(3) PP_CASE(4) PP_CASE(5) PP_CASE(6) PP_CASE(7)
 #undef PP_CASE
       default: break;
     }
   }
-  return launch_one<D, -1, S, MODE, int64_t>(a, st);
+  return launch_one<D, -1, 1, S, MODE, int64_t>(a, st);
 }
 
 }  // namespace ppk
