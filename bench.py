@@ -169,6 +169,9 @@ def make_inputs(size, channels, device):
 
 def step(x, grid, w):
     import nitorch_b200 as nb
+    from nitorch_b200 import spatial
+    # a step sees a new grid in practice: recompute the (cached) sample order
+    spatial._orders.clear()
     x.grad = None
     grid.grad = None
     y = nb.grid_pull(x, grid, ORDER, BOUND, EXTRAP, prefilter=True)

@@ -87,6 +87,12 @@ typedef struct pp_options {
   int32_t extrapolate;           /* bit 0: sample outside the field of view;
                                     bit 1: half-voxel tolerance             */
   int32_t flags;                 /* PP_DETERMINISTIC                        */
+  const int32_t* sample_order;   /* optional device array: the order in which
+                                    the grid's N*prod(grid spatial) sampling
+                                    points are processed (a permutation, e.g.
+                                    from pp_sample_order); NULL = natural.
+                                    Results do not depend on it beyond
+                                    floating-point summation order.        */
 } pp_options;
 
 /* Version of this ABI (major * 100 + minor). */
@@ -145,6 +151,16 @@ PP_API int pp_grid_grad_backward(const pp_tensor* grad, const pp_tensor* input,
                           const pp_tensor* grid, const pp_tensor* grad_input,
                           const pp_tensor* grad_grid, const pp_options* opt,
                           void* stream, void* workspace, size_t workspace_bytes);
+
+/* Source-sorted processing order of a grid's sampling points (no
+ * counterpart in the reference; a scheduling aid for rough deformations):
+ * writes to `perm` (int32, N*prod(grid spatial) entries) the sample indices
+ * sorted by the source voxel floor(coordinate) they fall in, for a source
+ * of spatial size `src_size` (D entries).  Needs
+ * pp_sample_order_workspace_bytes() bytes of device workspace. */
+PP_API size_t pp_sample_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size);
+PP_API int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
+                           void* workspace, size_t workspace_bytes, void* stream);
 
 /* interpol.coeff.spline_coeff (vendored: _ts/coeff.py:285-310):
  * interpolating B-spline coefficients along one axis of `input`, written to

@@ -51,6 +51,7 @@ class PPOptions(ctypes.Structure):
         ("order", ctypes.c_int32 * 3),
         ("extrapolate", ctypes.c_int32),
         ("flags", ctypes.c_int32),
+        ("sample_order", ctypes.c_void_p),
     ]
 
 
@@ -59,7 +60,7 @@ EXPORTS = (
     "pp_grid_pull", "pp_grid_pull_backward", "pp_grid_push",
     "pp_grid_push_backward", "pp_grid_count", "pp_grid_count_backward",
     "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
-    "pp_spline_coeff_nd",
+    "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
 )
 
 _lib = None
@@ -86,8 +87,13 @@ def _declare(L):
     L.pp_spline_coeff_nd.argtypes = [T, T, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                      ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                      ctypes.c_int32, vp]
+    I64P = ctypes.POINTER(ctypes.c_int64)
+    L.pp_sample_order_workspace_bytes.argtypes = [T, I64P]
+    L.pp_sample_order_workspace_bytes.restype = sz
+    L.pp_sample_order.argtypes = [T, I64P, vp, vp, sz, vp]
     for name in EXPORTS:
-        if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches"):
+        if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches",
+                        "pp_sample_order_workspace_bytes"):
             getattr(L, name).restype = ctypes.c_int
     return L
 
@@ -140,8 +146,9 @@ def ref(d):
     return None if d is None else ctypes.byref(d)
 
 
-def options(bound, order, extrapolate, flags=0):
+def options(bound, order, extrapolate, flags=0, sample_order=None):
     o = PPOptions()
+    o.sample_order = sample_order
     b = [int(x) for x in bound][:3]
     i = [int(x) for x in order][:3]
     o.nbound = len(b)

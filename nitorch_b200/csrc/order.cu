@@ -1,0 +1,234 @@
+// Source-sorted processing order of the sampling points.
+//
+// With a rough deformation, the 32 lanes of a warp (consecutive grid voxels)
+// sample source points scattered over a wide neighbourhood: every gather and
+// every scatter instruction touches ~30 distinct 32-byte sectors.  Processing
+// the sampling points in the order of their source voxel makes consecutive
+// lanes sample neighbouring source voxels again, so taps coalesce and
+// scatter atomics hit a few lines per instruction.
+//
+// pp_sample_order computes that order -- a permutation of the grid's sample
+// indices sorted by the linear index of the source voxel floor(coords)
+// (clamped into the source volume, batch-major) -- with a counting sort:
+//   1. key / rank: key = source voxel, rank = atomicAdd(&count[key], 1);
+//   2. exclusive scan of count (block reduce, scan of block sums, apply);
+//   3. perm[offset[key] + rank] = sample.
+// The permutation only depends on the grid, so the forward and backward
+// kernels of a step share one.  Order within a source voxel is arbitrary.
+#include "pp_capi_internal.cuh"
+#include "pp_kernels.cuh"
+
+namespace {
+
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+struct KeyArgs {
+  const void* grid;
+  int64_t N;
+  int64_t size[3];       // grid spatial sizes
+  int64_t src[3];        // source spatial sizes
+  int64_t gsN, gs[3], gsD;
+  int D;
+  int64_t nvox;
+  int64_t nsrc;          // prod(src)
+};
+
+template <class T>
+__global__ void order_keys(KeyArgs a, int32_t* count, int32_t* keys, int32_t* ranks) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= a.nvox) return;
+  int64_t v = s, sub[3] = {0, 0, 0};
+  for (int d = a.D - 1; d >= 0; --d) { sub[d] = v % a.size[d]; v /= a.size[d]; }
+  const int64_t n = v;
+  const T* g = static_cast<const T*>(a.grid) + n * a.gsN;
+  for (int d = 0; d < a.D; ++d) g += sub[d] * a.gs[d];
+  int64_t lin = 0;
+  for (int d = 0; d < a.D; ++d) {
+    T c = g[d * a.gsD];
+    // floor, clamped into the volume (NaN -> 0)
+    int64_t i = (c >= T(0)) ? static_cast<int64_t>(fmin(c, static_cast<T>(a.src[d] - 1))) : 0;
+    lin = lin * a.src[d] + i;
+  }
+  const int32_t key = static_cast<int32_t>(n * a.nsrc + lin);
+  keys[s] = key;
+  ranks[s] = atomicAdd(count + key, 1);
+}
+
+__device__ __forceinline__ int32_t block_exclusive_scan(int32_t x, int32_t& total) {
+  __shared__ int32_t warp_sums[SCAN_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int32_t inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) warp_sums[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    int32_t ws = lane < SCAN_THREADS / 32 ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += y;
+    }
+    if (lane < SCAN_THREADS / 32) warp_sums[lane] = ws;
+  }
+  __syncthreads();
+  const int32_t before = wid > 0 ? warp_sums[wid - 1] : 0;
+  total = warp_sums[SCAN_THREADS / 32 - 1];
+  __syncthreads();
+  return before + inc - x;
+}
+
+// 2a. per-tile sums
+__global__ void __launch_bounds__(SCAN_THREADS) scan_reduce(const int32_t* in, int64_t n, int32_t* partial) {
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * SCAN_TILE;
+  int32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    const int64_t i = base + static_cast<int64_t>(k) * SCAN_THREADS + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  int32_t total;
+  block_exclusive_scan(s, total);
+  if (threadIdx.x == 0) partial[blockIdx.x] = total;
+}
+
+// 2b. exclusive scan of the tile sums, one CTA (sequential chunks of SCAN_THREADS)
+__global__ void __launch_bounds__(SCAN_THREADS) scan_partials(int32_t* partial, int64_t np) {
+  int32_t carry = 0;
+  for (int64_t base = 0; base < np; base += SCAN_THREADS) {
+    const int64_t i = base + threadIdx.x;
+    const int32_t x = i < np ? partial[i] : 0;
+    int32_t total;
+    const int32_t ex = block_exclusive_scan(x, total);
+    if (i < np) partial[i] = carry + ex;
+    carry += total;
+  }
+}
+
+// 2c. exclusive scan inside each tile, plus the tile's offset (in place)
+__global__ void __launch_bounds__(SCAN_THREADS) scan_apply(int32_t* data, int64_t n, const int32_t* partial) {
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * SCAN_TILE + static_cast<int64_t>(threadIdx.x) * SCAN_ITEMS;
+  int32_t v[SCAN_ITEMS];
+  int32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    v[k] = (base + k < n) ? data[base + k] : 0;
+    s += v[k];
+  }
+  int32_t total;
+  int32_t run = block_exclusive_scan(s, total) + partial[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    if (base + k < n) data[base + k] = run;
+    run += v[k];
+  }
+}
+
+__global__ void order_scatter(const int32_t* keys, const int32_t* ranks, const int32_t* offset,
+                              int64_t nvox, int32_t* perm) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= nvox) return;
+  perm[offset[keys[s]] + ranks[s]] = static_cast<int32_t>(s);
+}
+
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+struct Layout {
+  size_t count, keys, ranks, partial, total;
+};
+
+Layout layout(int64_t nvox, int64_t nsrc_total) {
+  Layout L;
+  const int64_t ntile = (nsrc_total + SCAN_TILE - 1) / SCAN_TILE;
+  L.count = 0;
+  L.keys = L.count + align256(static_cast<size_t>(nsrc_total) * 4);
+  L.ranks = L.keys + align256(static_cast<size_t>(nvox) * 4);
+  L.partial = L.ranks + align256(static_cast<size_t>(nvox) * 4);
+  L.total = L.partial + align256(static_cast<size_t>(ntile > 0 ? ntile : 1) * 4);
+  return L;
+}
+
+int sizes_of(const pp_tensor* grid, const int64_t* src_size, int& D, int64_t& nvox, int64_t& nsrc) {
+  int rc = ppc::check_tensor(grid, "grid");
+  if (rc) return rc;
+  if (grid->ndim < 3 || grid->ndim > 5)
+    return ppc::fail(PP_ERR_ARG, "(): expected 3D, 4D or 5D grid but got input with %d dimensions", grid->ndim);
+  D = grid->ndim - 2;
+  if (grid->sizes[grid->ndim - 1] != D)
+    return ppc::fail(PP_ERR_ARG, "(): expected grid to have size %d in last dimension", D);
+  if (grid->dtype != PP_FLOAT32 && grid->dtype != PP_FLOAT64)
+    return ppc::fail(PP_ERR_DTYPE, "(): expected grid to be float32 or float64");
+  if (!src_size) return ppc::fail(PP_ERR_ARG, "(): expected source sizes");
+  nvox = grid->sizes[0];
+  nsrc = 1;
+  for (int d = 0; d < D; ++d) {
+    if (src_size[d] <= 0 || grid->sizes[1 + d] <= 0) return ppc::fail(PP_ERR_ARG, "(): expected non-empty sizes");
+    nvox *= grid->sizes[1 + d];
+    nsrc *= src_size[d];
+  }
+  if (nvox >= (int64_t(1) << 31) || nsrc * grid->sizes[0] >= (int64_t(1) << 31))
+    return ppc::fail(PP_ERR_UNSUPPORTED, "(): sample ordering needs fewer than 2^31 samples and source voxels");
+  return PP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t pp_sample_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size) {
+  int D;
+  int64_t nvox, nsrc;
+  if (sizes_of(grid, src_size, D, nvox, nsrc)) return 0;
+  return layout(nvox, nsrc * grid->sizes[0]).total;
+}
+
+int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
+                    void* workspace, size_t workspace_bytes, void* stream) {
+  int D;
+  int64_t nvox, nsrc;
+  int rc = sizes_of(grid, src_size, D, nvox, nsrc);
+  if (rc) return rc;
+  if (!perm) return ppc::fail(PP_ERR_ARG, "(): expected an output permutation");
+  const int64_t nsrc_total = nsrc * grid->sizes[0];
+  const Layout L = layout(nvox, nsrc_total);
+  if (!workspace || workspace_bytes < L.total)
+    return ppc::fail(PP_ERR_WORKSPACE, "(): sample ordering needs %zu bytes of workspace", L.total);
+  if (nvox == 0) return PP_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  int32_t* count = reinterpret_cast<int32_t*>(ws + L.count);
+  int32_t* keys = reinterpret_cast<int32_t*>(ws + L.keys);
+  int32_t* ranks = reinterpret_cast<int32_t*>(ws + L.ranks);
+  int32_t* partial = reinterpret_cast<int32_t*>(ws + L.partial);
+  if ((rc = ppc::cuda_check(cudaMemsetAsync(count, 0, static_cast<size_t>(nsrc_total) * 4, st), "order clear"))) return rc;
+  KeyArgs a;
+  a.grid = grid->data;
+  a.N = grid->sizes[0];
+  a.D = D;
+  a.gsN = grid->strides[0];
+  a.gsD = grid->strides[1 + D];
+  for (int d = 0; d < 3; ++d) {
+    a.size[d] = d < D ? grid->sizes[1 + d] : 1;
+    a.src[d] = d < D ? src_size[d] : 1;
+    a.gs[d] = d < D ? grid->strides[1 + d] : 0;
+  }
+  a.nvox = nvox;
+  a.nsrc = nsrc;
+  const unsigned nb = static_cast<unsigned>((nvox + 255) / 256);
+  if (grid->dtype == PP_FLOAT32) order_keys<float><<<nb, 256, 0, st>>>(a, count, keys, ranks);
+  else order_keys<double><<<nb, 256, 0, st>>>(a, count, keys, ranks);
+  const int64_t ntile = (nsrc_total + SCAN_TILE - 1) / SCAN_TILE;
+  scan_reduce<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, nsrc_total, partial);
+  scan_partials<<<1, SCAN_THREADS, 0, st>>>(partial, ntile);
+  scan_apply<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, nsrc_total, partial);
+  order_scatter<<<nb, 256, 0, st>>>(keys, ranks, count, nvox, perm);
+  ppc::count_launch(5);
+  return ppc::cuda_check(cudaGetLastError(), "sample order launch");
+}
+
+}  // extern "C"

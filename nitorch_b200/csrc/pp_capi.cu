@@ -236,6 +236,7 @@ int prepare(Call& k, const pp_tensor* grid, const pp_options* opt) {
   if (rc) return rc;
   for (int a = 0; a < 3; ++a) { k.a.bound[a] = k.bound[a]; k.a.order[a] = k.order[a]; }
   k.a.extrapolate = opt->extrapolate;
+  k.a.perm = opt->sample_order;
   k.a.grid = grid->data;
   set_grid(grid, k.D, k.a.grid_sN, k.a.grid_s, k.a.grid_sD);
   k.a.N = grid->sizes[0];

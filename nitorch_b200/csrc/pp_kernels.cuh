@@ -47,6 +47,7 @@ struct PPArgs {
   int extrapolate;
   int flags;
   int64_t nvox;
+  const int32_t* perm;  // optional processing order of the sampling points
 };
 
 template <int ORD> struct Taps { static constexpr int value = ORD < 0 ? 8 : (ORD == 0 ? 1 : ORD + 1); };
@@ -122,24 +123,36 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
   constexpr bool GATHER = MODE == K_PULL || MODE == K_SGRAD || MODE == K_PULLGRAD || MODE == K_PUSHGRAD || MODE == K_KD;
   constexpr bool SCATTER = MODE == K_PUSH || MODE == K_COUNT || MODE == K_PUSHGRAD || MODE == K_KD;
 
-  // ---- sampling point (n, x, y, z) from the 2-D tile mapping -----------
-  const I inner = static_cast<I>(a.trgt_size[D - 1]);
-  const I mid = D > 1 ? static_cast<I>(a.trgt_size[D - 2]) : I(1);
-  const I ntile = (inner + TILE_IN - 1) / TILE_IN;
-  const I outer_idx = static_cast<I>(blockIdx.x) / ntile;
-  const I ii = (static_cast<I>(blockIdx.x) - outer_idx * ntile) * TILE_IN + static_cast<I>(threadIdx.x);
-  const I mm = static_cast<I>(blockIdx.y) * TILE_MID + static_cast<I>(threadIdx.y);
-  if (ii >= inner || mm >= mid) return;
+  // ---- sampling point (n, x, y, z) -------------------------------------
   I sub[3] = {0, 0, 0};
   I n;
-  if (D == 3) {
-    sub[2] = ii; sub[1] = mm;
-    sub[0] = outer_idx % static_cast<I>(a.trgt_size[0]);
-    n = outer_idx / static_cast<I>(a.trgt_size[0]);
-  } else if (D == 2) {
-    sub[1] = ii; sub[0] = mm; n = outer_idx;
+  if (a.perm != nullptr) {
+    // explicit processing order (source-sorted): linear thread index
+    const int64_t t = (static_cast<int64_t>(blockIdx.x) * TILE_MID + threadIdx.y) * TILE_IN + threadIdx.x;
+    if (t >= a.nvox) return;
+    I v = static_cast<I>(__ldg(a.perm + t));
+    if (D > 2) { sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]); }
+    if (D > 1) { sub[1] = v % static_cast<I>(a.trgt_size[1]); v /= static_cast<I>(a.trgt_size[1]); }
+    sub[0] = v % static_cast<I>(a.trgt_size[0]);
+    n = v / static_cast<I>(a.trgt_size[0]);
   } else {
-    sub[0] = ii; n = outer_idx;
+    // 2-D tile mapping over the grid
+    const I inner = static_cast<I>(a.trgt_size[D - 1]);
+    const I mid = D > 1 ? static_cast<I>(a.trgt_size[D - 2]) : I(1);
+    const I ntile = (inner + TILE_IN - 1) / TILE_IN;
+    const I outer_idx = static_cast<I>(blockIdx.x) / ntile;
+    const I ii = (static_cast<I>(blockIdx.x) - outer_idx * ntile) * TILE_IN + static_cast<I>(threadIdx.x);
+    const I mm = static_cast<I>(blockIdx.y) * TILE_MID + static_cast<I>(threadIdx.y);
+    if (ii >= inner || mm >= mid) return;
+    if (D == 3) {
+      sub[2] = ii; sub[1] = mm;
+      sub[0] = outer_idx % static_cast<I>(a.trgt_size[0]);
+      n = outer_idx / static_cast<I>(a.trgt_size[0]);
+    } else if (D == 2) {
+      sub[1] = ii; sub[0] = mm; n = outer_idx;
+    } else {
+      sub[0] = ii; n = outer_idx;
+    }
   }
 
   // ---- coordinates ------------------------------------------------------
@@ -611,8 +624,8 @@ inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
   const int64_t inner = a.trgt_size[D - 1];
   const int64_t mid = D > 1 ? a.trgt_size[D - 2] : 1;
   const int64_t outer = a.N * (D == 3 ? a.trgt_size[0] : 1);
-  const int64_t gx = outer * ((inner + TILE_IN - 1) / TILE_IN);
-  const int64_t gy = (mid + TILE_MID - 1) / TILE_MID;
+  const int64_t gx = a.perm ? (a.nvox + PP_THREADS - 1) / PP_THREADS : outer * ((inner + TILE_IN - 1) / TILE_IN);
+  const int64_t gy = a.perm ? 1 : (mid + TILE_MID - 1) / TILE_MID;
   if (gx > 0x7fffffffLL || gy > 65535) return cudaErrorInvalidConfiguration;
   dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(gy), 1);
   dim3 block(TILE_IN, TILE_MID, 1);

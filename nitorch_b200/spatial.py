@@ -28,6 +28,7 @@ Argument errors raise ``RuntimeError`` with the reference's "(): expected
 """
 import ctypes
 import os
+import weakref
 
 import torch
 
@@ -36,10 +37,92 @@ from .enums import BoundType, InterpolationType
 
 __all__ = ["grid_pull", "grid_pull_backward", "grid_push", "grid_push_backward",
            "grid_count", "grid_count_backward", "grid_grad", "grid_grad_backward",
-           "BoundType", "InterpolationType", "set_deterministic", "get_deterministic"]
+           "BoundType", "InterpolationType", "set_deterministic", "get_deterministic",
+           "set_sample_order", "sample_order"]
 
 _FLOATS = (torch.float32, torch.float64, torch.bfloat16, torch.float16)
 _deterministic = bool(int(os.environ.get("PP_DETERMINISTIC", "0") or "0"))
+_sample_order_mode = os.environ.get("PP_SAMPLE_ORDER", "auto")
+_SORT_MIN_SAMPLES = 1 << 18
+
+
+def set_sample_order(mode="auto"):
+    """Processing order of the sampling points: "natural" (grid order),
+    "sorted" (source-sorted, see pp_sample_order) or "auto" (sorted for
+    grids of at least 2^18 points).  Only the speed depends on it."""
+    global _sample_order_mode
+    if mode not in ("auto", "natural", "sorted"):
+        raise ValueError(f"unknown sample order mode {mode}")
+    _sample_order_mode = mode
+
+
+class _OrderCache:
+    """Sample orders of recently used grids.  An entry is valid while the
+    grid tensor it was computed for is alive and unmodified (same storage
+    pointer, version counter, sizes and strides) -- the forward and backward
+    passes of a step then share one sort."""
+
+    def __init__(self, size=4):
+        self.size = size
+        self.entries = []
+
+    @staticmethod
+    def _key(grid, src):
+        return (grid.data_ptr(), grid._version, tuple(grid.shape), tuple(grid.stride()),
+                tuple(src), grid.device)
+
+    def get(self, grid, src):
+        key = self._key(grid, src)
+        for i, (ref, k, perm) in enumerate(self.entries):
+            if ref() is not None and k == key:
+                if i:
+                    self.entries.insert(0, self.entries.pop(i))
+                return perm
+        return None
+
+    def put(self, grid, src, perm):
+        self.entries = [e for e in self.entries if e[0]() is not None][: self.size - 1]
+        self.entries.insert(0, (weakref.ref(grid), self._key(grid, src), perm))
+
+    def clear(self):
+        self.entries = []
+
+
+_orders = _OrderCache()
+
+
+def sample_order(grid, src_size):
+    """Source-sorted processing order of `grid`'s sampling points (int32
+    permutation) for a source of spatial size `src_size`."""
+    L = _lib.load()
+    src = (ctypes.c_int64 * len(src_size))(*[int(v) for v in src_size])
+    d = _lib.desc(grid)
+    nbytes = L.pp_sample_order_workspace_bytes(ctypes.byref(d), src)
+    if nbytes == 0:
+        raise RuntimeError(L.pp_last_error().decode(errors="replace"))
+    nvox = grid.numel() // grid.shape[-1]
+    perm = torch.empty(nvox, dtype=torch.int32, device=grid.device)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=grid.device)
+    with _On(grid):
+        _lib.check(L.pp_sample_order(ctypes.byref(d), src, ctypes.c_void_p(perm.data_ptr()),
+                                     ctypes.c_void_p(ws.data_ptr()), nbytes, _lib.stream_of(grid)))
+    return perm
+
+
+def _order_for(grid, src_size):
+    mode = _sample_order_mode
+    if mode == "natural":
+        return None
+    nvox = grid.numel() // grid.shape[-1]
+    if mode == "auto" and nvox < _SORT_MIN_SAMPLES:
+        return None
+    if nvox >= (1 << 31):
+        return None
+    perm = _orders.get(grid, src_size)
+    if perm is None:
+        perm = sample_order(grid, src_size)
+        _orders.put(grid, src_size, perm)
+    return perm
 
 
 def set_deterministic(flag=True):
@@ -130,10 +213,14 @@ def _grid32(grid):
     return grid
 
 
-def _opts(bound, interpolation, extrapolate):
+def _opts(bound, interpolation, extrapolate, grid=None, src_size=None):
     _check_opts(bound, interpolation)
-    return _lib.options([int(b) for b in bound], [int(i) for i in interpolation],
-                        int(extrapolate), _lib.PP_DETERMINISTIC if _deterministic else 0)
+    perm = _order_for(grid, src_size) if grid is not None and grid.is_cuda else None
+    o = _lib.options([int(b) for b in bound], [int(i) for i in interpolation],
+                     int(extrapolate), _lib.PP_DETERMINISTIC if _deterministic else 0,
+                     None if perm is None else perm.data_ptr())
+    o._keep = perm       # keep the permutation alive for the call
+    return o
 
 
 class _On:
@@ -174,10 +261,11 @@ def _wsptr(ws):
 
 def grid_pull(input, grid, bound, interpolation, extrapolate):
     _check_pair(input, grid)
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(input)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, input.shape[2:])
     out = torch.empty((grid.shape[0], input.shape[1], *grid.shape[1:-1]),
                       dtype=input.dtype, device=input.device)
     with _On(input):
@@ -189,10 +277,11 @@ def grid_pull(input, grid, bound, interpolation, extrapolate):
 
 def grid_pull_backward(grad, input, grid, bound, interpolation, extrapolate):
     _check_pair(input, grid)
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(input)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, input.shape[2:])
     gi = torch.empty_like(input, memory_format=torch.contiguous_format) if input.requires_grad else None
     gg = torch.empty(g.shape, dtype=g.dtype, device=g.device) if grid.requires_grad else None
     ws, nws = _workspace(gi) if gi is not None else (None, 0)
@@ -229,11 +318,12 @@ def grid_push(input, grid, shape, bound, interpolation, extrapolate):
         _fail(f"expected input and grid to have same batch, width, height and (optionally) depth "
               f"sizes, but got input with sizes{list(input.shape)} and grid with sizes "
               f"{list(grid.shape)}")
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(input)
     shape = _push_shape(shape, input.shape[2:], dim)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, shape)
     out = torch.empty((grid.shape[0], input.shape[1], *shape), dtype=input.dtype, device=input.device)
     ws, nws = _workspace(out)
     with _On(input):
@@ -245,10 +335,11 @@ def grid_push(input, grid, shape, bound, interpolation, extrapolate):
 
 def grid_push_backward(grad, input, grid, bound, interpolation, extrapolate):
     _check_pair(input, grid)
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(input)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, grad.shape[2:])
     gi = torch.empty_like(input, memory_format=torch.contiguous_format) if input.requires_grad else None
     gg = torch.empty(g.shape, dtype=g.dtype, device=g.device) if grid.requires_grad else None
     with _On(input):
@@ -270,12 +361,13 @@ def grid_push_backward(grad, input, grid, bound, interpolation, extrapolate):
 
 def grid_count(grid, shape, bound, interpolation, extrapolate):
     _check_grid(grid)
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(grid)
     dim = grid.dim() - 2
     shape = _push_shape(shape, grid.shape[1:-1], dim)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, shape)
     out = torch.empty((grid.shape[0], 1, *shape), dtype=g.dtype, device=grid.device)
     ws, nws = _workspace(out)
     with _On(grid):
@@ -286,10 +378,11 @@ def grid_count(grid, shape, bound, interpolation, extrapolate):
 
 def grid_count_backward(grad, grid, bound, interpolation, extrapolate):
     _check_grid(grid)
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(grid)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, grad.shape[2:])
     gg = torch.empty(g.shape, dtype=g.dtype, device=g.device)
     gr = grad.to(g.dtype)
     with _On(grid):
@@ -305,10 +398,11 @@ def grid_count_backward(grad, grid, bound, interpolation, extrapolate):
 
 def grid_grad(input, grid, bound, interpolation, extrapolate):
     _check_pair(input, grid)
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(input)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, input.shape[2:])
     dim = grid.dim() - 2
     out = torch.empty((grid.shape[0], input.shape[1], *grid.shape[1:-1], dim),
                       dtype=input.dtype, device=input.device)
@@ -321,10 +415,11 @@ def grid_grad(input, grid, bound, interpolation, extrapolate):
 
 def grid_grad_backward(grad, input, grid, bound, interpolation, extrapolate):
     _check_pair(input, grid)
-    opt = _opts(bound, interpolation, extrapolate)
+    _check_opts(bound, interpolation)
     _require_cuda(input)
     L = _lib.load()
     g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, input.shape[2:])
     gi = torch.empty_like(input, memory_format=torch.contiguous_format) if input.requires_grad else None
     gg = torch.empty(g.shape, dtype=g.dtype, device=g.device) if grid.requires_grad else None
     ws, nws = _workspace(gi) if gi is not None else (None, 0)

@@ -148,3 +148,39 @@ def test_config1_checksums_and_adjoint():
         a = (p * Y.double()).sum().item()
         c = (X.double() * q).sum().item()
         assert abs(a - c) <= (1e-12 if dtype == torch.float64 else 1e-6) * abs(a)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("order", [0, 1, 3, 5])
+def test_sorted_sample_order_matches_natural(dim, order):
+    """Processing the sampling points in source-sorted order changes only the
+    floating-point summation order."""
+    from nitorch_b200 import spatial
+    vol, grid = make_case(dim, seed=40 + order, in_size=9, out_size=8, C=3, N=2, spread=2.0)
+    g = np.random.default_rng(1)
+    tgt = g.standard_normal((2, 3) + grid.shape[1:-1])
+    gpush = g.standard_normal(vol.shape)
+    gcount = g.standard_normal((2, 1) + vol.shape[2:])
+    ggrad = g.standard_normal((2, 3) + grid.shape[1:-1] + (dim,))
+    args = (vol, grid, tgt, gpush, gcount, ggrad, 2, order)
+    try:
+        spatial.set_sample_order("natural")
+        nat = all_ops(*args, ex=1, dtype=torch.float64)
+        spatial.set_sample_order("sorted")
+        srt = all_ops(*args, ex=1, dtype=torch.float64)
+        perm = spatial.sample_order(cu(grid, torch.float64), vol.shape[2:]).cpu().numpy()
+    finally:
+        spatial.set_sample_order("auto")
+    assert np.array_equal(np.sort(perm), np.arange(perm.size))
+    for name in KEYS:
+        assert relerr(srt[name], nat[name]) < 1e-12, name
+
+
+def test_sample_order_sorted_by_source_voxel():
+    from nitorch_b200 import spatial
+    vol, grid = make_case(3, seed=3, in_size=12, out_size=10, C=1, N=1, spread=3.0)
+    G = cu(grid, torch.float32)
+    perm = spatial.sample_order(G, vol.shape[2:]).cpu().numpy()
+    c = np.clip(np.floor(grid.reshape(-1, 3).astype(np.float32)), 0, 11).astype(np.int64)
+    key = (c[:, 0] * 12 + c[:, 1]) * 12 + c[:, 2]
+    assert np.all(np.diff(key[perm]) >= 0)
