@@ -162,6 +162,19 @@ PP_API size_t pp_sample_order_workspace_bytes(const pp_tensor* grid, const int64
 PP_API int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* pp_sample_order without any device allocation or caller workspace (no
+ * counterpart in the reference).  For callers that cannot allocate device
+ * memory when they need an order -- inside a CUDA graph capture, or from a
+ * host runtime that owns all device memory up front.  Uses a fixed 16 MiB
+ * scratch array compiled into the library (held on every device that loads
+ * it): 4 bytes per source voxel (times the batch) plus 8 bytes per sampling
+ * point must fit, else PP_ERR_WORKSPACE.  The first call on a device looks
+ * up the scratch address for that device; make that first call before any
+ * stream capture.  All calls share the scratch: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+PP_API int pp_sample_order_noalloc(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
+                                   void* stream);
+
 /* interpol.coeff.spline_coeff (vendored: _ts/coeff.py:285-310):
  * interpolating B-spline coefficients along one axis of `input`, written to
  * `out` (same sizes; may alias `input` for in-place).  `bound` uses the

@@ -61,6 +61,7 @@ EXPORTS = (
     "pp_grid_push_backward", "pp_grid_count", "pp_grid_count_backward",
     "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
     "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
+    "pp_sample_order_noalloc",
 )
 
 _lib = None
@@ -91,6 +92,7 @@ def _declare(L):
     L.pp_sample_order_workspace_bytes.argtypes = [T, I64P]
     L.pp_sample_order_workspace_bytes.restype = sz
     L.pp_sample_order.argtypes = [T, I64P, vp, vp, sz, vp]
+    L.pp_sample_order_noalloc.argtypes = [T, I64P, vp, vp]
     for name in EXPORTS:
         if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches",
                         "pp_sample_order_workspace_bytes"):

@@ -15,6 +15,8 @@
 //   3. perm[offset[key] + rank] = sample.
 // The permutation only depends on the grid, so the forward and backward
 // kernels of a step share one.  Order within a source voxel is arbitrary.
+#include <mutex>
+
 #include "pp_capi_internal.cuh"
 #include "pp_kernels.cuh"
 
@@ -229,6 +231,110 @@ int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* per
   order_scatter<<<nb, 256, 0, st>>>(keys, ranks, count, nvox, perm);
   ppc::count_launch(5);
   return ppc::cuda_check(cudaGetLastError(), "sample order launch");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Sample ordering without any device allocation.
+//
+// Some callers cannot allocate device memory at the moment they need an
+// order: code running while a stream is being captured into a CUDA graph
+// (cudaMalloc is not allowed there), and hosts that drive this library
+// through its C ABI from a runtime that owns all device memory up front or
+// works under a fixed memory budget (plugins of another framework, real-time
+// pipelines).  For them, pp_sample_order_noalloc uses a scratch area that is
+// part of the library image instead of a caller-provided workspace.
+//
+// The scratch is a file-scope device array of NOALLOC_SCRATCH_BYTES (16 MiB);
+// every GPU that loads the library holds it until the process exits.  It
+// covers grids whose counting-sort state fits in it: 4 bytes per source voxel
+// (times the batch) plus 8 bytes per sampling point, e.g. up to ~1.3 M
+// sampling points into a ~1.3 M-voxel source.  Larger requests are rejected
+// with PP_ERR_WORKSPACE.  All calls share the one array: calls whose work
+// overlaps on the GPU (different streams, or several host threads) race and
+// must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(16) << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current (host code cannot use the symbol itself).
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+std::mutex g_noalloc_mutex;
+
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return ppc::cuda_check(e, "noalloc: current device");
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return ppc::fail(PP_ERR_UNSUPPORTED, "(): device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return ppc::cuda_check(e, "noalloc: scratch address");
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return PP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pp_sample_order_noalloc(const pp_tensor* grid, const int64_t* src_size, int32_t* perm, void* stream) {
+  int D;
+  int64_t nvox, nsrc;
+  int rc = sizes_of(grid, src_size, D, nvox, nsrc);
+  if (rc) return rc;
+  if (!perm) return ppc::fail(PP_ERR_ARG, "(): expected an output permutation");
+  const int64_t nsrc_total = nsrc * grid->sizes[0];
+  const Layout L = layout(nvox, nsrc_total);
+  if (L.total > NOALLOC_SCRATCH_BYTES)
+    return ppc::fail(PP_ERR_WORKSPACE,
+                     "(): pp_sample_order_noalloc needs %zu bytes of scratch for %lld sampling points "
+                     "and %lld source voxels; its fixed scratch holds %zu bytes (use pp_sample_order "
+                     "with a workspace instead)",
+                     L.total, (long long)nvox, (long long)nsrc_total, NOALLOC_SCRATCH_BYTES);
+  void* scratch = nullptr;
+  if ((rc = noalloc_scratch(&scratch))) return rc;
+  if (nvox == 0) return PP_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned char* ws = static_cast<unsigned char*>(scratch);
+  int32_t* count = reinterpret_cast<int32_t*>(ws + L.count);
+  int32_t* keys = reinterpret_cast<int32_t*>(ws + L.keys);
+  int32_t* ranks = reinterpret_cast<int32_t*>(ws + L.ranks);
+  int32_t* partial = reinterpret_cast<int32_t*>(ws + L.partial);
+  // the histogram must start at zero; the scratch keeps the previous call's data
+  if ((rc = ppc::cuda_check(cudaMemsetAsync(count, 0, static_cast<size_t>(nsrc_total) * 4, st), "noalloc clear")))
+    return rc;
+  KeyArgs a;
+  a.grid = grid->data;
+  a.N = grid->sizes[0];
+  a.D = D;
+  a.gsN = grid->strides[0];
+  a.gsD = grid->strides[1 + D];
+  for (int d = 0; d < 3; ++d) {
+    a.size[d] = d < D ? grid->sizes[1 + d] : 1;
+    a.src[d] = d < D ? src_size[d] : 1;
+    a.gs[d] = d < D ? grid->strides[1 + d] : 0;
+  }
+  a.nvox = nvox;
+  a.nsrc = nsrc;
+  const unsigned nb = static_cast<unsigned>((nvox + 255) / 256);
+  if (grid->dtype == PP_FLOAT32) order_keys<float><<<nb, 256, 0, st>>>(a, count, keys, ranks);
+  else order_keys<double><<<nb, 256, 0, st>>>(a, count, keys, ranks);
+  const int64_t ntile = (nsrc_total + SCAN_TILE - 1) / SCAN_TILE;
+  scan_reduce<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, nsrc_total, partial);
+  scan_partials<<<1, SCAN_THREADS, 0, st>>>(partial, ntile);
+  scan_apply<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, nsrc_total, partial);
+  order_scatter<<<nb, 256, 0, st>>>(keys, ranks, count, nvox, perm);
+  ppc::count_launch(5);
+  return ppc::cuda_check(cudaGetLastError(), "sample order (no-alloc) launch");
 }
 
 }  // extern "C"
