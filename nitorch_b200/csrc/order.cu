@@ -8,8 +8,11 @@
 // scatter atomics hit a few lines per instruction.
 //
 // pp_sample_order computes that order -- a permutation of the grid's sample
-// indices sorted by the linear index of the source voxel floor(coords)
-// (clamped into the source volume, batch-major) -- with a counting sort:
+// indices sorted by the linear index (batch item, then the source voxel
+// floor(coords) clamped into the volume, last axis fastest) -- with a
+// counting sort.  (A brick-major key, 4x4x16 bricks, measured ~18 % slower
+// for the scatter kernels on B200 and gains nothing for the gathers.)
+// Steps:
 //   1. key / rank: key = source voxel, rank = atomicAdd(&count[key], 1);
 //   2. exclusive scan of count (block reduce, scan of block sums, apply);
 //   3. perm[offset[key] + rank] = sample.
@@ -34,8 +37,16 @@ struct KeyArgs {
   int64_t gsN, gs[3], gsD;
   int D;
   int64_t nvox;
-  int64_t nsrc;          // prod(src)
+  int64_t nsrc;          // number of keys per batch item (source voxels)
 };
+
+// Number of keys per batch item (source voxels) for sizes src[0..D-1].
+inline int64_t key_geometry(KeyArgs& a, int D, const int64_t* src) {
+  int64_t n = 1;
+  for (int d = 0; d < D; ++d) n *= src[d];
+  a.nsrc = n;
+  return n;
+}
 
 template <class T>
 __global__ void order_keys(KeyArgs a, int32_t* count, int32_t* keys, int32_t* ranks) {
@@ -167,12 +178,12 @@ int sizes_of(const pp_tensor* grid, const int64_t* src_size, int& D, int64_t& nv
     return ppc::fail(PP_ERR_DTYPE, "(): expected grid to be float32 or float64");
   if (!src_size) return ppc::fail(PP_ERR_ARG, "(): expected source sizes");
   nvox = grid->sizes[0];
-  nsrc = 1;
   for (int d = 0; d < D; ++d) {
     if (src_size[d] <= 0 || grid->sizes[1 + d] <= 0) return ppc::fail(PP_ERR_ARG, "(): expected non-empty sizes");
     nvox *= grid->sizes[1 + d];
-    nsrc *= src_size[d];
   }
+  KeyArgs tmp;
+  nsrc = key_geometry(tmp, D, src_size);
   if (nvox >= (int64_t(1) << 31) || nsrc * grid->sizes[0] >= (int64_t(1) << 31))
     return ppc::fail(PP_ERR_UNSUPPORTED, "(): sample ordering needs fewer than 2^31 samples and source voxels");
   return PP_OK;
@@ -220,7 +231,7 @@ int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* per
     a.gs[d] = d < D ? grid->strides[1 + d] : 0;
   }
   a.nvox = nvox;
-  a.nsrc = nsrc;
+  a.nsrc = key_geometry(a, D, src_size);
   const unsigned nb = static_cast<unsigned>((nvox + 255) / 256);
   if (grid->dtype == PP_FLOAT32) order_keys<float><<<nb, 256, 0, st>>>(a, count, keys, ranks);
   else order_keys<double><<<nb, 256, 0, st>>>(a, count, keys, ranks);
@@ -324,7 +335,7 @@ int pp_sample_order_noalloc(const pp_tensor* grid, const int64_t* src_size, int3
     a.gs[d] = d < D ? grid->strides[1 + d] : 0;
   }
   a.nvox = nvox;
-  a.nsrc = nsrc;
+  a.nsrc = key_geometry(a, D, src_size);
   const unsigned nb = static_cast<unsigned>((nvox + 255) / 256);
   if (grid->dtype == PP_FLOAT32) order_keys<float><<<nb, 256, 0, st>>>(a, count, keys, ranks);
   else order_keys<double><<<nb, 256, 0, st>>>(a, count, keys, ranks);

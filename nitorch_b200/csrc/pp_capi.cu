@@ -262,14 +262,81 @@ int run(Call& k, int mode, bool wide, cudaStream_t st) {
   return cuda_check(launch(k.dtype, k.D, mode, ord, wide, k.a, st), "push/pull kernel launch");
 }
 
-// 16-bit outputs of scatter modes accumulate into a float workspace.
+// Scatter-mode workspace: 16-bit outputs accumulate into a float buffer;
+// deterministic mode accumulates into int64 fixed point (256-byte header
+// holding the float bits of max |target|, then N*C*spatial int64).
 size_t scatter_ws_bytes(const pp_tensor* out, int flags) {
   if (!out) return 0;
-  size_t b = 0;
   const int64_t n = numel(out);
-  if (out->dtype == PP_BFLOAT16 || out->dtype == PP_FLOAT16) b += ((n * 4 + 255) / 256) * 256;
-  (void)flags;
-  return b;
+  if (flags & PP_DETERMINISTIC) return 256 + ((n * 8 + 255) / 256) * 256;
+  if (out->dtype == PP_BFLOAT16 || out->dtype == PP_FLOAT16) return ((n * 4 + 255) / 256) * 256;
+  return 0;
+}
+
+// max |t| over a strided tensor, as float bits (non-negative floats order
+// like their bit patterns, so an integer atomicMax is exact and
+// order-independent).
+template <class S>
+__global__ void det_absmax(const S* t, Strided s, unsigned int* out) {
+  int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  float m = 0.f;
+  for (; i < s.numel; i += step) m = fmaxf(m, fabsf(static_cast<float>(ppk::to_acc(t[strided_offset(s, i)]))));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+__global__ void det_set_one(unsigned int* out) { *out = __float_as_uint(1.0f); }
+
+// int64 fixed point -> strided output
+template <class S>
+__global__ void det_finalize(const unsigned long long* acc, S* dst, Strided s, const unsigned int* mx,
+                             double bound) {
+  const float m = __uint_as_float(*mx);
+  const double b = static_cast<double>(m) * bound;
+  double inv = 1.0;
+  if (b > 0.0) {
+    int ex;
+    frexp(b, &ex);
+    inv = ldexp(1.0, ex - 61);
+  }
+  int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (; i < s.numel; i += step) {
+    const double v = static_cast<double>(static_cast<long long>(acc[i])) * inv;
+    dst[strided_offset(s, i)] = ppk::from_acc<S>(static_cast<typename ppk::Acc<S>::type>(v));
+  }
+}
+
+int det_absmax_of(const pp_tensor* t, unsigned int* out, cudaStream_t st) {
+  const int64_t n = numel(t);
+  if (n == 0) return PP_OK;
+  Strided s = make_strided(t);
+  const int nb = grid_blocks(n);
+  switch (t->dtype) {
+    case PP_FLOAT32: det_absmax<float><<<nb, 256, 0, st>>>(static_cast<const float*>(t->data), s, out); break;
+    case PP_FLOAT64: det_absmax<double><<<nb, 256, 0, st>>>(static_cast<const double*>(t->data), s, out); break;
+    case PP_BFLOAT16: det_absmax<__nv_bfloat16><<<nb, 256, 0, st>>>(static_cast<const __nv_bfloat16*>(t->data), s, out); break;
+    default: det_absmax<__half><<<nb, 256, 0, st>>>(static_cast<const __half*>(t->data), s, out); break;
+  }
+  count_launch();
+  return cuda_check(cudaGetLastError(), "deterministic max");
+}
+
+int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const unsigned int* mx, double bound,
+                    cudaStream_t st) {
+  const int64_t n = numel(out);
+  if (n == 0) return PP_OK;
+  Strided s = make_strided(out);
+  const int nb = grid_blocks(n);
+  switch (out->dtype) {
+    case PP_FLOAT32: det_finalize<float><<<nb, 256, 0, st>>>(acc, static_cast<float*>(out->data), s, mx, bound); break;
+    case PP_FLOAT64: det_finalize<double><<<nb, 256, 0, st>>>(acc, static_cast<double*>(out->data), s, mx, bound); break;
+    case PP_BFLOAT16: det_finalize<__nv_bfloat16><<<nb, 256, 0, st>>>(acc, static_cast<__nv_bfloat16*>(out->data), s, mx, bound); break;
+    default: det_finalize<__half><<<nb, 256, 0, st>>>(acc, static_cast<__half*>(out->data), s, mx, bound); break;
+  }
+  count_launch();
+  return cuda_check(cudaGetLastError(), "deterministic finalize");
 }
 
 }  // namespace
@@ -335,23 +402,50 @@ int pp_grid_grad(const pp_tensor* input, const pp_tensor* grid, const pp_tensor*
 }
 
 // Scatter helper: push `trgt` (N,C,*grid[,K]) into `out` (N,C,*shape) with
-// `mode`, optionally fused with a grid gradient of `src`.
-static int scatter_into(Call& k, int mode, const pp_tensor* out, bool wide,
-                        void* ws, size_t ws_bytes, cudaStream_t st) {
+// `mode`, optionally fused with a grid gradient of `src`.  `trgt_t` is the
+// target tensor (NULL for count), used by the deterministic mode's bound.
+static int scatter_into(Call& k, int mode, const pp_tensor* out, const pp_tensor* trgt_t, bool wide,
+                        int flags, void* ws, size_t ws_bytes, cudaStream_t st) {
   int rc;
+  const bool det = (flags & PP_DETERMINISTIC) != 0;
   const bool half = out->dtype == PP_BFLOAT16 || out->dtype == PP_FLOAT16;
+  const size_t need = scatter_ws_bytes(out, flags);
+  if (need && (!ws || ws_bytes < need))
+    return fail(PP_ERR_WORKSPACE, "(): this push output needs %zu bytes of workspace", need);
+  // contiguous (N, C, *shape) strides of the accumulation buffers
+  int64_t cs[PP_MAX_DIM];
+  {
+    int64_t s = 1;
+    for (int i = out->ndim - 1; i >= 0; --i) { cs[i] = s; s *= out->sizes[i]; }
+  }
+  if (det) {
+    unsigned char* w = static_cast<unsigned char*>(ws);
+    unsigned int* mx = reinterpret_cast<unsigned int*>(w);
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(w + 256);
+    if ((rc = cuda_check(cudaMemsetAsync(ws, 0, need, st), "workspace clear"))) return rc;
+    if (trgt_t) {
+      if ((rc = det_absmax_of(trgt_t, mx, st))) return rc;
+    } else {
+      det_set_one<<<1, 1, 0, st>>>(mx);
+      count_launch();
+    }
+    int64_t per_item = 1;
+    for (int a = 0; a < k.D; ++a) per_item *= k.a.trgt_size[a];
+    k.a.det_acc = acc;
+    k.a.det_max = mx;
+    k.a.det_bound = static_cast<double>(per_item) * (mode == ppk::K_KD ? 2.0 * k.D : 1.0);
+    k.a.out = nullptr;
+    k.a.out_sN = cs[0];
+    k.a.out_sC = cs[1];
+    for (int a = 0; a < 3; ++a) k.a.out_s[a] = a < k.D ? cs[2 + a] : 0;
+    if ((rc = run(k, mode, wide, st))) return rc;
+    return det_finalize_to(acc, out, mx, k.a.det_bound, st);
+  }
   float* acc = nullptr;
   if (half) {
-    const size_t need = scatter_ws_bytes(out, 0);
-    if (!ws || ws_bytes < need)
-      return fail(PP_ERR_WORKSPACE, "(): 16-bit push output needs %zu bytes of workspace", need);
     acc = static_cast<float*>(ws);
     if ((rc = cuda_check(cudaMemsetAsync(acc, 0, numel(out) * 4, st), "workspace clear"))) return rc;
-    // dense (contiguous) float accumulator with the output's sizes
     k.a.out = acc;
-    int64_t s = 1;
-    int64_t cs[PP_MAX_DIM];
-    for (int i = out->ndim - 1; i >= 0; --i) { cs[i] = s; s *= out->sizes[i]; }
     k.a.out_sN = cs[0];
     k.a.out_sC = cs[1];
     for (int a = 0; a < 3; ++a) k.a.out_s[a] = a < k.D ? cs[2 + a] : 0;
@@ -386,8 +480,8 @@ int pp_grid_push(const pp_tensor* input, const pp_tensor* grid, const pp_tensor*
   k.a.C = input->sizes[1];
   set_image(input, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
   for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? out->sizes[2 + a] : 1;
-  return scatter_into(k, ppk::K_PUSH, out, need_wide(k, {input, out}), workspace, workspace_bytes,
-                      static_cast<cudaStream_t>(stream));
+  return scatter_into(k, ppk::K_PUSH, out, input, need_wide(k, {input, out}), opt->flags, workspace,
+                      workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
 int pp_grid_count(const pp_tensor* grid, const pp_tensor* out, const pp_options* opt, void* stream,
@@ -404,8 +498,8 @@ int pp_grid_count(const pp_tensor* grid, const pp_tensor* out, const pp_options*
   k.dtype = grid->dtype;
   k.a.C = 1;
   for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? out->sizes[2 + a] : 1;
-  return scatter_into(k, ppk::K_COUNT, out, need_wide(k, {out}), workspace, workspace_bytes,
-                      static_cast<cudaStream_t>(stream));
+  return scatter_into(k, ppk::K_COUNT, out, nullptr, need_wide(k, {out}), opt->flags, workspace,
+                      workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
 static int check_ggrad(const pp_tensor* gg, const pp_tensor* grid) {
@@ -446,9 +540,9 @@ int pp_grid_pull_backward(const pp_tensor* grad, const pp_tensor* input, const p
     set_grid(grad_grid, k.D, k.a.gg_sN, k.a.gg_s, k.a.gg_sD);
     k.a.flags = ppk::F_GRAD | (grad_input ? ppk::F_A : 0);
     if (!grad_input) return run(k, ppk::K_PUSHGRAD, wide, st);
-    return scatter_into(k, ppk::K_PUSHGRAD, grad_input, wide, workspace, workspace_bytes, st);
+    return scatter_into(k, ppk::K_PUSHGRAD, grad_input, grad, wide, opt->flags, workspace, workspace_bytes, st);
   }
-  return scatter_into(k, ppk::K_PUSH, grad_input, wide, workspace, workspace_bytes, st);
+  return scatter_into(k, ppk::K_PUSH, grad_input, grad, wide, opt->flags, workspace, workspace_bytes, st);
 }
 
 int pp_grid_push_backward(const pp_tensor* grad, const pp_tensor* input, const pp_tensor* grid,
@@ -542,7 +636,7 @@ int pp_grid_grad_backward(const pp_tensor* grad, const pp_tensor* input, const p
     set_grid(grad_grid, k.D, k.a.gg_sN, k.a.gg_s, k.a.gg_sD);
   }
   if (!grad_input) return run(k, ppk::K_KD, wide, st);
-  return scatter_into(k, ppk::K_KD, grad_input, wide, workspace, workspace_bytes, st);
+  return scatter_into(k, ppk::K_KD, grad_input, grad, wide, opt->flags, workspace, workspace_bytes, st);
 }
 
 }  // extern "C"

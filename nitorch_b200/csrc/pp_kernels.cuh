@@ -48,7 +48,26 @@ struct PPArgs {
   int flags;
   int64_t nvox;
   const int32_t* perm;  // optional processing order of the sampling points
+  // Deterministic scatter: when det_acc is set, scatter modes accumulate
+  // round(v * 2^e) into this int64 buffer (contiguous (N, C, *src_size))
+  // instead of float atomics into `out`; e is derived from the float bits of
+  // max |target| (det_max, written by a reduction) times det_bound so that
+  // no partial sum can overflow.  Integer addition is associative, so the
+  // result does not depend on the order of the atomics.
+  unsigned long long* det_acc;
+  const unsigned int* det_max;
+  double det_bound;
 };
+
+// Power-of-two scale of the deterministic accumulators: bound * scale < 2^61.
+__device__ __forceinline__ double det_scale(const PPArgs& a) {
+  const float m = __uint_as_float(__ldg(a.det_max));
+  const double bound = static_cast<double>(m) * a.det_bound;
+  if (!(bound > 0.0)) return 1.0;
+  int ex;
+  frexp(bound, &ex);            // bound = f * 2^ex, f in [0.5, 1)
+  return ldexp(1.0, 61 - ex);
+}
 
 template <int ORD> struct Taps { static constexpr int value = ORD < 0 ? 8 : (ORD == 0 ? 1 : ORD + 1); };
 // Unroll factor of the outermost (z) tap loop: full up to cubic, rolled for
@@ -125,7 +144,7 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
 
   // ---- sampling point (n, x, y, z) -------------------------------------
   I sub[3] = {0, 0, 0};
-  I n;
+  I n = 0;
   if (a.perm != nullptr) {
     // explicit processing order (source-sorted): linear thread index
     const int64_t t = (static_cast<int64_t>(blockIdx.x) * TILE_MID + threadIdx.y) * TILE_IN + threadIdx.x;
@@ -241,6 +260,17 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
   const S* src_n = GATHER ? static_cast<const S*>(a.src) + static_cast<int64_t>(n) * a.src_sN : nullptr;
   T* outs_n = SCATTER ? static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN : nullptr;
   const S* trg_v = static_cast<const S*>(a.trgt) + tvox;
+  const double dscale = (SCATTER && a.det_acc != nullptr) ? det_scale(a) : 0.0;
+  unsigned long long* dacc_n = (SCATTER && a.det_acc != nullptr) ? a.det_acc + static_cast<int64_t>(n) * a.out_sN : nullptr;
+  // scatter of v to tap offset `off` of channel cb of the current group
+#define PP_SCATTER(off, v)                                                                   \
+  do {                                                                                       \
+    if (dacc_n != nullptr)                                                                   \
+      atomicAdd(dacc_n + ((c0 + cb) * a.out_sC + (off)),                                     \
+                static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(v) * dscale))); \
+    else                                                                                     \
+      atomic_acc(opc + (cb * a.out_sC + (off)), (v));                                        \
+  } while (0)
 
 #define PP_TAP_VALID(i, j, k) (full || ((((ax.mask >> (i)) & (ay.mask >> (j)) & (az.mask >> (k))) & 1u) != 0u))
 
@@ -414,7 +444,7 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
                   PP_CB {
                     if (CB == 1 || cb < nc) {
                       const T v = wt * t[cb];
-                      if (v != T(0)) atomic_acc(opc + (cb * a.out_sC + off), v);
+                      if (v != T(0)) PP_SCATTER(off, v);
                     }
                   }
                 }
@@ -479,7 +509,7 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
                     PP_CB {
                       if (CB == 1 || cb < nc) {
                         const T pv = wt * t[cb];
-                        if (pv != T(0)) atomic_acc(opc + (cb * a.out_sC + off), pv);
+                        if (pv != T(0)) PP_SCATTER(off, pv);
                       }
                     }
                   }
@@ -571,7 +601,7 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
                         const T pa = ay.w[j] * az.w[k] * t0[cb];
                         const T pb = ay.g[j] * az.w[k] * t1[cb] + ay.w[j] * az.g[k] * t2[cb];
                         const T pv = ax.g[i] * pa + ax.w[i] * pb;
-                        if (pv != T(0)) atomic_acc(opc + (cb * a.out_sC + off), pv);
+                        if (pv != T(0)) PP_SCATTER(off, pv);
                       }
                     }
                   }
@@ -615,6 +645,8 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
   }
 #undef PP_GRAD_GATHER
 #undef PP_CB
+#undef PP_SCATTER
+
 #undef PP_TAP_VALID
 }
 

@@ -33,3 +33,20 @@ def config1_inputs(size=64):
     from nitorch_b200 import workloads
     x, grid, y = workloads.config1(size)
     return x.numpy(), grid.numpy(), y.numpy()
+
+
+def sort_keys(grid, src):
+    """Source-voxel key of every sampling point of `grid` ((N, *spatial, D)
+    numpy), as the source-sorted order defines it: batch item, then the
+    linear index of floor(coords) clamped into the source (last axis fastest)."""
+    D = grid.shape[-1]
+    N = grid.shape[0]
+    src = np.array(src)
+    c = np.floor(grid.reshape(N, -1, D).astype(np.float64))
+    c = np.where(np.isnan(c), 0, c)
+    c = np.clip(c, 0, src - 1).astype(np.int64)
+    lin = np.zeros(c.shape[:2], np.int64)
+    for d in range(D):
+        lin = lin * src[d] + c[..., d]
+    n = np.arange(N)[:, None]
+    return (n * np.prod(src) + lin).reshape(-1)

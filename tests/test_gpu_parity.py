@@ -181,6 +181,52 @@ def test_sample_order_sorted_by_source_voxel():
     vol, grid = make_case(3, seed=3, in_size=12, out_size=10, C=1, N=1, spread=3.0)
     G = cu(grid, torch.float32)
     perm = spatial.sample_order(G, vol.shape[2:]).cpu().numpy()
-    c = np.clip(np.floor(grid.reshape(-1, 3).astype(np.float32)), 0, 11).astype(np.int64)
-    key = (c[:, 0] * 12 + c[:, 1]) * 12 + c[:, 2]
+    from tests._cases import sort_keys
+    key = sort_keys(grid.astype(np.float32), vol.shape[2:])
     assert np.all(np.diff(key[perm]) >= 0)
+    for dim in (1, 2):
+        v, g = make_case(dim, seed=dim, in_size=40, out_size=30, C=1, N=2, spread=3.0)
+        p = spatial.sample_order(cu(g, torch.float32), v.shape[2:]).cpu().numpy()
+        k = sort_keys(g.astype(np.float32), v.shape[2:])
+        assert np.all(np.diff(k[p]) >= 0)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64, torch.bfloat16])
+@pytest.mark.parametrize("order", [1, 3])
+def test_deterministic_scatter_is_bit_stable_and_order_independent(dtype, order):
+    """PP_DETERMINISTIC: push / count / the push halves of the backward passes
+    are bit-identical run to run and whatever the processing order (natural
+    or source-sorted), and stay within the parity tolerances."""
+    from nitorch_b200 import spatial
+    vol, grid = make_case(3, seed=60 + order, in_size=20, out_size=18, C=3, N=2, spread=2.5)
+    g = np.random.default_rng(2)
+    tgt = g.standard_normal((2, 3) + grid.shape[1:-1])
+    ggrad = g.standard_normal((2, 3) + grid.shape[1:-1] + (3,))
+    b, o = enums(2, order)
+    T, Gd = cu(tgt, dtype), cu(grid, dtype, grid=True)
+    V = cu(vol, dtype, rg=True)
+    Gr = cu(grid, dtype, rg=True, grid=True)
+    runs = []
+    try:
+        spatial.set_deterministic(True)
+        for mode in ("natural", "sorted", "sorted", "natural"):
+            spatial.set_sample_order(mode)
+            spatial._orders.clear()
+            out = [spatial.grid_push(T, Gd, [20, 20, 20], b, o, 1),
+                   spatial.grid_count(Gd, [20, 20, 20], b, o, 1),
+                   spatial.grid_pull_backward(T, V, Gr, b, o, 1)[0],
+                   spatial.grid_grad_backward(cu(ggrad, dtype), V, Gr, b, o, 1)[0]]
+            runs.append([t.detach().cpu() for t in out])
+    finally:
+        spatial.set_deterministic(False)
+        spatial.set_sample_order("auto")
+    for r in runs[1:]:
+        for a_, b_ in zip(runs[0], r):
+            assert torch.equal(a_.view(torch.uint8) if False else a_, b_), "not bit-stable"
+    ref = [O.grid_push(T.double().cpu().numpy(), grid.astype(np.float32).astype(np.float64)
+                       if dtype != torch.float64 else grid, (20, 20, 20), [2], [order], 1)]
+    tol = {torch.float64: 1e-12, torch.float32: 1e-5, torch.bfloat16: 2.0 ** -8 + 1e-5}[dtype]
+    assert relerr(runs[0][0].double().numpy(), ref[0]) < tol
+    cnt = O.grid_count(grid.astype(np.float32).astype(np.float64) if dtype != torch.float64 else grid,
+                       (20, 20, 20), [2], [order], 1)
+    assert relerr(runs[0][1].double().numpy(), cnt) < tol

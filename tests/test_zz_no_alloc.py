@@ -24,9 +24,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _keys(grid, src):
-    c = np.floor(grid.reshape(-1, 3).astype(np.float64))
-    c = np.clip(c, 0, np.array(src) - 1).astype(np.int64)
-    return (c[:, 0] * src[1] + c[:, 1]) * src[2] + c[:, 2]
+    from tests._cases import sort_keys
+    return sort_keys(grid[None], src)
 
 
 def _grid(shape, src, seed):
