@@ -152,6 +152,25 @@ PP_API int pp_grid_grad_backward(const pp_tensor* grad, const pp_tensor* input,
                           const pp_tensor* grad_grid, const pp_options* opt,
                           void* stream, void* workspace, size_t workspace_bytes);
 
+/* Fused normal operator push(pull(input, grid), grid) in one pass (no
+ * counterpart in the reference, which calls ni::grid_pull then
+ * ni::grid_push on the same grid): out (input's sizes, any strides) =
+ * P^T P input, with the pulled values rounded to the storage type as a
+ * separate pull would store them.  Workspace as for pp_grid_push
+ * (pp_push_workspace_bytes of `out`). */
+PP_API int pp_grid_pull_push(const pp_tensor* input, const pp_tensor* grid, const pp_tensor* out,
+                             const pp_options* opt, void* stream, void* workspace,
+                             size_t workspace_bytes);
+
+/* Backward of pp_grid_pull_push for the loss gradient `grad` (input's sizes
+ * AND strides): grad_input = P^T P grad (the operator is self-adjoint) and
+ * the grid gradient (grid's sizes); either may be NULL.  One pass (the
+ * reference runs ni::grid_push_backward then ni::grid_pull_backward). */
+PP_API int pp_grid_pull_push_backward(const pp_tensor* grad, const pp_tensor* input,
+                                      const pp_tensor* grid, const pp_tensor* grad_input,
+                                      const pp_tensor* grad_grid, const pp_options* opt,
+                                      void* stream, void* workspace, size_t workspace_bytes);
+
 /* Source-sorted processing order of a grid's sampling points (no
  * counterpart in the reference; a scheduling aid for rough deformations):
  * writes to `perm` (int32, N*prod(grid spatial) entries) the sample indices

@@ -8,19 +8,20 @@ plus the spline_coeff prefilter, behind a C ABI (include/nitorch_b200.h).
 Entry points:
   nitorch_b200.grid_pull / grid_push / grid_count / grid_grad /
   spline_coeff / spline_coeff_nd / identity_grid   (nitorch.spatial API)
+  nitorch_b200.pull_push    fused push(pull(.)) (normal operator), one pass
   nitorch_b200.spatial      drop-in for the ``nitorch._C.spatial`` module
   nitorch_b200.coeff        drop-in for ``interpol.coeff``
   nitorch_b200.batch        many uneven volumes in one persistent launch
   nitorch_b200.install()    route an installed nitorch through this backend
 """
-from .api import (grid_count, grid_grad, grid_pull, grid_push, identity_grid,
+from .api import (grid_count, grid_grad, grid_pull, grid_push, identity_grid, pull_push,
                   spline_coeff, spline_coeff_nd)
 from .enums import BoundType, InterpolationType
 from .spatial import get_deterministic, set_deterministic
 from . import spatial, coeff, grid
 from .integration import install
 
-__all__ = ["grid_pull", "grid_push", "grid_count", "grid_grad", "spline_coeff",
+__all__ = ["grid_pull", "grid_push", "grid_count", "grid_grad", "pull_push", "spline_coeff",
            "spline_coeff_nd", "identity_grid", "BoundType", "InterpolationType",
            "set_deterministic", "get_deterministic", "spatial", "coeff", "grid",
            "install"]

@@ -61,7 +61,7 @@ EXPORTS = (
     "pp_grid_push_backward", "pp_grid_count", "pp_grid_count_backward",
     "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
     "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
-    "pp_sample_order_noalloc",
+    "pp_sample_order_noalloc", "pp_grid_pull_push", "pp_grid_pull_push_backward",
 )
 
 _lib = None
@@ -84,6 +84,8 @@ def _declare(L):
     L.pp_grid_count_backward.argtypes = [T, T, T, O, vp]
     L.pp_grid_grad.argtypes = [T, T, T, O, vp]
     L.pp_grid_grad_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
+    L.pp_grid_pull_push.argtypes = [T, T, T, O, vp, vp, sz]
+    L.pp_grid_pull_push_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
     L.pp_spline_coeff.argtypes = [T, T, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp]
     L.pp_spline_coeff_nd.argtypes = [T, T, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                      ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),

@@ -9,7 +9,7 @@ Same signatures, defaults, broadcasting and output shapes as
 """
 import torch
 
-from .grid import GridCount, GridGrad, GridPull, GridPush, SplineCoeff, SplineCoeffND
+from .grid import GridCount, GridGrad, GridPull, GridPullPush, GridPush, SplineCoeff, SplineCoeffND
 
 
 def _expanded_shape(*shapes):
@@ -101,6 +101,21 @@ def grid_push(input, grid, shape=None, interpolation="linear", bound="zero",
     if prefilter:
         out = spline_coeff_nd(out, interpolation=interpolation, bound=bound, dim=dim,
                               inplace=True)
+    return _postproc(out, shape_info, mode="push")
+
+
+def pull_push(input, grid, interpolation="linear", bound="zero", extrapolate=False, prefilter=False):
+    """push(pull(input, grid), grid) back onto the input's lattice, fused into
+    one pass forward and one backward (the normal operator P^T P of a
+    registration).  Equals grid_push(grid_pull(input, grid, ...), grid,
+    input.shape[-dim:], ...) up to floating-point summation order; the grid
+    may have any spatial shape.  `prefilter` applies to the pulled input, as
+    in grid_pull.  Not in the reference, which runs the two calls."""
+    grid, input, shape_info = _preproc(grid, input)
+    dim = grid.shape[-1]
+    if prefilter:
+        input = spline_coeff_nd(input, interpolation=interpolation, bound=bound, dim=dim)
+    out = GridPullPush.apply(input, grid, interpolation, bound, extrapolate)
     return _postproc(out, shape_info, mode="push")
 
 

@@ -12,113 +12,33 @@
 #include "pp_kernels.cuh"
 
 // Launchers compiled from pp_inst.cu, one per (dtype, dim, mode).
-cudaError_t pp_launch_f32_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f32_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f64_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_bf16_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d1_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d1_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d1_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d1_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d1_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d1_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d1_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d2_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d2_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d2_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d2_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d2_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d2_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d2_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d3_m0(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d3_m1(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d3_m2(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d3_m3(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d3_m4(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d3_m5(int, bool, const ppk::PPArgs&, cudaStream_t);
-cudaError_t pp_launch_f16_d3_m6(int, bool, const ppk::PPArgs&, cudaStream_t);
+#define PP_DECL_MODES(S, D)                                                        \
+  cudaError_t pp_launch_##S##_d##D##_m0(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m1(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m2(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m3(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m4(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m5(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m6(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m7(int, bool, const ppk::PPArgs&, cudaStream_t); \
+  cudaError_t pp_launch_##S##_d##D##_m8(int, bool, const ppk::PPArgs&, cudaStream_t);
+#define PP_DECL_DIMS(S) PP_DECL_MODES(S, 1) PP_DECL_MODES(S, 2) PP_DECL_MODES(S, 3)
+PP_DECL_DIMS(f32)
+PP_DECL_DIMS(f64)
+PP_DECL_DIMS(bf16)
+PP_DECL_DIMS(f16)
+#undef PP_DECL_DIMS
+#undef PP_DECL_MODES
 
-static const pp_launcher_t kLaunchers[4][3][7] = {
-  {
-    {pp_launch_f32_d1_m0, pp_launch_f32_d1_m1, pp_launch_f32_d1_m2, pp_launch_f32_d1_m3, pp_launch_f32_d1_m4, pp_launch_f32_d1_m5, pp_launch_f32_d1_m6},
-    {pp_launch_f32_d2_m0, pp_launch_f32_d2_m1, pp_launch_f32_d2_m2, pp_launch_f32_d2_m3, pp_launch_f32_d2_m4, pp_launch_f32_d2_m5, pp_launch_f32_d2_m6},
-    {pp_launch_f32_d3_m0, pp_launch_f32_d3_m1, pp_launch_f32_d3_m2, pp_launch_f32_d3_m3, pp_launch_f32_d3_m4, pp_launch_f32_d3_m5, pp_launch_f32_d3_m6},
-  },
-  {
-    {pp_launch_f64_d1_m0, pp_launch_f64_d1_m1, pp_launch_f64_d1_m2, pp_launch_f64_d1_m3, pp_launch_f64_d1_m4, pp_launch_f64_d1_m5, pp_launch_f64_d1_m6},
-    {pp_launch_f64_d2_m0, pp_launch_f64_d2_m1, pp_launch_f64_d2_m2, pp_launch_f64_d2_m3, pp_launch_f64_d2_m4, pp_launch_f64_d2_m5, pp_launch_f64_d2_m6},
-    {pp_launch_f64_d3_m0, pp_launch_f64_d3_m1, pp_launch_f64_d3_m2, pp_launch_f64_d3_m3, pp_launch_f64_d3_m4, pp_launch_f64_d3_m5, pp_launch_f64_d3_m6},
-  },
-  {
-    {pp_launch_bf16_d1_m0, pp_launch_bf16_d1_m1, pp_launch_bf16_d1_m2, pp_launch_bf16_d1_m3, pp_launch_bf16_d1_m4, pp_launch_bf16_d1_m5, pp_launch_bf16_d1_m6},
-    {pp_launch_bf16_d2_m0, pp_launch_bf16_d2_m1, pp_launch_bf16_d2_m2, pp_launch_bf16_d2_m3, pp_launch_bf16_d2_m4, pp_launch_bf16_d2_m5, pp_launch_bf16_d2_m6},
-    {pp_launch_bf16_d3_m0, pp_launch_bf16_d3_m1, pp_launch_bf16_d3_m2, pp_launch_bf16_d3_m3, pp_launch_bf16_d3_m4, pp_launch_bf16_d3_m5, pp_launch_bf16_d3_m6},
-  },
-  {
-    {pp_launch_f16_d1_m0, pp_launch_f16_d1_m1, pp_launch_f16_d1_m2, pp_launch_f16_d1_m3, pp_launch_f16_d1_m4, pp_launch_f16_d1_m5, pp_launch_f16_d1_m6},
-    {pp_launch_f16_d2_m0, pp_launch_f16_d2_m1, pp_launch_f16_d2_m2, pp_launch_f16_d2_m3, pp_launch_f16_d2_m4, pp_launch_f16_d2_m5, pp_launch_f16_d2_m6},
-    {pp_launch_f16_d3_m0, pp_launch_f16_d3_m1, pp_launch_f16_d3_m2, pp_launch_f16_d3_m3, pp_launch_f16_d3_m4, pp_launch_f16_d3_m5, pp_launch_f16_d3_m6},
-  },
-};
+#define PP_ROW(S, D)                                                                          \
+  {pp_launch_##S##_d##D##_m0, pp_launch_##S##_d##D##_m1, pp_launch_##S##_d##D##_m2,          \
+   pp_launch_##S##_d##D##_m3, pp_launch_##S##_d##D##_m4, pp_launch_##S##_d##D##_m5,          \
+   pp_launch_##S##_d##D##_m6, pp_launch_##S##_d##D##_m7, pp_launch_##S##_d##D##_m8}
+#define PP_TYPE(S) {PP_ROW(S, 1), PP_ROW(S, 2), PP_ROW(S, 3)}
+static const pp_launcher_t kLaunchers[4][3][ppk::K_NMODES] = {PP_TYPE(f32), PP_TYPE(f64), PP_TYPE(bf16),
+                                                              PP_TYPE(f16)};
+#undef PP_TYPE
+#undef PP_ROW
 
 namespace ppc {
 
@@ -637,6 +557,68 @@ int pp_grid_grad_backward(const pp_tensor* grad, const pp_tensor* input, const p
   }
   if (!grad_input) return run(k, ppk::K_KD, wide, st);
   return scatter_into(k, ppk::K_KD, grad_input, grad, wide, opt->flags, workspace, workspace_bytes, st);
+}
+
+// Fused push(pull(input)): out (laid out freely, input's shape) =
+// P^T P input for the sampling points of `grid`.  No counterpart in the
+// reference (where it is grid_pull then grid_push on the same grid).
+int pp_grid_pull_push(const pp_tensor* input, const pp_tensor* grid, const pp_tensor* out,
+                      const pp_options* opt, void* stream, void* workspace, size_t workspace_bytes) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if (input->sizes[0] != grid->sizes[0])
+    return fail(PP_ERR_ARG, "(): expected input and grid to have the same batch size");
+  if ((rc = check_tensor(out, "output"))) return rc;
+  if ((rc = check_same_sizes(out, input->sizes, input->ndim, "output"))) return rc;
+  if (out->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match input");
+  k.dtype = input->dtype;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  k.a.src = input->data;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  return scatter_into(k, ppk::K_PP, out, input, need_wide(k, {input, out}), opt->flags, workspace,
+                      workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+// Backward of pp_grid_pull_push for a loss gradient `grad` (input's shape
+// and strides): grad_input = P^T P grad, grad_grid as described in
+// pp_kernels.cuh (K_PP_BWD).  Either output may be NULL.
+int pp_grid_pull_push_backward(const pp_tensor* grad, const pp_tensor* input, const pp_tensor* grid,
+                               const pp_tensor* grad_input, const pp_tensor* grad_grid, const pp_options* opt,
+                               void* stream, void* workspace, size_t workspace_bytes) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if (input->sizes[0] != grid->sizes[0])
+    return fail(PP_ERR_ARG, "(): expected input and grid to have the same batch size");
+  if ((rc = check_tensor(grad, "grad"))) return rc;
+  if ((rc = check_same_sizes(grad, input->sizes, input->ndim, "grad"))) return rc;
+  if (grad->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad dtype must match input");
+  for (int i = 0; i < input->ndim; ++i)
+    if (input->sizes[i] > 1 && grad->strides[i] != input->strides[i])
+      return fail(PP_ERR_UNSUPPORTED, "(): fused pull-push backward needs grad laid out like the input");
+  if (grad_input && (rc = check_same_sizes(grad_input, input->sizes, input->ndim, "grad_input"))) return rc;
+  if (grad_input && grad_input->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad_input dtype must match input");
+  if (grad_grid && (rc = check_ggrad(grad_grid, grid))) return rc;
+  if (!grad_input && !grad_grid) return PP_OK;
+  k.dtype = input->dtype;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  k.a.src = input->data;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.trgt = grad->data;
+  k.a.flags = (grad_grid ? ppk::F_GRAD : 0) | (grad_input ? ppk::F_A : 0);
+  if (grad_grid) {
+    k.a.gg = grad_grid->data;
+    set_grid(grad_grid, k.D, k.a.gg_sN, k.a.gg_s, k.a.gg_sD);
+  }
+  const bool wide = need_wide(k, {input, grad, grad_input});
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!grad_input) return run(k, ppk::K_PP_BWD, wide, st);
+  return scatter_into(k, ppk::K_PP_BWD, grad_input, grad, wide, opt->flags, workspace, workspace_bytes, st);
 }
 
 }  // extern "C"

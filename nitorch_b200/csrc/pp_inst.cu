@@ -1,7 +1,7 @@
 // One (storage type, dimension, mode) slice of the push/pull kernel family.
 // Compiled several times by the Makefile with
 //   -DPP_STYPE=<float|double|__nv_bfloat16|__half> -DPP_SNAME=<f32|...>
-//   -DPP_DIM=<1|2|3> -DPP_MODE=<0..6>
+//   -DPP_DIM=<1|2|3> -DPP_MODE=<0..8>
 // and exports  pp_launch_<sname>_d<dim>_m<mode>(ord, wide, args, stream).
 #include "pp_kernels.cuh"
 

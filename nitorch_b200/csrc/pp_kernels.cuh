@@ -21,13 +21,21 @@
 //   K_PUSHGRAD pull_backward (+grid), count_backward (no target: t = 1)
 //   K_KD       grid_grad_backward              out[c] += sum_d dw_d t[c,d];
 //                                              gg_d = sum_c sum_e t[c,e] sum d2w_de src[c]
+//   K_PP       push(pull(src)) in one pass: y = sum w src (gathered, rounded to
+//              the storage type as a separate pull would store it), then
+//              out += w y at the same taps (no counterpart in the reference,
+//              which runs grid_pull then grid_push)
+//   K_PP_BWD   its adjoint pass: P^T P is self-adjoint, so with W = trgt
+//              (laid out like src) out += w (sum w W) and the grid gradient is
+//              gg_d = sum_c [ (P src)_c d(P W)_c/dx_d + (P W)_c d(P src)_c/dx_d ]
 // Runtime flags select the optional halves of the fused modes.
 #pragma once
 #include "pp_common.cuh"
 
 namespace ppk {
 
-enum Mode : int { K_PULL = 0, K_SGRAD, K_PUSH, K_COUNT, K_PULLGRAD, K_PUSHGRAD, K_KD, K_NMODES };
+enum Mode : int { K_PULL = 0, K_SGRAD, K_PUSH, K_COUNT, K_PULLGRAD, K_PUSHGRAD, K_KD,
+                  K_PP, K_PP_BWD, K_NMODES };
 enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4 };  // F_A: pull (PULLGRAD) / push (PUSHGRAD, KD)
 
 struct PPArgs {
@@ -132,47 +140,21 @@ constexpr int TILE_IN = 32, TILE_MID = 8, PP_THREADS = TILE_IN * TILE_MID;
 
 template <int MODE> struct MinBlocks { static constexpr int value = (MODE == K_PUSH || MODE == K_COUNT) ? 3 : 2; };
 
+// One sampling point (batch item n, grid position sub) of mode MODE: the
+// whole per-point computation, shared by the single-tensor kernel below and
+// the batched kernel (batch.cu).
 template <int D, int ORD, int CB, class S, int MODE, class I>
-__global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(const PPArgs a) {
+__device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], const I n) {
   using T = typename Acc<S>::type;
   constexpr int NT = Taps<ORD>::value;
   constexpr int NX = NT, NY = D > 1 ? NT : 1, NZ = D > 2 ? NT : 1;
-  constexpr bool NEED_G = MODE == K_SGRAD || MODE == K_PULLGRAD || MODE == K_PUSHGRAD || MODE == K_KD;
+  constexpr bool NEED_G = MODE == K_SGRAD || MODE == K_PULLGRAD || MODE == K_PUSHGRAD || MODE == K_KD ||
+                          MODE == K_PP_BWD;
   constexpr bool NEED_H = MODE == K_KD;
-  constexpr bool GATHER = MODE == K_PULL || MODE == K_SGRAD || MODE == K_PULLGRAD || MODE == K_PUSHGRAD || MODE == K_KD;
-  constexpr bool SCATTER = MODE == K_PUSH || MODE == K_COUNT || MODE == K_PUSHGRAD || MODE == K_KD;
-
-  // ---- sampling point (n, x, y, z) -------------------------------------
-  I sub[3] = {0, 0, 0};
-  I n = 0;
-  if (a.perm != nullptr) {
-    // explicit processing order (source-sorted): linear thread index
-    const int64_t t = (static_cast<int64_t>(blockIdx.x) * TILE_MID + threadIdx.y) * TILE_IN + threadIdx.x;
-    if (t >= a.nvox) return;
-    I v = static_cast<I>(__ldg(a.perm + t));
-    if (D > 2) { sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]); }
-    if (D > 1) { sub[1] = v % static_cast<I>(a.trgt_size[1]); v /= static_cast<I>(a.trgt_size[1]); }
-    sub[0] = v % static_cast<I>(a.trgt_size[0]);
-    n = v / static_cast<I>(a.trgt_size[0]);
-  } else {
-    // 2-D tile mapping over the grid
-    const I inner = static_cast<I>(a.trgt_size[D - 1]);
-    const I mid = D > 1 ? static_cast<I>(a.trgt_size[D - 2]) : I(1);
-    const I ntile = (inner + TILE_IN - 1) / TILE_IN;
-    const I outer_idx = static_cast<I>(blockIdx.x) / ntile;
-    const I ii = (static_cast<I>(blockIdx.x) - outer_idx * ntile) * TILE_IN + static_cast<I>(threadIdx.x);
-    const I mm = static_cast<I>(blockIdx.y) * TILE_MID + static_cast<I>(threadIdx.y);
-    if (ii >= inner || mm >= mid) return;
-    if (D == 3) {
-      sub[2] = ii; sub[1] = mm;
-      sub[0] = outer_idx % static_cast<I>(a.trgt_size[0]);
-      n = outer_idx / static_cast<I>(a.trgt_size[0]);
-    } else if (D == 2) {
-      sub[1] = ii; sub[0] = mm; n = outer_idx;
-    } else {
-      sub[0] = ii; n = outer_idx;
-    }
-  }
+  constexpr bool GATHER = MODE == K_PULL || MODE == K_SGRAD || MODE == K_PULLGRAD || MODE == K_PUSHGRAD ||
+                          MODE == K_KD || MODE == K_PP || MODE == K_PP_BWD;
+  constexpr bool SCATTER = MODE == K_PUSH || MODE == K_COUNT || MODE == K_PUSHGRAD || MODE == K_KD ||
+                           MODE == K_PP || MODE == K_PP_BWD;
 
   // ---- coordinates ------------------------------------------------------
   const T* gp = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
@@ -216,7 +198,7 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
           }
         }
       }
-      if ((MODE == K_PULLGRAD || MODE == K_PUSHGRAD || MODE == K_KD) && do_grad) {
+      if ((MODE == K_PULLGRAD || MODE == K_PUSHGRAD || MODE == K_KD || MODE == K_PP_BWD) && do_grad) {
         T* g = static_cast<T*>(a.gg) + gvox;
 #pragma unroll
         for (int d = 0; d < D; ++d) g[d * a.gg_sD] = T(0);
@@ -643,11 +625,244 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
       if (D > 2) g[2 * a.gg_sD] = og2;
     }
   }
+
+  if constexpr (MODE == K_PP) {
+    // One pass of push(pull(src)): the gather and the scatter share the
+    // stencil; out has src's shape (its own strides, offsets `oo`).
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      const S* sp = src_n + c0 * a.src_sC;
+      T* opc = outs_n + c0 * a.out_sC;
+      T y[CB];
+#pragma unroll
+      PP_CB y[cb] = T(0);
+#pragma unroll (OuterUnroll<ORD, NZ>::value)
+      for (int k = 0; k < NZ; ++k) {
+        if (k < tz) {
+          T accy[CB];
+#pragma unroll
+          PP_CB accy[cb] = T(0);
+#pragma unroll
+          for (int j = 0; j < NY; ++j) {
+            if (j < ty) {
+              const I oyz = ay.os[j] + az.os[k];
+              T accx[CB];
+#pragma unroll
+              PP_CB accx[cb] = T(0);
+#pragma unroll
+              for (int i = 0; i < NX; ++i) {
+                if (i < tx) {
+                  const I off = ax.os[i] + oyz;
+                  const bool valid = PP_TAP_VALID(i, j, k);
+#pragma unroll
+                  PP_CB {
+                    if (CB == 1 || cb < nc) {
+                      T v = ldg_acc(sp + (cb * a.src_sC + off));
+                      if (!valid) v = T(0);
+                      accx[cb] = fma(ax.w[i], v, accx[cb]);
+                    }
+                  }
+                }
+              }
+#pragma unroll
+              PP_CB accy[cb] = fma(ay.w[j], accx[cb], accy[cb]);
+            }
+          }
+#pragma unroll
+          PP_CB y[cb] = fma(az.w[k], accy[cb], y[cb]);
+        }
+      }
+      // the pulled value as a separate pull would have stored it
+#pragma unroll
+      PP_CB y[cb] = to_acc(from_acc<S>(y[cb]));
+#pragma unroll (OuterUnroll<ORD, NZ>::value)
+      for (int k = 0; k < NZ; ++k) {
+        if (k < tz) {
+#pragma unroll
+          for (int j = 0; j < NY; ++j) {
+            if (j < ty) {
+              const T wyz = ay.w[j] * az.w[k];
+              const I oyz = ay.oo[j] + az.oo[k];
+#pragma unroll
+              for (int i = 0; i < NX; ++i) {
+                if (i < tx && PP_TAP_VALID(i, j, k)) {
+                  const T wt = ax.w[i] * wyz;
+                  const I off = ax.oo[i] + oyz;
+#pragma unroll
+                  PP_CB {
+                    if (CB == 1 || cb < nc) {
+                      const T v = wt * y[cb];
+                      if (v != T(0)) PP_SCATTER(off, v);
+                    }
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+
+  if constexpr (MODE == K_PP_BWD) {
+    // Adjoint of K_PP.  trgt = W = d loss / d out, laid out like src
+    // (checked on the host), so it shares src's offsets `os`.
+    const S* wsrc_n = static_cast<const S*>(a.trgt) + static_cast<int64_t>(n) * a.src_sN;
+    T og0 = T(0), og1 = T(0), og2 = T(0);
+    for (int64_t c0 = 0; c0 < C; c0 += CB) {
+      const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+      const S* sp = src_n + c0 * a.src_sC;
+      const S* wp = wsrc_n + c0 * a.src_sC;
+      T* opc = do_a ? outs_n + c0 * a.out_sC : nullptr;
+      // interpolants of src (yv) and W (dv) and their spatial derivatives
+      T yv[CB], yx[CB], yy[CB], yz[CB], dv[CB], dxg[CB], dyg[CB], dzg[CB];
+#pragma unroll
+      PP_CB { yv[cb] = yx[cb] = yy[cb] = yz[cb] = dv[cb] = dxg[cb] = dyg[cb] = dzg[cb] = T(0); }
+#pragma unroll (OuterUnroll<ORD, NZ>::value)
+      for (int k = 0; k < NZ; ++k) {
+        if (k < tz) {
+          T pyw[CB], pygx[CB], pygy[CB], pdw[CB], pdgx[CB], pdgy[CB];
+#pragma unroll
+          PP_CB { pyw[cb] = pygx[cb] = pygy[cb] = pdw[cb] = pdgx[cb] = pdgy[cb] = T(0); }
+#pragma unroll
+          for (int j = 0; j < NY; ++j) {
+            if (j < ty) {
+              const I oyz = ay.os[j] + az.os[k];
+              T sx[CB], sdx[CB], wx[CB], wdx[CB];
+#pragma unroll
+              PP_CB { sx[cb] = sdx[cb] = wx[cb] = wdx[cb] = T(0); }
+#pragma unroll
+              for (int i = 0; i < NX; ++i) {
+                if (i < tx) {
+                  const I off = ax.os[i] + oyz;
+                  const bool valid = PP_TAP_VALID(i, j, k);
+#pragma unroll
+                  PP_CB {
+                    if (CB == 1 || cb < nc) {
+                      T v = ldg_acc(sp + (cb * a.src_sC + off));
+                      T u = ldg_acc(wp + (cb * a.src_sC + off));
+                      if (!valid) { v = T(0); u = T(0); }
+                      sx[cb] = fma(ax.w[i], v, sx[cb]);
+                      sdx[cb] = fma(ax.g[i], v, sdx[cb]);
+                      wx[cb] = fma(ax.w[i], u, wx[cb]);
+                      wdx[cb] = fma(ax.g[i], u, wdx[cb]);
+                    }
+                  }
+                }
+              }
+#pragma unroll
+              PP_CB {
+                pyw[cb] = fma(ay.w[j], sx[cb], pyw[cb]);
+                pygx[cb] = fma(ay.w[j], sdx[cb], pygx[cb]);
+                pygy[cb] = fma(ay.g[j], sx[cb], pygy[cb]);
+                pdw[cb] = fma(ay.w[j], wx[cb], pdw[cb]);
+                pdgx[cb] = fma(ay.w[j], wdx[cb], pdgx[cb]);
+                pdgy[cb] = fma(ay.g[j], wx[cb], pdgy[cb]);
+              }
+            }
+          }
+#pragma unroll
+          PP_CB {
+            yv[cb] = fma(az.w[k], pyw[cb], yv[cb]);
+            yx[cb] = fma(az.w[k], pygx[cb], yx[cb]);
+            yy[cb] = fma(az.w[k], pygy[cb], yy[cb]);
+            yz[cb] = fma(az.g[k], pyw[cb], yz[cb]);
+            dv[cb] = fma(az.w[k], pdw[cb], dv[cb]);
+            dxg[cb] = fma(az.w[k], pdgx[cb], dxg[cb]);
+            dyg[cb] = fma(az.w[k], pdgy[cb], dyg[cb]);
+            dzg[cb] = fma(az.g[k], pdw[cb], dzg[cb]);
+          }
+        }
+      }
+      // the values a separate pull / push-backward would have stored
+#pragma unroll
+      PP_CB {
+        yv[cb] = to_acc(from_acc<S>(yv[cb]));
+        dv[cb] = to_acc(from_acc<S>(dv[cb]));
+        if (CB == 1 || cb < nc) {
+          og0 += yv[cb] * dxg[cb] + dv[cb] * yx[cb];
+          og1 += yv[cb] * dyg[cb] + dv[cb] * yy[cb];
+          og2 += yv[cb] * dzg[cb] + dv[cb] * yz[cb];
+        }
+      }
+      if (do_a) {
+#pragma unroll (OuterUnroll<ORD, NZ>::value)
+        for (int k = 0; k < NZ; ++k) {
+          if (k < tz) {
+#pragma unroll
+            for (int j = 0; j < NY; ++j) {
+              if (j < ty) {
+                const T wyz = ay.w[j] * az.w[k];
+                const I oyz = ay.oo[j] + az.oo[k];
+#pragma unroll
+                for (int i = 0; i < NX; ++i) {
+                  if (i < tx && PP_TAP_VALID(i, j, k)) {
+                    const T wt = ax.w[i] * wyz;
+                    const I off = ax.oo[i] + oyz;
+#pragma unroll
+                    PP_CB {
+                      if (CB == 1 || cb < nc) {
+                        const T v = wt * dv[cb];
+                        if (v != T(0)) PP_SCATTER(off, v);
+                      }
+                    }
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    if (do_grad) {
+      T* g = static_cast<T*>(a.gg) + gvox;
+      g[0] = og0;
+      if (D > 1) g[a.gg_sD] = og1;
+      if (D > 2) g[2 * a.gg_sD] = og2;
+    }
+  }
 #undef PP_GRAD_GATHER
 #undef PP_CB
 #undef PP_SCATTER
 
 #undef PP_TAP_VALID
+}
+
+template <int D, int ORD, int CB, class S, int MODE, class I>
+__global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(const PPArgs a) {
+  // ---- sampling point (n, x, y, z) -------------------------------------
+  I sub[3] = {0, 0, 0};
+  I n = 0;
+  if (a.perm != nullptr) {
+    // explicit processing order (source-sorted): linear thread index
+    const int64_t t = (static_cast<int64_t>(blockIdx.x) * TILE_MID + threadIdx.y) * TILE_IN + threadIdx.x;
+    if (t >= a.nvox) return;
+    I v = static_cast<I>(__ldg(a.perm + t));
+    if (D > 2) { sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]); }
+    if (D > 1) { sub[1] = v % static_cast<I>(a.trgt_size[1]); v /= static_cast<I>(a.trgt_size[1]); }
+    sub[0] = v % static_cast<I>(a.trgt_size[0]);
+    n = v / static_cast<I>(a.trgt_size[0]);
+  } else {
+    // 2-D tile mapping over the grid
+    const I inner = static_cast<I>(a.trgt_size[D - 1]);
+    const I mid = D > 1 ? static_cast<I>(a.trgt_size[D - 2]) : I(1);
+    const I ntile = (inner + TILE_IN - 1) / TILE_IN;
+    const I outer_idx = static_cast<I>(blockIdx.x) / ntile;
+    const I ii = (static_cast<I>(blockIdx.x) - outer_idx * ntile) * TILE_IN + static_cast<I>(threadIdx.x);
+    const I mm = static_cast<I>(blockIdx.y) * TILE_MID + static_cast<I>(threadIdx.y);
+    if (ii >= inner || mm >= mid) return;
+    if (D == 3) {
+      sub[2] = ii; sub[1] = mm;
+      sub[0] = outer_idx % static_cast<I>(a.trgt_size[0]);
+      n = outer_idx / static_cast<I>(a.trgt_size[0]);
+    } else if (D == 2) {
+      sub[1] = ii; sub[0] = mm; n = outer_idx;
+    } else {
+      sub[0] = ii; n = outer_idx;
+    }
+  }
+
+  pp_point<D, ORD, CB, S, MODE, I>(a, sub, n);
 }
 
 template <int D, int ORD, int CB, class S, int MODE, class I>

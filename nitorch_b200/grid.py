@@ -138,6 +138,26 @@ class GridPush(torch.autograd.Function):
         return grad_input, grad_grid, None, None, None, None
 
 
+class GridPullPush(torch.autograd.Function):
+    """push(pull(input, grid), grid) as one op: one pass forward, one pass
+    backward.  Not in the reference, where it is GridPull then GridPush."""
+
+    @staticmethod
+    def forward(ctx, input, grid, interpolation, bound, extrapolate):
+        opt = _opt(bound, interpolation, extrapolate)
+        output = _spatial.grid_pull_push(input, grid, *opt)
+        ctx.opt = opt
+        ctx.save_for_backward(input, grid)
+        return output
+
+    @staticmethod
+    def backward(ctx, grad):
+        var = ctx.saved_tensors
+        grads = _spatial.grid_pull_push_backward(grad, *var, *ctx.opt)
+        grad_input, grad_grid = _unpack(ctx, grads)
+        return grad_input, grad_grid, None, None, None
+
+
 class GridCount(torch.autograd.Function):
 
     @staticmethod

@@ -38,7 +38,7 @@ from .enums import BoundType, InterpolationType
 __all__ = ["grid_pull", "grid_pull_backward", "grid_push", "grid_push_backward",
            "grid_count", "grid_count_backward", "grid_grad", "grid_grad_backward",
            "BoundType", "InterpolationType", "set_deterministic", "get_deterministic",
-           "set_sample_order", "sample_order"]
+           "set_sample_order", "sample_order", "grid_pull_push", "grid_pull_push_backward"]
 
 _FLOATS = (torch.float32, torch.float64, torch.bfloat16, torch.float16)
 _deterministic = bool(int(os.environ.get("PP_DETERMINISTIC", "0") or "0"))
@@ -428,6 +428,59 @@ def grid_grad_backward(grad, input, grid, bound, interpolation, extrapolate):
             ctypes.byref(_lib.desc(grad)), ctypes.byref(_lib.desc(input)),
             ctypes.byref(_lib.desc(g)), _lib.ref(_lib.desc(gi)), _lib.ref(_lib.desc(gg)),
             ctypes.byref(opt), _lib.stream_of(input), _wsptr(ws), nws))
+    out = []
+    if gi is not None:
+        out.append(gi)
+    if gg is not None:
+        out.append(gg.to(grid.dtype))
+    return out
+
+
+# --------------------------------------------------------------------- #
+# fused push(pull(.)) -- the normal operator P^T P                      #
+# --------------------------------------------------------------------- #
+
+def grid_pull_push(input, grid, bound, interpolation, extrapolate):
+    """push(pull(input, grid), grid) onto the input's lattice in one pass:
+    the result of grid_pull followed by grid_push with the input's spatial
+    shape (up to summation order).  Not in the reference."""
+    _check_pair(input, grid)
+    _check_opts(bound, interpolation)
+    _require_cuda(input)
+    L = _lib.load()
+    g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, input.shape[2:])
+    out = torch.empty_like(input, memory_format=torch.contiguous_format)
+    ws, nws = _workspace(out)
+    with _On(input):
+        _lib.check(L.pp_grid_pull_push(ctypes.byref(_lib.desc(input)), ctypes.byref(_lib.desc(g)),
+                                       ctypes.byref(_lib.desc(out)), ctypes.byref(opt), _lib.stream_of(input),
+                                       _wsptr(ws), nws))
+    return out
+
+
+def grid_pull_push_backward(grad, input, grid, bound, interpolation, extrapolate):
+    """Gradients of grid_pull_push w.r.t. the input (P^T P grad: the operator
+    is self-adjoint) and the grid, as requested by `requires_grad` (same
+    conventions as grid_pull_backward)."""
+    _check_pair(input, grid)
+    _check_opts(bound, interpolation)
+    _require_cuda(input)
+    L = _lib.load()
+    g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, input.shape[2:])
+    if grad.stride() != input.stride():
+        # the fused backward reads grad with the input's layout
+        grad = torch.empty_strided(input.shape, input.stride(), dtype=grad.dtype,
+                                   device=grad.device).copy_(grad)
+    gi = torch.empty_like(input, memory_format=torch.contiguous_format) if input.requires_grad else None
+    gg = torch.empty(g.shape, dtype=g.dtype, device=g.device) if grid.requires_grad else None
+    ws, nws = _workspace(gi) if gi is not None else (None, 0)
+    with _On(input):
+        _lib.check(L.pp_grid_pull_push_backward(
+            ctypes.byref(_lib.desc(grad)), ctypes.byref(_lib.desc(input)), ctypes.byref(_lib.desc(g)),
+            _lib.ref(_lib.desc(gi)), _lib.ref(_lib.desc(gg)), ctypes.byref(opt), _lib.stream_of(input),
+            _wsptr(ws), nws))
     out = []
     if gi is not None:
         out.append(gi)
