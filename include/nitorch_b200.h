@@ -194,6 +194,50 @@ PP_API int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32
 PP_API int pp_sample_order_noalloc(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
                                    void* stream);
 
+/* ---- Batched launches (no counterpart in the reference, which takes one
+ * tensor per call: nitorch/_C/src/pushpull.cpp:76-327) --------------------
+ * Many independent 3-D volumes (uneven shapes, one isotropic order 0-3 per
+ * volume, float32 or bfloat16 images shared by all entries, float32 grids)
+ * run one mode in a few launches: one per group of volumes with the same
+ * (order, channel block), each carrying up to 80 volumes' arguments.
+ * Tensors per mode (images (1, C, X, Y, Z), grids (1, X, Y, Z, 3); "grid
+ * shaped" = the grid's spatial shape; scatter outputs contiguous float32,
+ * zero-filled by pp_batch_run):
+ *   PP_BATCH_PULL          src -> out (grid shaped, image dtype)
+ *   PP_BATCH_PUSH          trgt (grid shaped) -> out (scatter, shape of out)
+ *   PP_BATCH_PUSH_BACKWARD src = d loss/d push output, trgt = pushed values
+ *                          -> out = d loss/d values (grid shaped, optional),
+ *                             gg = d loss/d grid (optional)
+ *   PP_BATCH_PULL_BACKWARD src = pulled image, trgt = d loss/d pulled
+ *                          -> out = d loss/d image (scatter, optional), gg
+ *   PP_BATCH_PULL_PUSH     src -> out = push(pull(src)) (scatter, src shaped)
+ *   PP_BATCH_PULL_PUSH_BACKWARD src, trgt = d loss/d out laid out like src
+ *                          -> out = d loss/d src (scatter, optional), gg
+ * opt.sample_order (optional) is read when the plan runs.  Deterministic
+ * mode is not available here. */
+#define PP_BATCH_PULL 0
+#define PP_BATCH_PUSH 2
+#define PP_BATCH_PUSH_BACKWARD 4
+#define PP_BATCH_PULL_BACKWARD 5
+#define PP_BATCH_PULL_PUSH 7
+#define PP_BATCH_PULL_PUSH_BACKWARD 8
+
+typedef struct pp_batch_entry {
+  pp_tensor src, trgt, grid, out, gg; /* unused: data = NULL */
+  pp_options opt;
+} pp_batch_entry;
+
+/* Host bytes of a plan for `nvol` volumes. */
+PP_API size_t pp_batch_plan_bytes(int32_t nvol);
+/* Validates the entries and writes a plan into `plan` (host memory of
+ * pp_batch_plan_bytes(nvol) bytes, owned by the caller).  ctas = 0: one CTA
+ * per 256 sampling points; ctas > 0: that many persistent CTAs.  The
+ * tensors must stay alive and in place while the plan is used. */
+PP_API int pp_batch_plan(const pp_batch_entry* entries, int32_t nvol, int32_t mode, int32_t ctas,
+                         void* plan, size_t plan_bytes);
+/* Enqueues the plan's zero fills and launches on `stream`. */
+PP_API int pp_batch_run(const void* plan, void* stream);
+
 /* interpol.coeff.spline_coeff (vendored: _ts/coeff.py:285-310):
  * interpolating B-spline coefficients along one axis of `input`, written to
  * `out` (same sizes; may alias `input` for in-place).  `bound` uses the

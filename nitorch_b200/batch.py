@@ -1,0 +1,311 @@
+"""Many volumes of uneven shapes in a few launches per mode.
+
+nitorch's backend processes one tensor per call; training and registration
+loops over many subjects then pay a launch (and a Python round trip) per
+volume and per op.  Here a batch of 3-D volumes -- any shapes, any channel
+count, isotropic orders 0-3, float32 or bfloat16 images -- goes through one
+launch per (order, channel block) group and mode (pull, push, their
+backward passes, or the fused pull-push and its backward), driven by a host
+plan (``pp_batch_plan`` / ``pp_batch_run`` in ``include/nitorch_b200.h``)
+whose per-volume arguments travel as kernel parameters.
+
+`PullPushBatch` is the pull -> push -> <z, w> -> backward step of the
+batched benchmark configuration, on static buffers ("arenas"), so the whole
+step -- per-volume sample ordering, the batched launches and the loss -- can
+be captured once in a CUDA graph and replayed.  By default it runs the fused
+normal operator (two batched passes per step); `fused=False` runs the four
+separate passes of the two-call chain.  `Autotuner` picks the launch shape
+and the sample order per (orders, dtype, channel mix, batch size) key and
+caches the choice on disk.
+
+`plan_shards` partitions a batch over ranks (longest processing time first
+on points x channels); the volumes are independent, so multi-GPU runs need
+no collective on the data path.
+"""
+import ctypes
+import gc
+import json
+import os
+import time
+
+import torch
+
+from . import _lib
+from .enums import BoundType
+
+
+def _entry(src=None, trgt=None, grid=None, out=None, gg=None, opt=None):
+    e = _lib.PPBatchEntry()
+    for name, t in (("src", src), ("trgt", trgt), ("grid", grid), ("out", out), ("gg", gg)):
+        if t is not None:
+            setattr(e, name, _lib.desc(t))
+    e.opt = opt
+    return e
+
+
+class BatchPlan:
+    """A plan of one batched mode over fixed tensors.  The tensors (and the
+    sample orders named in the options) must stay alive and in place while
+    the plan is used; `run` only enqueues work (graph-capturable)."""
+
+    def __init__(self, mode, entries, ctas=0, device=None):
+        L = _lib.load()
+        n = len(entries)
+        arr = (_lib.PPBatchEntry * n)(*entries)
+        nbytes = L.pp_batch_plan_bytes(n)
+        self.device = torch.device(device or "cuda")
+        self.buf = ctypes.create_string_buffer(nbytes)
+        self.mode = mode
+        _lib.check(L.pp_batch_plan(arr, n, mode, int(ctas), ctypes.cast(self.buf, ctypes.c_void_p), nbytes))
+
+    def run(self):
+        L = _lib.load()
+        stream = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.check(L.pp_batch_run(ctypes.cast(self.buf, ctypes.c_void_p), stream))
+
+
+def _arena(sizes, dtype, device):
+    """One flat buffer and per-volume views of the given shapes."""
+    total = sum(int(torch.Size(s).numel()) for s in sizes)
+    flat = torch.empty(total, dtype=dtype, device=device)
+    views, off = [], 0
+    for s in sizes:
+        n = int(torch.Size(s).numel())
+        views.append(flat[off:off + n].view(s))
+        off += n
+    return flat, views
+
+
+class PullPushBatch:
+    """Batched step: for every volume i,
+        y_i = pull(x_i, g_i);  z_i = push(y_i, g_i);  loss = sum_i <z_i, w_i>
+    and the gradients d loss / d x_i (float32) and d loss / d g_i.
+
+    shapes: list of 3-D spatial shapes; channels: list of C; orders: list of
+    isotropic orders (0-3).  Images are `dtype` (float32 or bfloat16); grids,
+    scatter outputs and gradients float32.  Inputs live in the arenas
+    `x`, `grid`, `w` (write them in place, e.g. `batch.x[i].copy_(...)`).
+    With `fused` (default) y_i is never stored: one pass computes z_i and one
+    pass the gradients; otherwise `y`, `dy` and the two grid-gradient terms
+    are kept in their own arenas.
+    """
+
+    def __init__(self, shapes, channels, orders, bound="dct2", extrapolate=False,
+                 dtype=torch.float32, device=None, sorted_order=True, ctas=0, fused=True):
+        self.device = torch.device(device or "cuda")
+        self.n = len(shapes)
+        self.shapes = [tuple(int(v) for v in s) for s in shapes]
+        self.channels = [int(c) for c in channels]
+        self.orders = [int(o) for o in orders]
+        self.dtype = dtype
+        self.sorted_order = bool(sorted_order)
+        self.ctas = int(ctas)
+        self.fused = bool(fused)
+        self.bound = int(BoundType[bound] if isinstance(bound, str) else bound)
+        self.extrapolate = int(extrapolate)
+        img = [(1, c, *s) for c, s in zip(self.channels, self.shapes)]
+        grd = [(1, *s, 3) for s in self.shapes]
+        dev = self.device
+        self.x_flat, self.x = _arena(img, dtype, dev)
+        self.grid_flat, self.grid = _arena(grd, torch.float32, dev)
+        self.w_flat, self.w = _arena(img, dtype, dev)
+        self.z_flat, self.z = _arena(img, torch.float32, dev)
+        self.dx_flat, self.dx = _arena(img, torch.float32, dev)
+        if not self.fused:
+            self.y_flat, self.y = _arena(img, dtype, dev)
+            self.dy_flat, self.dy = _arena(img, dtype, dev)
+            self.dg1_flat, self.dg1 = _arena(grd, torch.float32, dev)
+            self.dg2_flat, self.dg2 = _arena(grd, torch.float32, dev)
+        self.dgrid_flat, self.dgrid = _arena(grd, torch.float32, dev)
+        self.loss = torch.zeros((), dtype=torch.float32, device=dev)
+        self.perm_flat, self.perm = _arena([(int(torch.Size(s).numel()),) for s in self.shapes], torch.int32, dev)
+        L = _lib.load()
+        ws = 0
+        for g, s in zip(self.grid, self.shapes):
+            src = (ctypes.c_int64 * 3)(*s)
+            ws = max(ws, L.pp_sample_order_workspace_bytes(ctypes.byref(_lib.desc(g)), src))
+        self.sort_ws = torch.empty(max(ws, 256), dtype=torch.uint8, device=dev)
+        self._build_plans()
+        self.graph = None
+
+    # -- plans ---------------------------------------------------------------
+    def _opt(self, i):
+        perm = self.perm[i].data_ptr() if self.sorted_order else None
+        return _lib.options([self.bound], [self.orders[i]], self.extrapolate, 0, perm)
+
+    def _build_plans(self):
+        B = _lib
+        if self.fused:
+            ents = {"pp": [], "pp_bwd": []}
+            for i in range(self.n):
+                o = self._opt(i)
+                ents["pp"].append(_entry(src=self.x[i], grid=self.grid[i], out=self.z[i], opt=o))
+                ents["pp_bwd"].append(_entry(src=self.x[i], trgt=self.w[i], grid=self.grid[i], out=self.dx[i],
+                                             gg=self.dgrid[i], opt=o))
+            modes = {"pp": B.PP_BATCH_PULL_PUSH, "pp_bwd": B.PP_BATCH_PULL_PUSH_BACKWARD}
+        else:
+            ents = {m: [] for m in ("pull", "push", "push_bwd", "pull_bwd")}
+            for i in range(self.n):
+                o = self._opt(i)
+                ents["pull"].append(_entry(src=self.x[i], grid=self.grid[i], out=self.y[i], opt=o))
+                ents["push"].append(_entry(trgt=self.y[i], grid=self.grid[i], out=self.z[i], opt=o))
+                ents["push_bwd"].append(_entry(src=self.w[i], trgt=self.y[i], grid=self.grid[i], out=self.dy[i],
+                                               gg=self.dg1[i], opt=o))
+                ents["pull_bwd"].append(_entry(src=self.x[i], trgt=self.dy[i], grid=self.grid[i], out=self.dx[i],
+                                               gg=self.dg2[i], opt=o))
+            modes = {"pull": B.PP_BATCH_PULL, "push": B.PP_BATCH_PUSH,
+                     "push_bwd": B.PP_BATCH_PUSH_BACKWARD, "pull_bwd": B.PP_BATCH_PULL_BACKWARD}
+        self.plans = {k: BatchPlan(modes[k], ents[k], ctas=self.ctas, device=self.device) for k in ents}
+
+    # -- the step --------------------------------------------------------------
+    def _sort(self):
+        L = _lib.load()
+        stream = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        for i in range(self.n):
+            src = (ctypes.c_int64 * 3)(*self.shapes[i])
+            _lib.check(L.pp_sample_order(ctypes.byref(_lib.desc(self.grid[i])), src,
+                                         ctypes.c_void_p(self.perm[i].data_ptr()),
+                                         ctypes.c_void_p(self.sort_ws.data_ptr()), self.sort_ws.numel(), stream))
+
+    def _loss(self):
+        if self.dtype == torch.float32:
+            torch.dot(self.z_flat, self.w_flat, out=self.loss)
+        else:
+            self.loss.copy_((self.z_flat * self.w_flat.float()).sum())
+
+    def step_eager(self):
+        """One step without the graph; returns the loss tensor (device)."""
+        if self.sorted_order:
+            self._sort()
+        if self.fused:
+            self.plans["pp"].run()
+            self._loss()
+            self.plans["pp_bwd"].run()
+            return self.loss
+        self.plans["pull"].run()
+        self.plans["push"].run()
+        self._loss()
+        self.plans["push_bwd"].run()
+        self.plans["pull_bwd"].run()
+        torch.add(self.dg1_flat, self.dg2_flat, out=self.dgrid_flat)
+        return self.loss
+
+    def capture(self):
+        """Capture one step in a CUDA graph (after a warm-up step)."""
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self.step_eager()
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.step_eager()
+        return self
+
+    def step(self):
+        if self.graph is None:
+            return self.step_eager()
+        self.graph.replay()
+        return self.loss
+
+    def release(self):
+        """Drop the graph and the buffers (the object is unusable after)."""
+        self.graph = None
+        self.plans = {}
+        for k in list(vars(self)):
+            if isinstance(getattr(self, k), (torch.Tensor, list)):
+                setattr(self, k, None)
+
+    def points(self):
+        return sum(int(torch.Size(s).numel()) for s in self.shapes)
+
+
+# ---------------------------------------------------------------------------
+# autotuner
+# ---------------------------------------------------------------------------
+class Autotuner:
+    """Chooses the launch shape (persistent CTAs per SM, or one CTA per work
+    item) and the sample order of a batch by timing candidate
+    configurations of the captured step, and caches the winner on disk (JSON
+    at $PP_AUTOTUNE_CACHE, default ~/.cache/nitorch_b200/autotune.json),
+    keyed by GPU, dtype, the set of orders, the channel mix, the batch size
+    and the step form (fused or chain)."""
+
+    # (persistent CTAs per SM, 0 = one CTA per work item) x sample order
+    CANDIDATES = [(ctas_per_sm, srt) for srt in (True, False) for ctas_per_sm in (0, 4)]
+
+    def __init__(self, path=None):
+        self.path = path or os.environ.get("PP_AUTOTUNE_CACHE") or os.path.join(
+            os.path.expanduser("~"), ".cache", "nitorch_b200", "autotune.json")
+        try:
+            with open(self.path) as f:
+                self.cache = json.load(f)
+        except (OSError, ValueError):
+            self.cache = {}
+
+    @staticmethod
+    def key(shapes, channels, orders, dtype, device, fused=True):
+        name = torch.cuda.get_device_name(device)
+        nb = 1 << max(0, (len(shapes) - 1).bit_length())
+        cmix = ",".join(str(c) for c in sorted(set(channels)))
+        omix = ",".join(str(o) for o in sorted(set(orders)))
+        return f"{name}|{dtype}|o{omix}|c{cmix}|n{nb}|{'fused' if fused else 'chain'}"
+
+    def choose(self, shapes, channels, orders, dtype=torch.float32, device=None, bound="dct2",
+               extrapolate=False, reps=3, init=None, fused=True):
+        """Returns (ctas, sorted_order, timings).  `init(batch)` fills the
+        input arenas of a candidate batch before it is timed."""
+        device = torch.device(device or "cuda")
+        k = self.key(shapes, channels, orders, dtype, device, fused)
+        if k in self.cache:
+            c = self.cache[k]
+            return c["ctas"], c["sorted"], c.get("ms", {})
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+        timings = {}
+        best = None
+        for per_sm, srt in self.CANDIDATES:
+            b = PullPushBatch(shapes, channels, orders, bound, extrapolate, dtype, device, srt, per_sm * sms, fused)
+            if init is not None:
+                init(b)
+            b.capture()
+            b.step()
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                b.step()
+            torch.cuda.synchronize(device)
+            ms = (time.perf_counter() - t0) * 1e3 / reps
+            timings[f"{per_sm}x{'sorted' if srt else 'natural'}"] = round(ms, 3)
+            if best is None or ms < best[0]:
+                best = (ms, per_sm * sms, srt)
+            b.release()
+            del b
+            gc.collect()
+            torch.cuda.empty_cache()
+        self.cache[k] = {"ctas": best[1], "sorted": best[2], "ms": timings}
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            with open(self.path, "w") as f:
+                json.dump(self.cache, f, indent=1)
+        except OSError:
+            pass
+        return best[1], best[2], timings
+
+
+# ---------------------------------------------------------------------------
+# multi-GPU sharding
+# ---------------------------------------------------------------------------
+def plan_shards(costs, world):
+    """Longest-processing-time-first partition of independent volumes over
+    `world` ranks.  costs: per-volume work (points x channels).  Returns a
+    list of index lists, one per rank, and their loads."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    shards = [[] for _ in range(world)]
+    loads = [0] * world
+    for i in order:
+        r = min(range(world), key=lambda k: (loads[k], k))
+        shards[r].append(i)
+        loads[r] += costs[i]
+    for s in shards:
+        s.sort()
+    return shards, loads

@@ -153,4 +153,10 @@ inline int store_f32(const float* acc, const pp_tensor* t, cudaStream_t st) {
   return cuda_check(cudaGetLastError(), "16-bit store");
 }
 
+// Defined in pp_capi.cu, shared with the batched entry points.
+int read_options(const pp_options* o, int D, int bound[3], int order[3]);
+void set_image(const pp_tensor* t, int D, int64_t& sN, int64_t& sC, int64_t s[3]);
+void set_grid(const pp_tensor* t, int D, int64_t& sN, int64_t s[3], int64_t& sD);
+bool fits32(int64_t v);
+
 }  // namespace ppc

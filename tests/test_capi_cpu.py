@@ -86,3 +86,39 @@ def test_workspace_query():
     assert n >= 2 * 8 * 8 * 8 * 4 and n % 256 == 0
     d = _lib.desc(torch.zeros((1, 2, 8, 8, 8), dtype=torch.float32))
     assert L.pp_push_workspace_bytes(ctypes.byref(d), 0) == 0
+
+
+def test_batch_plan_validation_on_host():
+    """pp_batch_plan validates and plans on the host only (no CUDA call)."""
+    from nitorch_b200.batch import _entry
+    L = _lib.load()
+    x = torch.zeros(1, 2, 6, 5, 4)
+    g = torch.zeros(1, 6, 5, 4, 3)
+    z = torch.zeros(1, 2, 6, 5, 4)
+    w = torch.zeros(1, 2, 6, 5, 4)
+    dx = torch.zeros(1, 2, 6, 5, 4)
+    dg = torch.zeros(1, 6, 5, 4, 3)
+    nb = L.pp_batch_plan_bytes(2)
+    buf = ctypes.create_string_buffer(nb)
+    p = ctypes.cast(buf, ctypes.c_void_p)
+
+    def plan(mode, ents, nbytes=nb):
+        arr = (_lib.PPBatchEntry * len(ents))(*ents)
+        return L.pp_batch_plan(arr, len(ents), mode, 0, p, nbytes)
+
+    ok = _entry(src=x, grid=g, out=z, opt=_lib.options([2], [3], 0))
+    assert plan(_lib.PP_BATCH_PULL_PUSH, [ok, ok]) == _lib.PP_OK
+    bwd = _entry(src=x, trgt=w, grid=g, out=dx, gg=dg, opt=_lib.options([2], [1], 0))
+    assert plan(_lib.PP_BATCH_PULL_PUSH_BACKWARD, [bwd, ok]) == _lib.PP_ERR_ARG  # second entry lacks trgt
+    assert plan(_lib.PP_BATCH_PULL_PUSH_BACKWARD, [bwd]) == _lib.PP_OK
+    assert plan(_lib.PP_BATCH_PULL_PUSH, [ok], nbytes=16) == _lib.PP_ERR_WORKSPACE
+    high = _entry(src=x, grid=g, out=z, opt=_lib.options([2], [5], 0))
+    assert plan(_lib.PP_BATCH_PULL_PUSH, [high]) == _lib.PP_ERR_UNSUPPORTED
+    det = _entry(src=x, grid=g, out=z, opt=_lib.options([2], [1], 0, flags=_lib.PP_DETERMINISTIC))
+    assert plan(_lib.PP_BATCH_PULL_PUSH, [det]) == _lib.PP_ERR_UNSUPPORTED
+    small = _entry(src=x, grid=g, out=torch.zeros(1, 2, 6, 5, 3), opt=_lib.options([2], [1], 0))
+    assert plan(_lib.PP_BATCH_PULL_PUSH, [small]) == _lib.PP_ERR_ARG
+    half = _entry(src=x, grid=g, out=z.bfloat16(), opt=_lib.options([2], [1], 0))
+    assert plan(_lib.PP_BATCH_PULL_PUSH, [half]) == _lib.PP_ERR_DTYPE
+    assert plan(3, [ok]) == _lib.PP_ERR_UNSUPPORTED  # count is not a batched mode
+    assert L.pp_batch_run(None, None) == _lib.PP_ERR_ARG
