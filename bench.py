@@ -13,12 +13,16 @@ Metric: output-grid voxels per second (Gvox/s) of that step.
 --impl b200 (default) prints one JSON line with the device-timed value, the
 end-to-end value through the public API with host buffers (`e2e`), the
 roofline of the dominant kernel, the CPU baseline (the reference's own C++
-backend on a bounded sample), clocks and kernel-launch counts.
+backend on a bounded sample), clocks and kernel-launch counts; `fused`
+reports the same step through the fused pull_push operator, and `batched`
+the config-4 workload (64 uneven volumes, float32 and bfloat16) as one
+captured batched step against the per-call loop.
 --impl reference times the reference's CPU implementation of the same step
 on the host cores (bounded sample) and prints the same metric.
-With N > 1 (torchrun), every rank runs an independent replica of the step
-(the workload does not shard; "replicas only"); value = all ranks' voxels
-/ max-over-ranks time.
+With N > 1 (torchrun), every rank runs an independent replica of the
+single-volume step (it does not shard; "replicas only"); value = all ranks'
+voxels / max-over-ranks time.  The batched volumes are sharded over the
+ranks (LPT on points x channels), timed as max over ranks.
 """
 import argparse
 import json
@@ -107,18 +111,20 @@ class OpTimer:
     """Wraps the nitorch_b200 entry points the step calls so that each call
     is bracketed by CUDA events on the launching (current) stream."""
 
-    def __init__(self):
+    CHAIN = {"grid_pull": "pull_fwd", "grid_push": "push_fwd", "grid_push_backward": "push_bwd",
+             "grid_pull_backward": "pull_bwd", "spline_coeff_nd": "prefilter"}
+    FUSED = {"grid_pull_push": "pp_fwd", "grid_pull_push_backward": "pp_bwd", "spline_coeff_nd": "prefilter"}
+
+    def __init__(self, labels=None):
+        self.labels = labels or self.CHAIN
         self.events = {}
         self.enabled = False
         self._orig = []
 
     def install(self):
         from nitorch_b200 import coeff, spatial
-        for mod, name, label in ((spatial, "grid_pull", "pull_fwd"),
-                                 (spatial, "grid_push", "push_fwd"),
-                                 (spatial, "grid_push_backward", "push_bwd"),
-                                 (spatial, "grid_pull_backward", "pull_bwd"),
-                                 (coeff, "spline_coeff_nd", "prefilter")):
+        for name, label in self.labels.items():
+            mod = coeff if name == "spline_coeff_nd" else spatial
             fn = getattr(mod, name)
             self._orig.append((mod, name, fn))
             setattr(mod, name, self._wrap(fn, label))
@@ -153,6 +159,7 @@ class OpTimer:
 def algo_bytes(label, s, C):
     return {"pull_fwd": 12 + 2 * s * C, "push_fwd": 12 + 2 * s * C,
             "push_bwd": 24 + 3 * s * C, "pull_bwd": 24 + 3 * s * C,
+            "pp_fwd": 12 + 2 * s * C, "pp_bwd": 24 + 3 * s * C,
             "prefilter": 3 * 2 * s * C}[label]
 
 
@@ -185,123 +192,274 @@ def flush_l2(buf):
     buf.zero_()
 
 
-def run_b200(args, rank, world, device):
+def step_fused(x, grid, w):
+    """The same step through the fused normal operator (one pass forward,
+    one pass backward); same outputs as `step` up to summation order."""
+    import nitorch_b200 as nb
+    from nitorch_b200 import spatial
+    spatial._orders.clear()
+    x.grad = None
+    grid.grad = None
+    z = nb.pull_push(x, grid, ORDER, BOUND, EXTRAP, prefilter=True)
+    loss = (z * w).sum()
+    loss.backward()
+    return loss
+
+
+def timed_steps(fn, args, world, device, l2buf, timer=None, clocks=None, steps=None):
+    """Device time (ms, max over ranks) of `steps` calls of fn(), L2 flushed
+    between steps outside the timed windows; the library's kernel launches
+    and the clock record of the window."""
     from nitorch_b200 import _lib
+    steps = steps or args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    launches0 = _lib.kernel_launches()
+    if timer:
+        timer.enabled = True
+    for i in range(steps):
+        flush_l2(l2buf)
+        starts[i].record()
+        fn()
+        ends[i].record()
+    if timer:
+        timer.enabled = False
+    torch.cuda.synchronize()
+    launches = _lib.kernel_launches() - launches0
+    clk = clocks.stop() if clocks else None
+    if world > 1:
+        torch.distributed.barrier()
+    total_ms = float(np.sum([s.elapsed_time(e) for s, e in zip(starts, ends)]))
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    return total_ms, launches, clk
+
+
+def roofline(ops, labels, nvox, C, ms_per_step, traffic):
+    hbm, src = peaks()
+    dom = max(ops, key=lambda k: ops[k]["total_ms"])
+    per = algo_bytes(dom, 4, C) * nvox
+    achieved = per / (ops[dom]["avg_ms"] * 1e-3) / 1e9
+    step_bytes = sum(algo_bytes(k, 4, C) for k in labels) * nvox
+    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
+            "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": src,
+            "algorithmic_bytes_per_launch": per, "traffic": traffic,
+            "step_frac": round(step_bytes / (ms_per_step * 1e-3) / 1e9 / hbm, 4)}
+
+
+def run_b200(args, rank, world, device):
     size, C = args.size, 3
     x, grid, w, oob = make_inputs(size, C, device)
     x.requires_grad_(True)
     grid.requires_grad_(True)
     nvox = size ** 3
     l2buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
-
-    for _ in range(args.warmup):
-        step(x, grid, w)
-    torch.cuda.synchronize()
-
-    timer = OpTimer()
-    timer.install()
-    clocks = ClockSampler(device.index or 0) if rank == 0 else None
-    if clocks:
-        clocks.start()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    launches0 = _lib.kernel_launches()
-    timer.enabled = True
-    for i in range(args.steps):
-        flush_l2(l2buf)                 # between timed steps, outside the timed window
-        starts[i].record()
-        step(x, grid, w)
-        ends[i].record()
-    timer.enabled = False
-    torch.cuda.synchronize()
-    launches = _lib.kernel_launches() - launches0
-    if world > 1:
-        torch.distributed.barrier()
-    clk = clocks.stop() if clocks else None
-    timer.uninstall()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = float(np.sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    value = world * nvox * args.steps / (total_ms * 1e-3) / 1e9
-
-    ops = timer.summary()
-
-    # ---- end to end: public API, host buffers, H2D inputs + D2H loss -------
     xh = x.detach().cpu().pin_memory()
     gh = grid.detach().cpu().pin_memory()
     wh = w.detach().cpu().pin_memory()
     lh = torch.empty((), dtype=torch.float32).pin_memory()
-
-    def e2e_step():
-        xd = xh.to(device, non_blocking=True).requires_grad_(True)
-        gd = gh.to(device, non_blocking=True).requires_grad_(True)
-        wd = wh.to(device, non_blocking=True)
-        loss = step(xd, gd, wd)
-        lh.copy_(loss.detach(), non_blocking=True)
-        return lh
-
-    for _ in range(max(1, min(args.warmup, 3))):
-        e2e_step()
-    torch.cuda.synchronize()
-    e_s = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    e_e = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
-    for i in range(args.steps):
-        flush_l2(l2buf)
-        e_s[i].record()
-        e2e_step()
-        e_e[i].record()
-    torch.cuda.synchronize()
-    e2e_ms = float(np.sum([s.elapsed_time(e) for s, e in zip(e_s, e_e)]))
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * nvox * args.steps / (e2e_ms * 1e-3) / 1e9
     h2d = (xh.numel() + gh.numel() + wh.numel()) * 4
 
+    def measure(stepfn, labels, with_clocks, traffic):
+        for _ in range(args.warmup):
+            stepfn(x, grid, w)
+        torch.cuda.synchronize()
+        timer = OpTimer(labels)
+        timer.install()
+        clocks = ClockSampler(device.index or 0) if (rank == 0 and with_clocks) else None
+        total_ms, launches, clk = timed_steps(lambda: stepfn(x, grid, w), args, world, device, l2buf,
+                                              timer, clocks)
+        timer.uninstall()
+
+        # end to end: public API, host buffers, H2D inputs + D2H loss
+        def e2e_step():
+            xd = xh.to(device, non_blocking=True).requires_grad_(True)
+            gd = gh.to(device, non_blocking=True).requires_grad_(True)
+            wd = wh.to(device, non_blocking=True)
+            loss = stepfn(xd, gd, wd)
+            lh.copy_(loss.detach(), non_blocking=True)
+            return lh
+
+        for _ in range(max(1, min(args.warmup, 3))):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_ms, _, _ = timed_steps(e2e_step, args, world, device, l2buf)
+        ms_per_step = total_ms / args.steps
+        ops = timer.summary()
+        return {
+            "value": round(world * nvox * args.steps / (total_ms * 1e-3) / 1e9, 4),
+            "ms_per_step": round(ms_per_step, 4),
+            "e2e": {"value": round(world * nvox * args.steps / (e2e_ms * 1e-3) / 1e9, 4), "unit": "Gvox/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4},
+            "roofline": roofline(ops, [k for k in labels.values() if k != "prefilter"], nvox, C, ms_per_step,
+                                 traffic),
+            "ops": {k: {kk: round(vv, 4) if isinstance(vv, float) else vv for kk, vv in v.items()}
+                    for k, v in ops.items()},
+            "gpu_launches": int(launches),
+            "gpu_launches_per_step": round(launches / args.steps, 2),
+            "clocks": clk,
+        }
+
+    chain = measure(step, OpTimer.CHAIN, True, args.traffic)
+    fused = measure(step_fused, OpTimer.FUSED, False, None)
     if rank != 0:
         return None
 
-    # ---- roofline of the dominant op -----------------------------------------
-    hbm, src = peaks()
-    dom = max(ops, key=lambda k: ops[k]["total_ms"])
-    per = algo_bytes(dom, 4, C) * nvox
-    achieved = per / (ops[dom]["avg_ms"] * 1e-3) / 1e9
-    step_bytes = sum(algo_bytes(k, 4, C) for k in ("pull_fwd", "push_fwd", "push_bwd", "pull_bwd")) * nvox
-    roof = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
-            "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": src,
-            "algorithmic_bytes_per_launch": per, "traffic": args.traffic,
-            "step_frac": round(step_bytes / (ms_per_step * 1e-3) / 1e9 / hbm, 4)}
-
     line = {
-        "metric": METRIC, "value": round(value, 4), "unit": "Gvox/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "metric": METRIC, "value": chain["value"], "unit": "Gvox/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": chain["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded; smoothed N(0,1) image, smoothed displacement)",
         "config": {"workload": f"1x{C}x{size}^3 order-3 dct2 prefilter pull+push fwd+bwd (cfg2)",
+                   "api": "grid_pull -> grid_push (the nitorch call chain), autograd",
                    "voxels_per_step": nvox, "channels": C, "oob_fraction": round(oob, 4),
                    "l2": "flushed (256 MiB write) between timed steps; inputs > L2",
                    "parallelism": f"replicas x{world}"},
-        "e2e": {"value": round(e2e_value, 4), "unit": "Gvox/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": 4},
-        "roofline": roof,
-        "ops": {k: {kk: round(vv, 4) if isinstance(vv, float) else vv for kk, vv in v.items()}
-                for k, v in ops.items()},
-        "gpu_launches": int(launches),
-        "gpu_launches_per_step": round(launches / args.steps, 2),
-        "clocks": clk,
+        "e2e": chain["e2e"],
+        "roofline": chain["roofline"],
+        "ops": chain["ops"],
+        "gpu_launches": chain["gpu_launches"],
+        "gpu_launches_per_step": chain["gpu_launches_per_step"],
+        "clocks": chain["clocks"],
+        "fused": {"api": "pull_push (fused normal operator, same outputs), autograd",
+                  **{k: fused[k] for k in ("value", "ms_per_step", "e2e", "roofline", "ops", "gpu_launches",
+                                           "gpu_launches_per_step")}},
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.cpu_size, steps=2, warmup=1)
+    return line
+
+
+# ---------------------------------------------------------------------- #
+# batched configuration: many uneven volumes                              #
+# ---------------------------------------------------------------------- #
+def cfg4_volumes(n):
+    from nitorch_b200 import workloads
+    items = workloads.config4(n_volumes=n)
+    return [it[0] for it in items], [it[1] for it in items], [it[2] for it in items]
+
+
+def fill_cfg4(batch, seed=31):
+    """Seeded synthetic inputs drawn on the GPU: images U[0,1); grids =
+    identity + smooth displacement (coarse normal field, trilinear
+    upsampling, std 2 voxels)."""
+    g = torch.Generator(device=batch.device).manual_seed(seed)
+    for i, s in enumerate(batch.shapes):
+        batch.x[i].copy_(torch.rand(batch.x[i].shape, generator=g, device=batch.device))
+        batch.w[i].copy_(torch.randn(batch.w[i].shape, generator=g, device=batch.device))
+        coarse = tuple(max(4, v // 8) for v in s)
+        d = torch.randn((1, 3, *coarse), generator=g, device=batch.device)
+        d = torch.nn.functional.interpolate(d, size=s, mode="trilinear", align_corners=True)
+        d = d * (2.0 / d.std())
+        mesh = torch.stack(torch.meshgrid(*[torch.arange(n, dtype=torch.float32, device=batch.device)
+                                            for n in s], indexing="ij"), -1)
+        batch.grid[i].copy_(mesh[None] + d.movedim(1, -1))
+
+
+def plain_step(batch):
+    """The per-call form: the public API volume by volume, autograd (what a
+    loop over subjects does with nitorch's own functions)."""
+    import nitorch_b200 as nb
+    from nitorch_b200 import spatial
+    spatial._orders.clear()
+    loss = torch.zeros((), device=batch.device)
+    for i in range(batch.n):
+        x = batch.x[i].detach().requires_grad_(True)
+        g = batch.grid[i].detach().requires_grad_(True)
+        y = nb.grid_pull(x, g, batch.orders[i], "dct2", False)
+        z = nb.grid_push(y, g, None, batch.orders[i], "dct2", False)
+        li = (z.float() * batch.w[i].float()).sum()
+        li.backward()
+        loss = loss + li.detach()
+    return loss
+
+
+def run_batched(args, rank, world, device):
+    from nitorch_b200.batch import Autotuner, PullPushBatch, plan_shards
+    shapes, chans, orders = cfg4_volumes(args.batch_volumes)
+    costs = [int(np.prod(s)) * c for s, c in zip(shapes, chans)]
+    shards, _ = plan_shards(costs, world)
+    mine = shards[rank]
+    shapes_r = [shapes[i] for i in mine]
+    chans_r = [chans[i] for i in mine]
+    orders_r = [orders[i] for i in mine]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    total_points = sum(int(np.prod(s)) for s in shapes)
+    out = {"workload": f"cfg4: {len(shapes)} volumes, axes U{{96..256}}, C U{{1..4}}, orders 1/3 "
+                       "alternating, dct2; pull -> push -> <z,w> -> backward",
+           "points_per_step": total_points, "channels_total": int(sum(chans)),
+           "sharding": f"LPT over {world} rank(s), no collective on the data path"}
+    for dtype in (torch.float32, torch.bfloat16):
+        tag = "f32" if dtype == torch.float32 else "bf16"
+        tuner = Autotuner()
+        ctas, srt, tried = tuner.choose(shapes_r, chans_r, orders_r, dtype=dtype, device=device,
+                                        init=fill_cfg4)
+        b = PullPushBatch(shapes_r, chans_r, orders_r, dtype=dtype, device=device, sorted_order=srt, ctas=ctas)
+        fill_cfg4(b)
+        b.capture()
+        for _ in range(args.warmup):
+            b.step()
+        torch.cuda.synchronize(device)
+        ms_graph, launches, _ = timed_steps(b.step, args, world, device, flush, steps=args.batch_steps)
+        for _ in range(max(1, min(args.warmup, 2))):
+            plain_step(b)
+        torch.cuda.synchronize(device)
+        ms_plain, _, _ = timed_steps(lambda: plain_step(b), args, world, device, flush, steps=args.batch_steps)
+        res = {"batched_graph": {"value": round(total_points * args.batch_steps / (ms_graph * 1e-3) / 1e9, 4),
+                                 "unit": "Gvox/s", "ms_per_step": round(ms_graph / args.batch_steps, 3),
+                                 "gpu_launches_per_step": round(launches / args.batch_steps, 1)},
+               "plain_per_call": {"value": round(total_points * args.batch_steps / (ms_plain * 1e-3) / 1e9, 4),
+                                  "unit": "Gvox/s", "ms_per_step": round(ms_plain / args.batch_steps, 3)},
+               "speedup": round(ms_plain / ms_graph, 3),
+               "autotune": {"ctas": ctas, "sorted_order": srt, "candidates_ms": tried}}
+        if rank == 0 and dtype == torch.bfloat16 and not args.no_cpu_baseline:
+            res["error_vs_fp64_oracle"] = bf16_error(b)
+        out[tag] = res
+        b.release()
+        del b
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+    return out
+
+
+def bf16_error(b):
+    """Max relative error of the batched bfloat16 step's forward output z =
+    push(pull(x)) of the smallest volume against the FP64 CPU oracle chain
+    on the same stored (bf16) input."""
+    from oracle import oracle as O
+    i = min(range(b.n), key=lambda k: int(np.prod(b.shapes[k])) * b.channels[k])
+    b.step_eager()
+    torch.cuda.synchronize(b.device)
+    x = b.x[i].double().cpu().numpy()
+    g = b.grid[i].double().cpu().numpy()
+    ref = O.grid_push(O.grid_pull(x, g, [2], [b.orders[i]], 0), g, x.shape[2:], [2], [b.orders[i]], 0)
+    z = b.z[i].double().cpu().numpy()
+    err = float(np.abs(z - ref).max() / np.abs(ref).max())
+    return {"volume": list(b.shapes[i]), "channels": b.channels[i], "order": b.orders[i],
+            "push_of_pull_max_rel_err": err,
+            "bound": "2^-8 (one bf16 rounding of the pulled values; non-negative image) + 1e-5"}
+
+
+def run_all(args, rank, world, device):
+    import gc
+    line = run_b200(args, rank, world, device)
+    gc.collect()
+    torch.cuda.empty_cache()
+    if not args.no_batched:
+        from nitorch_b200 import _lib
+        l0 = _lib.kernel_launches()
+        b = run_batched(args, rank, world, device)
+        if line is not None:
+            b["gpu_launches"] = _lib.kernel_launches() - l0
+            line["batched"] = b
     return line
 
 
@@ -398,6 +556,9 @@ def main():
     ap.add_argument("--size", type=int, default=192)
     ap.add_argument("--cpu-size", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-volumes", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
     args = ap.parse_args()
@@ -418,7 +579,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=device)
     try:
-        line = run_b200(args, rank, world, device)
+        line = run_all(args, rank, world, device)
         if line is not None:
             print(json.dumps(line), flush=True)
     finally:
