@@ -407,14 +407,14 @@ def run_batched(args, rank, world, device):
         for _ in range(args.warmup):
             b.step()
         torch.cuda.synchronize(device)
-        ms_graph, launches, _ = timed_steps(b.step, args, world, device, flush, steps=args.batch_steps)
+        ms_graph, _, _ = timed_steps(b.step, args, world, device, flush, steps=args.batch_steps)
         for _ in range(max(1, min(args.warmup, 2))):
             plain_step(b)
         torch.cuda.synchronize(device)
         ms_plain, _, _ = timed_steps(lambda: plain_step(b), args, world, device, flush, steps=args.batch_steps)
         res = {"batched_graph": {"value": round(total_points * args.batch_steps / (ms_graph * 1e-3) / 1e9, 4),
                                  "unit": "Gvox/s", "ms_per_step": round(ms_graph / args.batch_steps, 3),
-                                 "gpu_launches_per_step": round(launches / args.batch_steps, 1)},
+                                 "gpu_launches_per_step": b.graph_launches},
                "plain_per_call": {"value": round(total_points * args.batch_steps / (ms_plain * 1e-3) / 1e9, 4),
                                   "unit": "Gvox/s", "ms_per_step": round(ms_plain / args.batch_steps, 3)},
                "speedup": round(ms_plain / ms_graph, 3),

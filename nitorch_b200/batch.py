@@ -127,6 +127,7 @@ class PullPushBatch:
         self.sort_ws = torch.empty(max(ws, 256), dtype=torch.uint8, device=dev)
         self._build_plans()
         self.graph = None
+        self.graph_launches = 0
 
     # -- plans ---------------------------------------------------------------
     def _opt(self, i):
@@ -198,8 +199,11 @@ class PullPushBatch:
             self.step_eager()
         torch.cuda.current_stream(self.device).wait_stream(s)
         self.graph = torch.cuda.CUDAGraph()
+        l0 = _lib.kernel_launches()
         with torch.cuda.graph(self.graph):
             self.step_eager()
+        # the library's kernels inside the graph: what each replay launches
+        self.graph_launches = _lib.kernel_launches() - l0
         return self
 
     def step(self):

@@ -3,6 +3,9 @@
 * ``load_compiled()``: the reference's own C++ CPU backend, compiled from the
   reference sources by ``oracle/build_ref.py`` into ``oracle/_ref/``
   (the module ``nitorch._C.spatial``).  Returns None when not built.
+* ``load_compiled_cuda()``: the same module built with the reference's CUDA
+  backend for sm_100a by ``oracle/build_ref_cuda.py`` (``oracle/_ref/cuda/``),
+  used to time the reference's own GPU kernels beside this library's.
 * ``load_ts_coeff()``: the reference's vendored prefilter
   ``nitorch/_C/_ts/coeff.py`` imported from the reference tree, when that
   tree is present (only in the development container, never on a GPU box).
@@ -16,9 +19,11 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "spatial.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "cuda", "spatial_cuda.so")
 REFERENCE_ROOT = os.environ.get("NITORCH_REFERENCE", "/root/reference")
 
 _compiled = None
+_compiled_cuda = None
 _ts = None
 
 
@@ -32,6 +37,18 @@ def load_compiled():
         spec.loader.exec_module(mod)
         _compiled = mod
     return _compiled
+
+
+def load_compiled_cuda():
+    """The reference module with its CUDA backend (sm_100a) or None."""
+    global _compiled_cuda
+    if _compiled_cuda is None and os.path.exists(REF_CUDA_SO):
+        import torch  # noqa: F401
+        spec = importlib.util.spec_from_file_location("spatial_cuda", REF_CUDA_SO)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _compiled_cuda = mod
+    return _compiled_cuda
 
 
 def load_ts_coeff():
