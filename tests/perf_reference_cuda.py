@@ -44,7 +44,7 @@ def chain(mod, x, g, w):
         return out
 
     y = rec("pull_fwd", lambda: mod.grid_pull(x, g, b, o, 0))
-    z = rec("push_fwd", lambda: mod.grid_push(y, g, [], b, o, 0))
+    z = rec("push_fwd", lambda: mod.grid_push(y, g, list(x.shape[2:]), b, o, 0))
     yr = y.detach().requires_grad_(True)
     gr = g.detach().requires_grad_(True)
     dy, dg1 = rec("push_bwd", lambda: mod.grid_push_backward(w, yr, gr, b, o, 0))
