@@ -138,7 +138,7 @@ __device__ __forceinline__ void unit_axis(Axis<NT, T, I>& ax) {
 // then share most of their support, which the L1 serves.
 constexpr int TILE_IN = 32, TILE_MID = 8, PP_THREADS = TILE_IN * TILE_MID;
 
-template <int MODE> struct MinBlocks { static constexpr int value = (MODE == K_PUSH || MODE == K_COUNT) ? 3 : 2; };
+template <int MODE> struct MinBlocks { static constexpr int value = (MODE == K_PUSH || MODE == K_COUNT) ? 4 : 2; };
 
 // One sampling point (batch item n, grid position sub) of mode MODE: the
 // whole per-point computation, shared by the single-tensor kernel below and
