@@ -242,16 +242,32 @@ def timed_steps(fn, args, world, device, l2buf, timer=None, clocks=None, steps=N
     return total_ms, launches, clk
 
 
+# Ceiling of the scatter kernels: float reductions (RED) per second that this
+# GPU's atomic path sustains when fully coalesced, measured on B200 with
+# tests/perf_atomic_throughput.py (1.46 T scalar adds/s; vector forms 1.6 T).
+ATOMIC_ADDS_PER_S = 1.46e12
+SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
+
+
 def roofline(ops, labels, nvox, C, ms_per_step, traffic):
     hbm, src = peaks()
     dom = max(ops, key=lambda k: ops[k]["total_ms"])
     per = algo_bytes(dom, 4, C) * nvox
     achieved = per / (ops[dom]["avg_ms"] * 1e-3) / 1e9
     step_bytes = sum(algo_bytes(k, 4, C) for k in labels) * nvox
-    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
-            "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": src,
-            "algorithmic_bytes_per_launch": per, "traffic": traffic,
-            "step_frac": round(step_bytes / (ms_per_step * 1e-3) / 1e9 / hbm, 4)}
+    out = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
+           "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": src,
+           "algorithmic_bytes_per_launch": per, "traffic": traffic,
+           "step_frac": round(step_bytes / (ms_per_step * 1e-3) / 1e9 / hbm, 4)}
+    if dom in SCATTER_OPS:
+        # the binding resource of a scatter: 64 taps x C channels float adds per point (cubic 3-D)
+        adds = 64 * C * nvox
+        rate = adds / (ops[dom]["avg_ms"] * 1e-3)
+        out["atomic"] = {"adds_per_launch": adds, "achieved_adds_per_s": round(rate / 1e9, 1),
+                         "ceiling_adds_per_s": ATOMIC_ADDS_PER_S / 1e9, "unit": "G adds/s",
+                         "frac": round(rate / ATOMIC_ADDS_PER_S, 3),
+                         "ceiling_source": "measured on B200 by tests/perf_atomic_throughput.py"}
+    return out
 
 
 def run_b200(args, rank, world, device):
