@@ -30,13 +30,16 @@
 //              gg_d = sum_c [ (P src)_c d(P W)_c/dx_d + (P W)_c d(P src)_c/dx_d ]
 // Runtime flags select the optional halves of the fused modes.
 #pragma once
+#include <type_traits>
+
 #include "pp_common.cuh"
 
 namespace ppk {
 
 enum Mode : int { K_PULL = 0, K_SGRAD, K_PUSH, K_COUNT, K_PULLGRAD, K_PUSHGRAD, K_KD,
                   K_PP, K_PP_BWD, K_NMODES };
-enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4 };  // F_A: pull (PULLGRAD) / push (PUSHGRAD, KD)
+enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4, F_VEC = 8 };  // F_A: pull (PULLGRAD) / push (PUSHGRAD, KD)
+// F_VEC: `out` is a channel-interleaved float accumulator (pp_lanes_kernel)
 
 struct PPArgs {
   const void* src;   // gathered tensor (N, C, *src_size)
@@ -138,6 +141,21 @@ __device__ __forceinline__ void unit_axis(Axis<NT, T, I>& ax) {
 // then share most of their support, which the L1 serves.
 constexpr int TILE_IN = 32, TILE_MID = 8, PP_THREADS = TILE_IN * TILE_MID;
 
+// Vector reduction of CP interleaved float channels (red.global.add.v2/v4.f32).
+template <int CP> __device__ __forceinline__ void red_vec(float* p, const float (&v)[CP]) {
+  if constexpr (CP == 4)
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+                 "f"(v[3]) : "memory");
+  else
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(v[0]), "f"(v[1]) : "memory");
+}
+// Channel blocks that can scatter into a channel-interleaved float
+// accumulator (flag F_VEC): float arithmetic, 2-4 channels in one block.
+template <class T, int CB> struct PPVec {
+  static constexpr bool ok = std::is_same<T, float>::value && CB >= 2;
+  static constexpr int CP = CB == 2 ? 2 : 4;
+};
+
 template <int MODE> struct MinBlocks { static constexpr int value = (MODE == K_PUSH || MODE == K_COUNT) ? 4 : 2; };
 
 // One sampling point (batch item n, grid position sub) of mode MODE: the
@@ -168,6 +186,7 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
 
   const bool do_a = (a.flags & F_A) != 0;
   const bool do_grad = (a.flags & F_GRAD) != 0;
+  const bool vec = (a.flags & F_VEC) != 0;  // channel-interleaved float accumulator
 
   // per-voxel output locations (gathered outputs / grid gradient)
   int64_t ovox = static_cast<int64_t>(n) * a.out_sN;
@@ -252,6 +271,27 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
                 static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(v) * dscale))); \
     else                                                                                     \
       atomic_acc(opc + (cb * a.out_sC + (off)), (v));                                        \
+  } while (0)
+
+// scatter of one tap's channel values VAL(cb): one vector reduction into the
+// interleaved accumulator when `vec`, else one reduction per nonzero value
+#define PP_SCATTER_CH(off, VAL)                                                     \
+  do {                                                                              \
+    if constexpr (PPVec<T, CB>::ok) {                                               \
+      if (vec) {                                                                    \
+        float vals_[PPVec<T, CB>::CP];                                              \
+        _Pragma("unroll") for (int q_ = 0; q_ < PPVec<T, CB>::CP; ++q_) vals_[q_] = 0.f; \
+        _Pragma("unroll") for (int cb = 0; cb < CB; ++cb) vals_[cb] = VAL(cb);     \
+        red_vec<PPVec<T, CB>::CP>(opc + (off), vals_);                              \
+        break;                                                                      \
+      }                                                                             \
+    }                                                                               \
+    _Pragma("unroll") PP_CB {                                                       \
+      if (CB == 1 || cb < nc) {                                                     \
+        const T v_ = VAL(cb);                                                       \
+        if (v_ != T(0)) PP_SCATTER(off, v_);                                        \
+      }                                                                             \
+    }                                                                               \
   } while (0)
 
 #define PP_TAP_VALID(i, j, k) (full || ((((ax.mask >> (i)) & (ay.mask >> (j)) & (az.mask >> (k))) & 1u) != 0u))
@@ -422,13 +462,8 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
                 if (i < tx && PP_TAP_VALID(i, j, k)) {
                   const T wt = ax.w[i] * wyz;
                   const I off = ax.oo[i] + oyz;
-#pragma unroll
-                  PP_CB {
-                    if (CB == 1 || cb < nc) {
-                      const T v = wt * t[cb];
-                      if (v != T(0)) PP_SCATTER(off, v);
-                    }
-                  }
+                  auto val = [&](int cb) { return wt * t[cb]; };
+                  PP_SCATTER_CH(off, val);
                 }
               }
             }
@@ -487,13 +522,8 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
                   if (do_a && valid) {
                     const T wt = ax.w[i] * wyz;
                     const I off = ax.oo[i] + ooyz;
-#pragma unroll
-                    PP_CB {
-                      if (CB == 1 || cb < nc) {
-                        const T pv = wt * t[cb];
-                        if (pv != T(0)) PP_SCATTER(off, pv);
-                      }
-                    }
+                    auto val = [&](int cb) { return wt * t[cb]; };
+                    PP_SCATTER_CH(off, val);
                   }
                 }
               }
@@ -576,16 +606,13 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
                   }
                   if (do_a && valid) {
                     const I off = ax.oo[i] + ooyz;
-#pragma unroll
-                    PP_CB {
-                      if (CB == 1 || cb < nc) {
-                        // push value: gx wy wz t0 + wx (gy wz t1 + wy gz t2)
-                        const T pa = ay.w[j] * az.w[k] * t0[cb];
-                        const T pb = ay.g[j] * az.w[k] * t1[cb] + ay.w[j] * az.g[k] * t2[cb];
-                        const T pv = ax.g[i] * pa + ax.w[i] * pb;
-                        if (pv != T(0)) PP_SCATTER(off, pv);
-                      }
-                    }
+                    // push value: gx wy wz t0 + wx (gy wz t1 + wy gz t2)
+                    auto val = [&](int cb) {
+                      const T pa = ay.w[j] * az.w[k] * t0[cb];
+                      const T pb = ay.g[j] * az.w[k] * t1[cb] + ay.w[j] * az.g[k] * t2[cb];
+                      return ax.g[i] * pa + ax.w[i] * pb;
+                    };
+                    PP_SCATTER_CH(off, val);
                   }
                 }
               }
@@ -688,13 +715,8 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
                 if (i < tx && PP_TAP_VALID(i, j, k)) {
                   const T wt = ax.w[i] * wyz;
                   const I off = ax.oo[i] + oyz;
-#pragma unroll
-                  PP_CB {
-                    if (CB == 1 || cb < nc) {
-                      const T v = wt * y[cb];
-                      if (v != T(0)) PP_SCATTER(off, v);
-                    }
-                  }
+                  auto val = [&](int cb) { return wt * y[cb]; };
+                  PP_SCATTER_CH(off, val);
                 }
               }
             }
@@ -799,13 +821,8 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
                   if (i < tx && PP_TAP_VALID(i, j, k)) {
                     const T wt = ax.w[i] * wyz;
                     const I off = ax.oo[i] + oyz;
-#pragma unroll
-                    PP_CB {
-                      if (CB == 1 || cb < nc) {
-                        const T v = wt * dv[cb];
-                        if (v != T(0)) PP_SCATTER(off, v);
-                      }
-                    }
+                    auto val = [&](int cb) { return wt * dv[cb]; };
+                    PP_SCATTER_CH(off, val);
                   }
                 }
               }
@@ -826,6 +843,7 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
 #undef PP_SCATTER
 
 #undef PP_TAP_VALID
+#undef PP_SCATTER_CH
 }
 
 template <int D, int ORD, int CB, class S, int MODE, class I>
@@ -865,9 +883,153 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
   pp_point<D, ORD, CB, S, MODE, I>(a, sub, n);
 }
 
+// Push / count with the last axis' taps spread over lanes (3-D, orders 1
+// and 3): NT = taps-per-axis consecutive lanes serve one sampling point,
+// lane q adding the contributions of last-axis tap q.  Consecutive lanes
+// then write consecutive floats -- a point's last-axis taps, followed by the
+// next point's, which in source-sorted (or natural, last axis fastest) order
+// sits one voxel further along the same row -- so a reduction instruction
+// touches one or two sectors instead of one or more per lane.  Each lane
+// builds the whole stencil (cheap next to the reductions it saves).
+//
+// With CP > 0 (flag F_VEC), `out` is a float accumulator with the channels
+// of a voxel interleaved in CP slots ((N, X, Y, Z, CP), CP = 2 or 4): one
+// vector reduction (red.global.add.v2/v4.f32) then adds all channels of a
+// tap, C times fewer reduction instructions; the host converts the
+// accumulator to the output layout afterwards.
+template <int ORD, int CB, class S, int MODE, class I, int CP>
+__global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_lanes_kernel(const PPArgs a) {
+  using T = typename Acc<S>::type;
+  constexpr int NT = Taps<ORD>::value;
+  constexpr int PPB = PP_THREADS / NT;  // sampling points per CTA
+  const int q = static_cast<int>(threadIdx.x) % NT;
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
+  if (t >= a.nvox) return;
+  I v = a.perm != nullptr ? static_cast<I>(__ldg(a.perm + t)) : static_cast<I>(t);
+  I sub[3];
+  sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]);
+  sub[1] = v % static_cast<I>(a.trgt_size[1]); v /= static_cast<I>(a.trgt_size[1]);
+  sub[0] = v % static_cast<I>(a.trgt_size[0]);
+  const I n = v / static_cast<I>(a.trgt_size[0]);
+
+  const T* gp = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
+  int64_t tvox = static_cast<int64_t>(n) * a.trgt_sN;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    gp += static_cast<int64_t>(sub[d]) * a.grid_s[d];
+    tvox += static_cast<int64_t>(sub[d]) * a.trgt_s[d];
+  }
+  T coord[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
+  {
+    const T tol = (a.extrapolate & 2) ? static_cast<T>(0.5 + 5e-2) : static_cast<T>(5e-2);
+    bool inb = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) inb = inb && in_fov<T>(coord[d], a.src_size[d], tol);
+    if (!((a.extrapolate & 1) || inb)) return;
+  }
+  Axis<NT, T, I> ax, ay, az;
+  build_axis<NT, false, false, false, true, T, I>(ax, ORD, a.bound[0], coord[0], static_cast<I>(a.src_size[0]),
+                                                   I(0), static_cast<I>(a.out_s[0]));
+  build_axis<NT, false, false, false, true, T, I>(ay, ORD, a.bound[1], coord[1], static_cast<I>(a.src_size[1]),
+                                                   I(0), static_cast<I>(a.out_s[1]));
+  build_axis<NT, false, false, false, true, T, I>(az, ORD, a.bound[2], coord[2], static_cast<I>(a.src_size[2]),
+                                                   I(0), static_cast<I>(a.out_s[2]));
+  // this lane's last-axis tap (selected without dynamic register indexing)
+  T wz = T(0);
+  I oz = 0;
+  bool vz = false;
+#pragma unroll
+  for (int k = 0; k < NT; ++k)
+    if (k == q) { wz = az.w[k]; oz = az.oo[k]; vz = ((az.mask >> k) & 1u) != 0u; }
+  if (!vz) return;
+
+  const S* trg_v = static_cast<const S*>(a.trgt) + tvox;
+  T* outs_n = a.det_acc == nullptr ? static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN : nullptr;
+  unsigned long long* dacc_n = a.det_acc != nullptr ? a.det_acc + static_cast<int64_t>(n) * a.out_sN : nullptr;
+  const double dscale = a.det_acc != nullptr ? det_scale(a) : 0.0;
+  if constexpr (CP > 0) {
+    // all channels (C <= CP) of a tap in one vector reduction
+    float tv[CP];
+#pragma unroll
+    for (int c = 0; c < CP; ++c) tv[c] = c < a.C ? static_cast<float>(ldg_acc(trg_v + c * a.trgt_sC)) : 0.f;
+    float* acc_n = static_cast<float*>(a.out) + static_cast<int64_t>(n) * a.out_sN;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      const T wyz = ay.w[j] * wz;
+      const I oyz = ay.oo[j] + oz;
+#pragma unroll
+      for (int i = 0; i < NT; ++i) {
+        if ((((ax.mask >> i) & (ay.mask >> j)) & 1u) == 0u) continue;
+        const float wt = static_cast<float>(ax.w[i] * wyz);
+        if (wt == 0.f) continue;
+        float vals[CP];
+#pragma unroll
+        for (int c = 0; c < CP; ++c) vals[c] = wt * tv[c];
+        red_vec<CP>(acc_n + (ax.oo[i] + oyz), vals);
+      }
+    }
+    return;
+  }
+  const int64_t C = MODE == K_COUNT ? 1 : a.C;
+  for (int64_t c0 = 0; c0 < C; c0 += CB) {
+    const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
+    T tv[CB];
+#pragma unroll
+    for (int cb = 0; cb < CB; ++cb)
+      tv[cb] = (MODE == K_COUNT) ? T(1) : ((CB == 1 || cb < nc) ? ldg_acc(trg_v + (c0 + cb) * a.trgt_sC) : T(0));
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      const T wyz = ay.w[j] * wz;
+      const I oyz = ay.oo[j] + oz;
+#pragma unroll
+      for (int i = 0; i < NT; ++i) {
+        if ((((ax.mask >> i) & (ay.mask >> j)) & 1u) == 0u) continue;
+        const T wt = ax.w[i] * wyz;
+        const I off = ax.oo[i] + oyz;
+#pragma unroll
+        for (int cb = 0; cb < CB; ++cb) {
+          if (CB == 1 || cb < nc) {
+            const T val = wt * tv[cb];
+            if (val == T(0)) continue;
+            if (dacc_n != nullptr)
+              atomicAdd(dacc_n + ((c0 + cb) * a.out_sC + off),
+                        static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(val) * dscale)));
+            else
+              atomic_acc(outs_n + ((c0 + cb) * a.out_sC + off), val);
+          }
+        }
+      }
+    }
+  }
+}
+
+// The lane-split push applies to 3-D push / count at orders 1 and 3.
+template <int D, int ORD, int MODE> struct UseLanes {
+  static constexpr bool value = D == 3 && (ORD == 1 || ORD == 3) && (MODE == K_PUSH || MODE == K_COUNT);
+};
+bool lanes_enabled();  // host switch (pp_capi.cu), on unless PP_PUSH_LANES=0
+
 template <int D, int ORD, int CB, class S, int MODE, class I>
 inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
   if (a.nvox == 0) return cudaSuccess;
+  if constexpr (UseLanes<D, ORD, MODE>::value) {
+    if (lanes_enabled()) {
+      constexpr int PPB = PP_THREADS / Taps<ORD>::value;
+      const int64_t nb = (a.nvox + PPB - 1) / PPB;
+      if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+      if (a.flags & F_VEC) {
+        if constexpr (MODE == K_PUSH && CB >= 2 && std::is_same<typename Acc<S>::type, float>::value) {
+          pp_lanes_kernel<ORD, CB, S, MODE, I, (CB == 2 ? 2 : 4)><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
+          return cudaGetLastError();
+        }
+        return cudaErrorInvalidValue;  // the host only sets F_VEC where a vector kernel exists
+      }
+      pp_lanes_kernel<ORD, CB, S, MODE, I, 0><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
+      return cudaGetLastError();
+    }
+  }
   const int64_t inner = a.trgt_size[D - 1];
   const int64_t mid = D > 1 ? a.trgt_size[D - 2] : 1;
   const int64_t outer = a.N * (D == 3 ? a.trgt_size[0] : 1);

@@ -84,7 +84,13 @@ def test_workspace_query():
     d = _lib.desc(torch.zeros((1, 2, 8, 8, 8), dtype=torch.bfloat16))
     n = L.pp_push_workspace_bytes(ctypes.byref(d), 0)
     assert n >= 2 * 8 * 8 * 8 * 4 and n % 256 == 0
-    d = _lib.desc(torch.zeros((1, 2, 8, 8, 8), dtype=torch.float32))
+    # float32, 3-D, 2-4 channels: room for the channel-interleaved accumulator
+    # of the vectorised push (optional: the push runs without it)
+    d = _lib.desc(torch.zeros((1, 3, 8, 8, 8), dtype=torch.float32))
+    assert L.pp_push_workspace_bytes(ctypes.byref(d), 0) == 8 * 8 * 8 * 4 * 4
+    d = _lib.desc(torch.zeros((1, 1, 8, 8, 8), dtype=torch.float32))
+    assert L.pp_push_workspace_bytes(ctypes.byref(d), 0) == 0
+    d = _lib.desc(torch.zeros((1, 2, 8, 8), dtype=torch.float32))
     assert L.pp_push_workspace_bytes(ctypes.byref(d), 0) == 0
 
 
