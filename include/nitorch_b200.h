@@ -229,12 +229,17 @@ typedef struct pp_batch_entry {
 
 /* Host bytes of a plan for `nvol` volumes. */
 PP_API size_t pp_batch_plan_bytes(int32_t nvol);
+/* Device scratch (bytes) that lets the scatter entries of 2-4 channels at
+ * orders 2-3 accumulate with vector reductions (0 if no entry does). */
+PP_API size_t pp_batch_scratch_bytes(const pp_batch_entry* entries, int32_t nvol, int32_t mode);
 /* Validates the entries and writes a plan into `plan` (host memory of
  * pp_batch_plan_bytes(nvol) bytes, owned by the caller).  ctas = 0: one CTA
- * per 256 sampling points; ctas > 0: that many persistent CTAs.  The
- * tensors must stay alive and in place while the plan is used. */
+ * per 256 sampling points; ctas > 0: that many persistent CTAs.  `scratch`
+ * (device, 256-byte aligned, pp_batch_scratch_bytes bytes) is optional:
+ * without it every entry scatters with scalar reductions.  The tensors and
+ * the scratch must stay alive and in place while the plan is used. */
 PP_API int pp_batch_plan(const pp_batch_entry* entries, int32_t nvol, int32_t mode, int32_t ctas,
-                         void* plan, size_t plan_bytes);
+                         void* plan, size_t plan_bytes, void* scratch, size_t scratch_bytes);
 /* Enqueues the plan's zero fills and launches on `stream`. */
 PP_API int pp_batch_run(const void* plan, void* stream);
 

@@ -69,7 +69,7 @@ EXPORTS = (
     "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
     "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
     "pp_sample_order_noalloc", "pp_grid_pull_push", "pp_grid_pull_push_backward",
-    "pp_batch_plan_bytes", "pp_batch_plan", "pp_batch_run",
+    "pp_batch_plan_bytes", "pp_batch_scratch_bytes", "pp_batch_plan", "pp_batch_run",
 )
 
 PP_BATCH_PULL, PP_BATCH_PUSH, PP_BATCH_PUSH_BACKWARD = 0, 2, 4
@@ -99,8 +99,10 @@ def _declare(L):
     L.pp_grid_pull_push_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
     L.pp_batch_plan_bytes.argtypes = [ctypes.c_int32]
     L.pp_batch_plan_bytes.restype = sz
+    L.pp_batch_scratch_bytes.argtypes = [ctypes.POINTER(PPBatchEntry), ctypes.c_int32, ctypes.c_int32]
+    L.pp_batch_scratch_bytes.restype = sz
     L.pp_batch_plan.argtypes = [ctypes.POINTER(PPBatchEntry), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-                                vp, sz]
+                                vp, sz, vp, sz]
     L.pp_batch_run.argtypes = [vp, vp]
     L.pp_spline_coeff.argtypes = [T, T, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp]
     L.pp_spline_coeff_nd.argtypes = [T, T, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
@@ -113,7 +115,7 @@ def _declare(L):
     L.pp_sample_order_noalloc.argtypes = [T, I64P, vp, vp]
     for name in EXPORTS:
         if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches",
-                        "pp_sample_order_workspace_bytes", "pp_batch_plan_bytes"):
+                        "pp_sample_order_workspace_bytes", "pp_batch_plan_bytes", "pp_batch_scratch_bytes"):
             getattr(L, name).restype = ctypes.c_int
     return L
 

@@ -56,7 +56,12 @@ class BatchPlan:
         self.device = torch.device(device or "cuda")
         self.buf = ctypes.create_string_buffer(nbytes)
         self.mode = mode
-        _lib.check(L.pp_batch_plan(arr, n, mode, int(ctas), ctypes.cast(self.buf, ctypes.c_void_p), nbytes))
+        # interleaved accumulators of the vectorised scatters (device scratch)
+        sbytes = L.pp_batch_scratch_bytes(arr, n, mode)
+        self.scratch = torch.empty(sbytes, dtype=torch.uint8, device=self.device) if sbytes else None
+        sptr = ctypes.c_void_p(self.scratch.data_ptr()) if sbytes else None
+        _lib.check(L.pp_batch_plan(arr, n, mode, int(ctas), ctypes.cast(self.buf, ctypes.c_void_p), nbytes,
+                                   sptr, sbytes))
 
     def run(self):
         L = _lib.load()

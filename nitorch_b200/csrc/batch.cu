@@ -16,6 +16,7 @@
 // items).  Everything pp_batch_run issues (zero fills and kernels) is
 // stream-ordered and takes no host synchronisation.
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -43,9 +44,42 @@ namespace ppb {
 constexpr int kMaxGroups = 16;     // (order 0-3) x (channel block 1-4)
 constexpr uint32_t kMagic = 0x50504231u;
 
+// Interleaved float accumulator (X*Y*Z*CP floats, channel fastest) of one
+// volume -> its contiguous float32 output (1, C, X, Y, Z).
+struct VecStore {
+  const float* acc;
+  float* out;
+  int64_t V;
+  int32_t C, CP;
+};
+constexpr int kMaxStores = 256;
+struct StoreLaunch {
+  int32_t n, pad;
+  int64_t first[kMaxStores + 1];  // element prefix sums (V * C per volume)
+  VecStore s[kMaxStores];
+};
+static_assert(sizeof(StoreLaunch) <= 32764, "store argument above the kernel-parameter limit");
+
+__global__ void __launch_bounds__(256) batch_store_kernel(const __grid_constant__ StoreLaunch L) {
+  const int64_t total = L.first[L.n];
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int lo = 0, hi = L.n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (L.first[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    const VecStore& v = L.s[lo];
+    const int64_t j = i - L.first[lo];  // = c * V + lin
+    const int64_t c = j / v.V, lin = j - c * v.V;
+    v.out[j] = v.acc[lin * v.CP + c];
+  }
+}
+
+
 struct PlanHeader {
   uint32_t magic;
-  int32_t mode, ctas, nvol, dtype, ngroups, nfill, pad;
+  int32_t mode, ctas, nvol, dtype, ngroups, nfill, nstore;
   int32_t gfirst[kMaxGroups], gcount[kMaxGroups], gorder[kMaxGroups], gcb[kMaxGroups];
 };
 
@@ -55,9 +89,19 @@ struct Fill {  // a byte range to zero before the launches
 };
 
 // Layout of the host plan buffer: header, then per volume its PPArgs and its
-// item count (sorted by group), then the fill ranges.
+// item count (sorted by group), the fill ranges, then the interleaved stores.
 inline size_t plan_bytes(int nvol) {
-  return sizeof(PlanHeader) + static_cast<size_t>(nvol) * (sizeof(ppk::PPArgs) + sizeof(int64_t) + sizeof(Fill));
+  return sizeof(PlanHeader) +
+         static_cast<size_t>(nvol) * (sizeof(ppk::PPArgs) + sizeof(int64_t) + sizeof(Fill) + sizeof(VecStore));
+}
+
+// Channel slots of the interleaved accumulator of a scatter entry (0: the
+// entry scatters with scalar reductions): 2-4 channels, orders 2 and 3
+// (orders 0-1 scatter few taps, where the extra store pass does not pay).
+inline int entry_slots(int mode, int64_t C, int iso) {
+  const bool scatter = mode == ppk::K_PUSH || mode == ppk::K_PUSHGRAD || mode == ppk::K_PP || mode == ppk::K_PP_BWD;
+  if (!scatter || iso < 2 || iso > 3 || !ppk::lanes_enabled()) return 0;
+  return C == 2 ? 2 : (C == 3 || C == 4) ? 4 : 0;
 }
 
 bool is_scatter(int mode) {
@@ -73,8 +117,27 @@ extern "C" {
 
 size_t pp_batch_plan_bytes(int32_t nvol) { return nvol > 0 ? plan_bytes(nvol) : 0; }
 
+// Device scratch for the channel-interleaved accumulators of the entries
+// that scatter with vector reductions (0 if none does).
+size_t pp_batch_scratch_bytes(const pp_batch_entry* items, int32_t nvol, int32_t mode) {
+  if (!items || nvol <= 0) return 0;
+  size_t total = 0;
+  for (int v = 0; v < nvol; ++v) {
+    const pp_batch_entry& it = items[v];
+    if (!it.out.data || it.out.ndim != 5) continue;
+    int bound[3], ord[3];
+    if (read_options(&it.opt, 3, bound, ord)) continue;
+    const int iso = (ord[0] == ord[1] && ord[0] == ord[2]) ? ord[0] : -1;
+    const int CP = entry_slots(mode, it.out.sizes[1], iso);
+    if (!CP) continue;
+    const int64_t V = it.out.sizes[2] * it.out.sizes[3] * it.out.sizes[4];
+    total += ((static_cast<size_t>(V) * CP * 4 + 255) / 256) * 256;
+  }
+  return total;
+}
+
 int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32_t ctas, void* plan,
-                  size_t plan_bytes_) {
+                  size_t plan_bytes_, void* scratch, size_t scratch_bytes) {
   if (!items || nvol <= 0) return fail(PP_ERR_ARG, "(): expected at least one batch entry");
   if (mode != ppk::K_PULL && mode != ppk::K_PUSH && mode != ppk::K_PULLGRAD && mode != ppk::K_PUSHGRAD &&
       mode != ppk::K_PP && mode != ppk::K_PP_BWD)
@@ -86,6 +149,10 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
   std::vector<int> order(nvol), cbs(nvol);
   std::vector<int64_t> nitems(nvol);
   std::vector<Fill> fills;
+  std::vector<VecStore> stores;
+  size_t scratch_used = 0;
+  const bool use_scratch = scratch && scratch_bytes >= pp_batch_scratch_bytes(items, nvol, mode) &&
+                           reinterpret_cast<uintptr_t>(scratch) % 256 == 0;
   int dtype = -1;
   const bool scatter = is_scatter(mode);
   for (int v = 0; v < nvol; ++v) {
@@ -192,7 +259,26 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
     order[v] = iso;
     cbs[v] = static_cast<int>(a.C >= 4 ? 4 : a.C);
     nitems[v] = (a.nvox + kBatchPoints - 1) / kBatchPoints;
-    if (scatter && out) fills.push_back({out->data, static_cast<size_t>(numel(out)) * 4});
+    const int CP = scatter && out && use_scratch ? entry_slots(mode, a.C, iso) : 0;
+    if (CP) {
+      // vector reductions into this entry's interleaved accumulator, stored
+      // to `out` after the launches
+      const int64_t V = out->sizes[2] * out->sizes[3] * out->sizes[4];
+      float* acc = reinterpret_cast<float*>(static_cast<unsigned char*>(scratch) + scratch_used);
+      scratch_used += ((static_cast<size_t>(V) * CP * 4 + 255) / 256) * 256;
+      if (!fits32(V * CP)) return fail(PP_ERR_UNSUPPORTED, "(): batch entry %d: volume too large", v);
+      a.out = acc;
+      a.out_sN = V * CP;
+      a.out_sC = 1;
+      a.out_s[2] = CP;
+      a.out_s[1] = out->sizes[4] * CP;
+      a.out_s[0] = out->sizes[3] * out->sizes[4] * CP;
+      a.flags |= ppk::F_VEC;
+      fills.push_back({acc, static_cast<size_t>(V) * CP * 4});
+      stores.push_back({acc, static_cast<float*>(out->data), V, static_cast<int32_t>(a.C), CP});
+    } else if (scatter && out) {
+      fills.push_back({out->data, static_cast<size_t>(numel(out)) * 4});
+    }
   }
   // group by (order, channel block)
   std::vector<int> idx(nvol);
@@ -235,6 +321,9 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
       pf[nf++] = f;
   }
   h->nfill = nf;
+  VecStore* ps = reinterpret_cast<VecStore*>(pf + nvol);
+  for (size_t i = 0; i < stores.size(); ++i) ps[i] = stores[i];
+  h->nstore = static_cast<int32_t>(stores.size());
   return PP_OK;
 }
 
@@ -246,6 +335,7 @@ int pp_batch_run(const void* plan, void* stream) {
   const ppk::PPArgs* pa = reinterpret_cast<const ppk::PPArgs*>(p + sizeof(PlanHeader));
   const int64_t* pn = reinterpret_cast<const int64_t*>(pa + h->nvol);
   const Fill* pf = reinterpret_cast<const Fill*>(pn + h->nvol);
+  const VecStore* ps = reinterpret_cast<const VecStore*>(pf + h->nvol);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc;
   for (int f = 0; f < h->nfill; ++f)
@@ -265,6 +355,21 @@ int pp_batch_run(const void* plan, void* stream) {
       const cudaError_t err = fn ? fn(h->gorder[g], h->gcb[g], L, h->ctas, st) : cudaErrorInvalidValue;
       if ((rc = cuda_check(err, "batched kernel launch"))) return rc;
     }
+  }
+  // interleaved accumulators -> outputs
+  static thread_local StoreLaunch SL;
+  for (int s0 = 0; s0 < h->nstore; s0 += kMaxStores) {
+    const int n = std::min(kMaxStores, h->nstore - s0);
+    SL.n = n;
+    SL.first[0] = 0;
+    for (int e = 0; e < n; ++e) {
+      SL.s[e] = ps[s0 + e];
+      SL.first[e + 1] = SL.first[e] + SL.s[e].V * SL.s[e].C;
+    }
+    const int nb = grid_blocks(SL.first[n]);
+    batch_store_kernel<<<nb, 256, 0, st>>>(SL);
+    count_launch();
+    if ((rc = cuda_check(cudaGetLastError(), "batched interleaved store"))) return rc;
   }
   return PP_OK;
 }

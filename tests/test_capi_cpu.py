@@ -110,7 +110,7 @@ def test_batch_plan_validation_on_host():
 
     def plan(mode, ents, nbytes=nb):
         arr = (_lib.PPBatchEntry * len(ents))(*ents)
-        return L.pp_batch_plan(arr, len(ents), mode, 0, p, nbytes)
+        return L.pp_batch_plan(arr, len(ents), mode, 0, p, nbytes, None, 0)
 
     ok = _entry(src=x, grid=g, out=z, opt=_lib.options([2], [3], 0))
     assert plan(_lib.PP_BATCH_PULL_PUSH, [ok, ok]) == _lib.PP_OK
@@ -128,3 +128,10 @@ def test_batch_plan_validation_on_host():
     assert plan(_lib.PP_BATCH_PULL_PUSH, [half]) == _lib.PP_ERR_DTYPE
     assert plan(3, [ok]) == _lib.PP_ERR_UNSUPPORTED  # count is not a batched mode
     assert L.pp_batch_run(None, None) == _lib.PP_ERR_ARG
+    # interleaved scratch: 2-4 channel scatter entries at orders 2-3 only
+    arr = (_lib.PPBatchEntry * 2)(ok, high)
+    assert L.pp_batch_scratch_bytes(arr, 2, _lib.PP_BATCH_PULL_PUSH) == 6 * 5 * 4 * 2 * 4 // 256 * 256 + 256
+    lin = _entry(src=x, grid=g, out=z, opt=_lib.options([2], [1], 0))
+    arr = (_lib.PPBatchEntry * 1)(lin)
+    assert L.pp_batch_scratch_bytes(arr, 1, _lib.PP_BATCH_PULL_PUSH) == 0
+    assert L.pp_batch_scratch_bytes(arr, 1, _lib.PP_BATCH_PULL) == 0
