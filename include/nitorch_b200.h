@@ -171,6 +171,49 @@ PP_API int pp_grid_pull_push_backward(const pp_tensor* grad, const pp_tensor* in
                                       const pp_tensor* grad_grid, const pp_options* opt,
                                       void* stream, void* workspace, size_t workspace_bytes);
 
+/* Displacement self-composition u <- u + pull(u, id + u), the step of the
+ * scaling-and-squaring exponentiation of a stationary velocity field
+ * (nitorch/spatial/_svf.py:85-94 with _pull_vel :323-362, which materialise
+ * id + u and call ni::grid_pull).  disp and out: (N, *spatial, D) float32 or
+ * float64 fields, displacement components last, any strides; out must not
+ * alias disp.  The options' bound / order / extrapolate apply to the pull
+ * (nitorch's defaults there: dft, linear, extrapolate). */
+PP_API int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_options* opt,
+                          void* stream);
+
+/* Gradient of <grad, u + pull(u, id + u)> with respect to u (the exact
+ * adjoint of pp_svf_compose), written to grad_disp (disp's sizes, zero-filled
+ * by the call, must not alias the inputs).  No deterministic mode. */
+PP_API int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp,
+                                   const pp_tensor* grad_disp, const pp_options* opt, void* stream);
+
+/* ---- Affine sampling without a materialised grid ----------------------
+ * nitorch builds affine_grid(mat, shape) (nitorch/spatial/_grid.py:579-615)
+ * and calls ni::grid_pull on it (resize :618-754, reslice :860-914); these
+ * entry points compute the coordinate A [sub; 1] of every grid point in the
+ * kernel instead (12 bytes per point less traffic, no grid allocation).
+ * mat: (N, D, D+1) or (N, D+1, D+1) matrices of the grid dtype (float32 for
+ * 16-bit images), rows of D+1 contiguous entries; the first D rows are used. */
+
+/* out (N, C, *shape) = input (N, C, *inshape) sampled at A [sub; 1]. */
+PP_API int pp_affine_pull(const pp_tensor* input, const pp_tensor* mat, const pp_tensor* out,
+                          const pp_options* opt, void* stream);
+
+/* Adjoint of pp_affine_pull: out (N, C, *outshape) = push of input
+ * (N, C, *shape).  Workspace as for pp_grid_push (pp_push_workspace_bytes(out)). */
+PP_API int pp_affine_push(const pp_tensor* input, const pp_tensor* mat, const pp_tensor* out,
+                          const pp_options* opt, void* stream, void* workspace, size_t workspace_bytes);
+
+/* Gradient of <grad, pp_affine_pull(input, mat)> with respect to the first
+ * D rows of the matrices, into grad_mat (N, D, D+1) float32 with contiguous
+ * rows (the input gradient is pp_affine_push of grad).  Needs
+ * pp_affine_grad_workspace_bytes(grad) bytes of workspace; images of
+ * float32 / 16-bit storage. */
+PP_API size_t pp_affine_grad_workspace_bytes(const pp_tensor* grad);
+PP_API int pp_affine_grad_matrix(const pp_tensor* grad, const pp_tensor* input, const pp_tensor* mat,
+                                 const pp_tensor* grad_mat, const pp_options* opt, void* stream,
+                                 void* workspace, size_t workspace_bytes);
+
 /* Source-sorted processing order of a grid's sampling points (no
  * counterpart in the reference; a scheduling aid for rough deformations):
  * writes to `perm` (int32, N*prod(grid spatial) entries) the sample indices

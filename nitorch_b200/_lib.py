@@ -70,6 +70,8 @@ EXPORTS = (
     "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
     "pp_sample_order_noalloc", "pp_grid_pull_push", "pp_grid_pull_push_backward",
     "pp_batch_plan_bytes", "pp_batch_scratch_bytes", "pp_batch_plan", "pp_batch_run",
+    "pp_svf_compose", "pp_svf_compose_backward", "pp_affine_pull", "pp_affine_push",
+    "pp_affine_grad_workspace_bytes", "pp_affine_grad_matrix",
 )
 
 PP_BATCH_PULL, PP_BATCH_PUSH, PP_BATCH_PUSH_BACKWARD = 0, 2, 4
@@ -97,6 +99,13 @@ def _declare(L):
     L.pp_grid_grad_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
     L.pp_grid_pull_push.argtypes = [T, T, T, O, vp, vp, sz]
     L.pp_grid_pull_push_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
+    L.pp_svf_compose.argtypes = [T, T, O, vp]
+    L.pp_svf_compose_backward.argtypes = [T, T, T, O, vp]
+    L.pp_affine_pull.argtypes = [T, T, T, O, vp]
+    L.pp_affine_push.argtypes = [T, T, T, O, vp, vp, sz]
+    L.pp_affine_grad_workspace_bytes.argtypes = [T]
+    L.pp_affine_grad_workspace_bytes.restype = sz
+    L.pp_affine_grad_matrix.argtypes = [T, T, T, T, O, vp, vp, sz]
     L.pp_batch_plan_bytes.argtypes = [ctypes.c_int32]
     L.pp_batch_plan_bytes.restype = sz
     L.pp_batch_scratch_bytes.argtypes = [ctypes.POINTER(PPBatchEntry), ctypes.c_int32, ctypes.c_int32]
@@ -115,7 +124,8 @@ def _declare(L):
     L.pp_sample_order_noalloc.argtypes = [T, I64P, vp, vp]
     for name in EXPORTS:
         if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches",
-                        "pp_sample_order_workspace_bytes", "pp_batch_plan_bytes", "pp_batch_scratch_bytes"):
+                        "pp_sample_order_workspace_bytes", "pp_batch_plan_bytes", "pp_batch_scratch_bytes",
+                        "pp_affine_grad_workspace_bytes"):
             getattr(L, name).restype = ctypes.c_int
     return L
 

@@ -9,6 +9,7 @@ Same signatures, defaults, broadcasting and output shapes as
 """
 import torch
 
+from .affine import affine_pull, affine_push
 from .grid import GridCount, GridGrad, GridPull, GridPullPush, GridPush, SplineCoeff, SplineCoeffND
 
 
@@ -155,3 +156,124 @@ def identity_grid(shape, dtype=None, device=None):
     mesh1d = [torch.arange(float(s), dtype=dtype, device=device) for s in shape]
     grid = torch.meshgrid(*mesh1d, indexing="ij")
     return torch.stack(grid, dim=-1)
+
+
+def affine_grid(mat, shape):
+    """Dense transformation grid (..., *shape, D) of affine matrices
+    (..., D[+1], D+1) (nitorch/spatial/_grid.py:579-615).  resize / reslice
+    below do not build it: their kernels compute the coordinates."""
+    mat = torch.as_tensor(mat)
+    shape = list(shape)
+    dim = mat.shape[-1] - 1
+    if dim != len(shape):
+        raise ValueError(f"Dimension of the affine matrix ({dim}) and shape ({len(shape)}) are not the same.")
+    if mat.shape[-2] not in (dim, dim + 1):
+        raise ValueError(f"First argument should be matrices of shape (..., {dim}, {dim + 1}) or "
+                         f"(..., {dim + 1}, {dim + 1}) but got {tuple(mat.shape)}.")
+    batch = mat.shape[:-2]
+    grid = identity_grid(shape, dtype=mat.dtype, device=mat.device)
+    grid = grid.reshape([1] * len(batch) + list(grid.shape))
+    lin = mat[..., :dim, :dim].reshape(*batch, *([1] * dim), dim, dim)
+    off = mat[..., :dim, -1].reshape(*batch, *([1] * dim), dim)
+    return torch.matmul(lin, grid[..., None])[..., 0] + off
+
+
+def _resize_transform(inshape, factor, shape, anchor):
+    """Output shape and per-axis (scale, shift) with input = scale * output
+    + shift (nitorch/spatial/_grid.py:682-727)."""
+    nb_dim = len(inshape)
+    factor = list(factor) if isinstance(factor, (list, tuple)) else [factor or 0.] * nb_dim
+    factor = (factor + factor[-1:] * nb_dim)[:nb_dim]
+    factor = [f or 0. for f in factor]
+    outshape = list(shape) if shape is not None else [None] * nb_dim
+    outshape = (outshape + outshape[-1:] * nb_dim)[:nb_dim]
+    anchor = [a[0].lower() for a in (anchor if isinstance(anchor, (list, tuple)) else [anchor] * nb_dim)]
+    outshape = [o or max(1, int(i * f)) for i, o, f in zip(inshape, outshape, factor)]
+    if any(not s for s in outshape):
+        raise ValueError("Either factor or shape must be set in all dimensions")
+    factor = [f or o / i for o, i, f in zip(outshape, inshape, factor)]
+    scales, shifts = [], []
+    for anch, f, i, o in zip(anchor, factor, inshape, outshape):
+        if i == 1 or o == 1:
+            anch = "e"
+        if anch == "c":
+            scales.append((i - 1) / (o - 1))
+            shifts.append(0.)
+        elif anch == "e":
+            scale = i / o
+            scales.append(scale)
+            shifts.append(0.5 * (scale - 1))
+        elif anch == "f":
+            scales.append(1 / f)
+            shifts.append(0.)
+        elif anch == "l":
+            scales.append(1 / f)
+            shifts.append((i - 1) - (o - 1) / f)
+        else:
+            raise ValueError(f"Unknown anchor {anch}")
+    return outshape, factor, scales, shifts
+
+
+def resize(image, factor=None, shape=None, affine=None, anchor="c", dim=None, *args, **kwargs):
+    """Resize an image by a factor or to a shape (nitorch/spatial/_grid.py:618-754):
+    same arguments, anchors and output shapes; `prefilter` defaults to True.
+    The sampling coordinates are computed in the kernel (no grid).  With
+    `affine` (input orientation matrix, (..., D+1, D+1)), the resized
+    image's orientation matrix is returned too."""
+    image = torch.as_tensor(image)
+    nb_dim = dim or (len(shape) if shape is not None else image.dim() - 2)
+    inshape = list(image.shape[-nb_dim:])
+    outshape, factor, scales, shifts = _resize_transform(inshape, factor, shape, anchor)
+    interpolation = kwargs.pop("interpolation", args[0] if len(args) > 0 else "linear")
+    bound = kwargs.pop("bound", args[1] if len(args) > 1 else "zero")
+    extrapolate = kwargs.pop("extrapolate", args[2] if len(args) > 2 else False)
+    prefilter = kwargs.pop("prefilter", True)
+    batch = image.shape[:-nb_dim]
+    x = image.reshape(-1, 1, *inshape)
+    gdt = torch.float64 if x.dtype == torch.float64 else torch.float32
+    mat = torch.zeros((nb_dim, nb_dim + 1), dtype=gdt, device=x.device)
+    for d in range(nb_dim):
+        mat[d, d] = scales[d]
+        mat[d, nb_dim] = shifts[d]
+    if prefilter:
+        x = spline_coeff_nd(x, interpolation=interpolation, bound=bound, dim=nb_dim)
+    out = affine_pull(x, mat, outshape, interpolation, bound, extrapolate)
+    out = out.reshape(*batch, *outshape)
+    if affine is not None:
+        affine = torch.as_tensor(affine)
+        T = torch.eye(nb_dim + 1, dtype=affine.dtype, device=affine.device)
+        T[:nb_dim, :nb_dim] = torch.diag(torch.as_tensor(scales, dtype=affine.dtype, device=affine.device))
+        T[:nb_dim, nb_dim] = torch.as_tensor(shifts, dtype=affine.dtype, device=affine.device)
+        return out, affine.matmul(T)
+    return out
+
+
+def reslice(image, affine, affine_to, shape_to=None, **kwargs):
+    """Reslice an image to another space (nitorch/spatial/_grid.py:860-914):
+    the voxel-to-voxel matrix affine^-1 affine_to drives the kernel directly
+    (no grid); `prefilter` defaults to True."""
+    image = torch.as_tensor(image)
+    gdt = torch.float64 if image.dtype == torch.float64 else torch.float32
+    affine = torch.as_tensor(affine, dtype=gdt, device=image.device)
+    affine_to = torch.as_tensor(affine_to, dtype=gdt, device=image.device)
+    dim = affine.shape[-1] - 1
+    batch = affine.shape[:-2]
+    channels = image.shape[len(batch):-dim]
+    shape = image.shape[-dim:]
+    shape_to = list(shape_to or shape)
+    transformation = torch.linalg.solve(affine, affine_to)
+    n = 1
+    for b in batch:
+        n *= b
+    nc = 1
+    for c in channels:
+        nc *= c
+    x = image.reshape(n, nc, *shape)
+    interpolation = kwargs.pop("interpolation", "linear")
+    bound = kwargs.pop("bound", "zero")
+    extrapolate = kwargs.pop("extrapolate", False)
+    if kwargs.pop("prefilter", True):
+        x = spline_coeff_nd(x, interpolation=interpolation, bound=bound, dim=dim)
+    mat = transformation.reshape(-1, dim + 1, dim + 1)
+    out = affine_pull(x, mat, shape_to, interpolation, bound, extrapolate)
+    return out.reshape(*batch, *channels, *shape_to)

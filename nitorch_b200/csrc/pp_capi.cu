@@ -2,6 +2,7 @@
 // nitorch/_C/src/pushpull.cpp:19-72), output preparation (the zero-filled
 // allocations of pushpull_common.cpp:476-571), mode wiring (pushpull.cpp
 // flag table) and dispatch to the kernel family of pp_kernels.cuh.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdint>
@@ -711,6 +712,284 @@ int pp_grid_pull_push_backward(const pp_tensor* grad, const pp_tensor* input, co
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (!grad_input) return run(k, ppk::K_PP_BWD, wide, st);
   return scatter_into(k, ppk::K_PP_BWD, grad_input, grad, wide, opt->flags, workspace, workspace_bytes, st);
+}
+
+// Displacement self-composition, the step of scaling-and-squaring
+// (nitorch/spatial/_svf.py:85-94 with _pull_vel, :323-362):
+//   out = u + pull(u, id + u)
+// u, out: (N, *spatial, D) fields, component last (any strides); the pull
+// reads the components of u as its D channels.  out must not alias u.
+static void field_as_image(const pp_tensor* f, int D, int64_t& sN, int64_t& sC, int64_t s[3]) {
+  sN = f->strides[0];
+  sC = f->strides[1 + D];
+  for (int a = 0; a < 3; ++a) s[a] = a < D ? f->strides[1 + a] : 0;
+}
+
+int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_options* opt, void* stream) {
+  Call k;
+  int rc = prepare(k, disp, opt);
+  if (rc) return rc;
+  if ((rc = check_tensor(out, "output"))) return rc;
+  if ((rc = check_same_sizes(out, disp->sizes, disp->ndim, "output"))) return rc;
+  if (out->dtype != disp->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match the field");
+  if (out->data == disp->data) return fail(PP_ERR_ARG, "(): output must not alias the field");
+  k.a.perm = nullptr;
+  k.dtype = disp->dtype;
+  k.a.C = k.D;
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? disp->sizes[1 + a] : 1;
+  k.a.src = disp->data;
+  field_as_image(disp, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.out = out->data;
+  field_as_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  k.a.flags = ppk::F_IDGRID | ppk::F_ADDSELF;
+  return run(k, ppk::K_PULL, need_wide(k, {disp, out}), static_cast<cudaStream_t>(stream));
+}
+
+// Its backward: grad_disp = g + push(g, id + u) + sum_c g_c grad(u_c)(id + u),
+// the gradient of <g, u + pull(u, id + u)> with respect to u, in one pass
+// (the push and the point's own terms accumulate atomically).
+int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const pp_tensor* grad_disp,
+                            const pp_options* opt, void* stream) {
+  Call k;
+  int rc = prepare(k, disp, opt);
+  if (rc) return rc;
+  if (opt->flags & PP_DETERMINISTIC)
+    return fail(PP_ERR_UNSUPPORTED, "(): the self-composition backward has no deterministic mode");
+  if ((rc = check_tensor(grad, "grad"))) return rc;
+  if ((rc = check_same_sizes(grad, disp->sizes, disp->ndim, "grad"))) return rc;
+  if ((rc = check_tensor(grad_disp, "grad_disp"))) return rc;
+  if ((rc = check_same_sizes(grad_disp, disp->sizes, disp->ndim, "grad_disp"))) return rc;
+  if (grad->dtype != disp->dtype || grad_disp->dtype != disp->dtype)
+    return fail(PP_ERR_DTYPE, "(): grad and grad_disp must have the field's dtype");
+  if (grad_disp->data == disp->data || grad_disp->data == grad->data)
+    return fail(PP_ERR_ARG, "(): grad_disp must not alias its inputs");
+  k.a.perm = nullptr;
+  k.dtype = disp->dtype;
+  k.a.C = k.D;
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? disp->sizes[1 + a] : 1;
+  k.a.src = disp->data;
+  field_as_image(disp, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.trgt = grad->data;
+  field_as_image(grad, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  k.a.out = grad_disp->data;
+  field_as_image(grad_disp, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  k.a.flags = ppk::F_A | ppk::F_GRAD | ppk::F_IDGRID | ppk::F_ADDSELF;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((rc = zero_fill(grad_disp, st))) return rc;
+  return run(k, ppk::K_PUSHGRAD, need_wide(k, {disp, grad, grad_disp}), st);
+}
+
+// ---------------------------------------------------------------------------
+// Affine sampling without a materialised grid (resize / reslice):
+// nitorch/spatial/_grid.py builds affine_grid(mat, shape) (:579-615) and
+// calls grid_pull on it (resize :618-754, reslice :860-914).  Here the
+// kernels compute the coordinate A [sub; 1] of every grid point.
+// ---------------------------------------------------------------------------
+
+// mat: (N, D, D+1) or (N, D+1, D+1), rows of D+1 contiguous entries.
+static int check_matrix(const pp_tensor* mat, int D, int64_t N, int dtype) {
+  int rc = check_tensor(mat, "affine");
+  if (rc) return rc;
+  if (mat->ndim != 3 || mat->sizes[2] != D + 1 || (mat->sizes[1] != D && mat->sizes[1] != D + 1))
+    return fail(PP_ERR_ARG, "(): expected affine matrices of shape (N, %d[+1], %d)", D, D + 1);
+  if (mat->sizes[0] != N) return fail(PP_ERR_ARG, "(): expected one affine matrix per batch item");
+  if (mat->strides[2] != 1 || (mat->sizes[1] > 1 && mat->strides[1] != D + 1))
+    return fail(PP_ERR_ARG, "(): affine matrices must have contiguous rows");
+  if (mat->dtype != dtype) return fail(PP_ERR_DTYPE, "(): affine matrices must have the grid dtype");
+  return PP_OK;
+}
+
+// Call set-up of an affine op whose sampling lattice is `lat` (N, C, *shape).
+static int prepare_affine(Call& k, const pp_tensor* lat, const pp_tensor* mat, const pp_options* opt,
+                          int image_dtype) {
+  int rc = check_tensor(lat, "image");
+  if (rc) return rc;
+  if (lat->ndim < 3 || lat->ndim > 5) return fail(PP_ERR_ARG, "(): expected a 1D, 2D or 3D image");
+  k.D = lat->ndim - 2;
+  if ((rc = read_options(opt, k.D, k.bound, k.order))) return rc;
+  const int gdt = grid_dtype_for(image_dtype);
+  if ((rc = check_matrix(mat, k.D, lat->sizes[0], gdt))) return rc;
+  for (int a = 0; a < 3; ++a) { k.a.bound[a] = k.bound[a]; k.a.order[a] = k.order[a]; }
+  k.a.extrapolate = opt->extrapolate;
+  k.a.perm = nullptr;
+  k.a.grid = mat->data;
+  k.a.grid_sN = mat->strides[0];
+  k.a.N = lat->sizes[0];
+  int64_t nv = lat->sizes[0];
+  for (int a = 0; a < 3; ++a) {
+    k.a.trgt_size[a] = a < k.D ? lat->sizes[2 + a] : 1;
+    if (k.a.trgt_size[a] <= 0) return fail(PP_ERR_ARG, "(): expected non-empty spatial dimensions");
+    nv *= k.a.trgt_size[a];
+  }
+  k.a.nvox = nv;
+  k.a.flags = ppk::F_AFFINE;
+  return PP_OK;
+}
+
+int pp_affine_pull(const pp_tensor* input, const pp_tensor* mat, const pp_tensor* out, const pp_options* opt,
+                   void* stream) {
+  Call k;
+  int rc = check_tensor(input, "input");
+  if (rc) return rc;
+  if ((rc = prepare_affine(k, out, mat, opt, input->dtype))) return rc;
+  if (input->ndim != k.D + 2 || input->sizes[0] != out->sizes[0] || input->sizes[1] != out->sizes[1])
+    return fail(PP_ERR_ARG, "(): expected input (N, C, *inshape) and output (N, C, *shape)");
+  for (int i = 2; i < input->ndim; ++i)
+    if (input->sizes[i] <= 0) return fail(PP_ERR_ARG, "(): expected non-empty input");
+  if (out->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match input");
+  k.dtype = input->dtype;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  k.a.src = input->data;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.out = out->data;
+  set_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  return run(k, ppk::K_PULL, need_wide(k, {input, out}), static_cast<cudaStream_t>(stream));
+}
+
+// Adjoint of pp_affine_pull: out (N, C, *outshape) = push of `input`
+// (N, C, *shape, sampled at A [sub; 1]).  Workspace: pp_push_workspace_bytes(out).
+int pp_affine_push(const pp_tensor* input, const pp_tensor* mat, const pp_tensor* out, const pp_options* opt,
+                   void* stream, void* workspace, size_t workspace_bytes) {
+  Call k;
+  int rc = check_tensor(out, "output");
+  if (rc) return rc;
+  if ((rc = prepare_affine(k, input, mat, opt, input->dtype))) return rc;
+  if (out->ndim != k.D + 2 || out->sizes[0] != input->sizes[0] || out->sizes[1] != input->sizes[1])
+    return fail(PP_ERR_ARG, "(): output must be (N, C, *outshape)");
+  for (int i = 2; i < out->ndim; ++i)
+    if (out->sizes[i] <= 0) return fail(PP_ERR_ARG, "(): expected non-empty output shape");
+  if (out->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match input");
+  k.dtype = input->dtype;
+  k.a.trgt = input->data;
+  k.a.C = input->sizes[1];
+  set_image(input, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? out->sizes[2 + a] : 1;
+  return scatter_into(k, ppk::K_PUSH, out, input, need_wide(k, {input, out}), opt->flags, workspace,
+                      workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+size_t pp_affine_grad_workspace_bytes(const pp_tensor* grad) {
+  if (!grad || grad->ndim < 3 || grad->ndim > 5) return 0;
+  const int D = grad->ndim - 2;
+  int64_t n = grad->sizes[0] * D;
+  for (int i = 2; i < grad->ndim; ++i) n *= grad->sizes[i];
+  return ((static_cast<size_t>(n) * 4 + 255) / 256) * 256;
+}
+
+}  // extern "C"
+
+namespace {
+// grad_mat[n, d, e] += sum over the grid points p of item n of
+// gg[p, d] * h_e(p), h = (sub_0, .., sub_{D-1}, 1): one partial sum per
+// CTA (block reduction in shared memory), then D (D+1) atomics per CTA.
+template <int D>
+__global__ void __launch_bounds__(256) affine_reduce(const float* gg, int64_t P, int64_t s1, int64_t s2,
+                                                     float* gm, int64_t gm_sN, int64_t gm_sR) {
+  constexpr int K = D * (D + 1);
+  __shared__ float red[K][8];
+  const int64_t n = blockIdx.y;
+  float acc[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) acc[q] = 0.f;
+  for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < P;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    float h[D + 1];
+    int64_t r = p;  // lattice index, last axis fastest
+    if constexpr (D == 3) {
+      h[2] = static_cast<float>(r % s2); r /= s2;
+      h[1] = static_cast<float>(r % s1); r /= s1;
+    } else if constexpr (D == 2) {
+      h[1] = static_cast<float>(r % s1); r /= s1;
+    }
+    h[0] = static_cast<float>(r);
+    h[D] = 1.f;
+    const float* g = gg + (n * P + p) * D;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const float gd = g[d];
+#pragma unroll
+      for (int e = 0; e <= D; ++e) acc[d * (D + 1) + e] = fmaf(gd, h[e], acc[d * (D + 1) + e]);
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    float v = acc[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[q][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    float v = 0.f;
+    for (int w = 0; w < 8; ++w) v += red[threadIdx.x][w];
+    const int d = threadIdx.x / (D + 1), e = threadIdx.x % (D + 1);
+    atomicAdd(gm + n * gm_sN + d * gm_sR + e, v);
+  }
+}
+}  // namespace
+
+extern "C" {
+
+// Gradient of <grad, affine_pull(input, mat)> with respect to the first D
+// rows of each matrix: per grid point the gradient of the pulled values with
+// respect to the coordinate (sum_c grad_c * d/dx interp(input_c)), then
+// grad_mat[n] = sum_p g(p) [sub_p; 1]^T.  grad_mat: (N, D, D+1) float32,
+// contiguous rows; workspace: pp_affine_grad_workspace_bytes(grad) bytes.
+// float32 / bfloat16 / float16 images only (float32 grid arithmetic).
+int pp_affine_grad_matrix(const pp_tensor* grad, const pp_tensor* input, const pp_tensor* mat,
+                          const pp_tensor* grad_mat, const pp_options* opt, void* stream, void* workspace,
+                          size_t workspace_bytes) {
+  Call k;
+  int rc = check_tensor(input, "input");
+  if (rc) return rc;
+  if (input->dtype == PP_FLOAT64) return fail(PP_ERR_DTYPE, "(): affine matrix gradients are float32 only");
+  if ((rc = prepare_affine(k, grad, mat, opt, input->dtype))) return rc;
+  if (input->ndim != k.D + 2 || input->sizes[0] != grad->sizes[0] || input->sizes[1] != grad->sizes[1])
+    return fail(PP_ERR_ARG, "(): expected input (N, C, *inshape) and grad (N, C, *shape)");
+  if (grad->dtype != input->dtype) return fail(PP_ERR_DTYPE, "(): grad dtype must match input");
+  if ((rc = check_tensor(grad_mat, "grad_affine"))) return rc;
+  if (grad_mat->ndim != 3 || grad_mat->sizes[0] != grad->sizes[0] || grad_mat->sizes[1] != k.D ||
+      grad_mat->sizes[2] != k.D + 1 || grad_mat->strides[2] != 1 || grad_mat->dtype != PP_FLOAT32)
+    return fail(PP_ERR_ARG, "(): expected a float32 (N, %d, %d) grad_affine with contiguous rows", k.D, k.D + 1);
+  const size_t need = pp_affine_grad_workspace_bytes(grad);
+  if (!workspace || workspace_bytes < need)
+    return fail(PP_ERR_WORKSPACE, "(): the affine gradient needs %zu bytes of workspace", need);
+  k.dtype = input->dtype;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  k.a.src = input->data;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.trgt = grad->data;
+  set_image(grad, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  // per-point coordinate gradients (N, *shape, D), contiguous
+  float* gg = static_cast<float*>(workspace);
+  const int64_t P = k.a.nvox / k.a.N;
+  k.a.gg = gg;
+  k.a.gg_sN = P * k.D;
+  k.a.gg_sD = 1;
+  {
+    int64_t sd = k.D;
+    for (int a = k.D - 1; a >= 0; --a) { k.a.gg_s[a] = sd; sd *= k.a.trgt_size[a]; }
+    for (int a = k.D; a < 3; ++a) k.a.gg_s[a] = 0;
+  }
+  k.a.flags |= ppk::F_GRAD;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((rc = run(k, ppk::K_PULLGRAD, need_wide(k, {input, grad}), st))) return rc;
+  if ((rc = zero_fill(grad_mat, st))) return rc;
+  const int64_t blocks = std::min<int64_t>((P + 255) / 256, 148 * 4);
+  dim3 g(static_cast<unsigned>(blocks), static_cast<unsigned>(k.a.N), 1);
+  float* gm = static_cast<float*>(grad_mat->data);
+  if (k.D == 3)
+    affine_reduce<3><<<g, 256, 0, st>>>(gg, P, k.a.trgt_size[1], k.a.trgt_size[2], gm, grad_mat->strides[0],
+                                        grad_mat->strides[1]);
+  else if (k.D == 2)
+    affine_reduce<2><<<g, 256, 0, st>>>(gg, P, k.a.trgt_size[1], 1, gm, grad_mat->strides[0],
+                                        grad_mat->strides[1]);
+  else
+    affine_reduce<1><<<g, 256, 0, st>>>(gg, P, 1, 1, gm, grad_mat->strides[0], grad_mat->strides[1]);
+  count_launch();
+  return cuda_check(cudaGetLastError(), "affine gradient reduction");
 }
 
 }  // extern "C"

@@ -38,8 +38,18 @@ namespace ppk {
 
 enum Mode : int { K_PULL = 0, K_SGRAD, K_PUSH, K_COUNT, K_PULLGRAD, K_PUSHGRAD, K_KD,
                   K_PP, K_PP_BWD, K_NMODES };
-enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4, F_VEC = 8 };  // F_A: pull (PULLGRAD) / push (PUSHGRAD, KD)
+enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4, F_VEC = 8, F_IDGRID = 16, F_ADDSELF = 32, F_AFFINE = 64 };
+// F_A: pull (PULLGRAD) / push (PUSHGRAD, KD)
 // F_VEC: `out` is a channel-interleaved float accumulator (pp_lanes_kernel)
+// F_IDGRID: the sampling coordinate is the point's own voxel plus the grid
+//   value (the grid holds a displacement, not a transformation)
+// F_ADDSELF (with F_IDGRID, C = D; displacement self-composition):
+//   K_PULL      out = src(point) + pulled value        (u + u o (id + u))
+//   K_PUSHGRAD  out += g(point) + grid gradient at the point, atomically,
+//               on top of the push of g (its adjoint w.r.t. u)
+// F_AFFINE: no grid tensor: the coordinate of grid point `sub` is
+//   A [sub; 1], A the D x (D+1) row-major matrix of batch item n at
+//   grid + n * grid_sN (resize / reslice without a materialised grid)
 
 struct PPArgs {
   const void* src;   // gathered tensor (N, C, *src_size)
@@ -175,14 +185,29 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
                            MODE == K_PP || MODE == K_PP_BWD;
 
   // ---- coordinates ------------------------------------------------------
-  const T* gp = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
-  int64_t goff = 0;
-#pragma unroll
-  for (int d = 0; d < D; ++d) goff += static_cast<int64_t>(sub[d]) * a.grid_s[d];
-  gp += goff;
   T coord[3];
+  if (a.flags & F_AFFINE) {
+    const T* m = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
 #pragma unroll
-  for (int d = 0; d < D; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
+    for (int d = 0; d < D; ++d) {
+      T x = __ldg(m + d * (D + 1) + D);
+#pragma unroll
+      for (int e = 0; e < D; ++e) x = fma(__ldg(m + d * (D + 1) + e), static_cast<T>(sub[e]), x);
+      coord[d] = x;
+    }
+  } else {
+    const T* gp = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
+    int64_t goff = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) goff += static_cast<int64_t>(sub[d]) * a.grid_s[d];
+    gp += goff;
+#pragma unroll
+    for (int d = 0; d < D; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
+  }
+  if (a.flags & F_IDGRID) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) coord[d] += static_cast<T>(sub[d]);
+  }
 
   const bool do_a = (a.flags & F_A) != 0;
   const bool do_grad = (a.flags & F_GRAD) != 0;
@@ -206,6 +231,26 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
 #pragma unroll
     for (int d = 0; d < D; ++d) inb = inb && in_fov<T>(coord[d], a.src_size[d], tol);
     if (!((a.extrapolate & 1) || inb)) {
+      if (a.flags & F_ADDSELF) {
+        // self-composition outside the field of view: only the identity terms
+        int64_t so = 0, oo = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          so += static_cast<int64_t>(sub[d]) * a.src_s[d];
+          oo += static_cast<int64_t>(sub[d]) * a.out_s[d];
+        }
+        if (MODE == K_PULL) {
+          const S* sp = static_cast<const S*>(a.src) + static_cast<int64_t>(n) * a.src_sN + so;
+          S* op = static_cast<S*>(a.out) + ovox;
+          for (int64_t c = 0; c < a.C; ++c) op[c * a.out_sC] = sp[c * a.src_sC];
+        }
+        if (MODE == K_PUSHGRAD) {
+          const S* tp = static_cast<const S*>(a.trgt) + tvox;
+          T* op = static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN + oo;
+          for (int64_t c = 0; c < a.C; ++c) atomic_acc(op + c * a.out_sC, ldg_acc(tp + c * a.trgt_sC));
+        }
+        return;
+      }
       if (MODE == K_PULL || MODE == K_SGRAD || (MODE == K_PULLGRAD && do_a)) {
         S* op = static_cast<S*>(a.out) + ovox;
         for (int64_t c = 0; c < a.C; ++c) {
@@ -346,6 +391,15 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
 #pragma unroll
           PP_CB acc[cb] = fma(az.w[k], accy[cb], acc[cb]);
         }
+      }
+#pragma unroll
+      if (a.flags & F_ADDSELF) {
+        // self-composition: add the field's own value at the point
+        int64_t so = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) so += static_cast<int64_t>(sub[d]) * a.src_s[d];
+#pragma unroll
+        PP_CB if (CB == 1 || cb < nc) acc[cb] += ldg_acc(sp + cb * a.src_sC + so);
       }
 #pragma unroll
       PP_CB if (CB == 1 || cb < nc) op[(c0 + cb) * a.out_sC] = from_acc<S>(acc[cb]);
@@ -546,7 +600,17 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
 #pragma unroll
       PP_CB { og0 = fma(t[cb], gx[cb], og0); og1 = fma(t[cb], gy[cb], og1); og2 = fma(t[cb], gz[cb], og2); }
     }
-    if (do_grad) {
+    if (a.flags & F_ADDSELF) {
+      // self-composition backward: g and the grid gradient at the point go to
+      // the same output as the push, atomically
+      int64_t oo = 0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) oo += static_cast<int64_t>(sub[d]) * a.out_s[d];
+      T* op = static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN + oo;
+      const T og[3] = {og0, og1, og2};
+#pragma unroll
+      for (int d = 0; d < D; ++d) atomic_acc(op + d * a.out_sC, og[d] + ldg_acc(trg_v + d * a.trgt_sC));
+    } else if (do_grad) {
       T* g = static_cast<T*>(a.gg) + gvox;
       g[0] = og0;
       if (D > 1) g[a.gg_sD] = og1;
@@ -915,13 +979,23 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_lanes_k
   const T* gp = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
   int64_t tvox = static_cast<int64_t>(n) * a.trgt_sN;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    gp += static_cast<int64_t>(sub[d]) * a.grid_s[d];
-    tvox += static_cast<int64_t>(sub[d]) * a.trgt_s[d];
-  }
+  for (int d = 0; d < 3; ++d) tvox += static_cast<int64_t>(sub[d]) * a.trgt_s[d];
   T coord[3];
+  if (a.flags & F_AFFINE) {
+    // coordinate A [sub; 1] (gp points at this item's 3 x 4 matrix)
 #pragma unroll
-  for (int d = 0; d < 3; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
+    for (int d = 0; d < 3; ++d) {
+      T x = __ldg(gp + d * 4 + 3);
+#pragma unroll
+      for (int e = 0; e < 3; ++e) x = fma(__ldg(gp + d * 4 + e), static_cast<T>(sub[e]), x);
+      coord[d] = x;
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) gp += static_cast<int64_t>(sub[d]) * a.grid_s[d];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
+  }
   {
     const T tol = (a.extrapolate & 2) ? static_cast<T>(0.5 + 5e-2) : static_cast<T>(5e-2);
     bool inb = true;

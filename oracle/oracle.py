@@ -298,3 +298,59 @@ def spline_coeff_nd(inp, bound_ts, order, dim=None):
 
 # compiled-backend bound code -> prefilter code (grid.py:133 via _TSBoundType)
 BOUND_TO_TS = {0: 1, 1: 2, 2: 3, 3: 4, 4: 5, 5: 6, 7: 0}
+
+
+# --------------------------------------------------------------------- #
+# Stationary velocity fields: scaling and squaring (FP64)               #
+# --------------------------------------------------------------------- #
+
+def _identity_np(shape):
+    mesh = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
+    return np.stack(mesh, -1)
+
+
+def svf_compose(u, bound=5, order=1, extrapolate=1):
+    """u + pull(u, id + u) for a displacement u (N, *spatial, D): the step of
+    nitorch/spatial/_svf.py:85-94, with _pull_vel (:323-362) moving the
+    components to the channel axis and pulling at id + u."""
+    u = np.asarray(u, np.float64)
+    img = np.moveaxis(u, -1, 1)
+    grid = _identity_np(u.shape[1:-1])[None] + u
+    pulled = grid_pull(img, grid, [bound], [order], extrapolate)
+    return u + np.moveaxis(pulled, 1, -1)
+
+
+def svf_compose_backward(g, u, bound=5, order=1, extrapolate=1):
+    """Exact gradient of <g, svf_compose(u)> w.r.t. u: g, plus the pull's
+    input gradient (a push of g) and its grid gradient (d grid / d u = I)."""
+    u = np.asarray(u, np.float64)
+    g = np.asarray(g, np.float64)
+    img = np.moveaxis(u, -1, 1)
+    grid = _identity_np(u.shape[1:-1])[None] + u
+    gi, gg = grid_pull_backward(np.moveaxis(g, -1, 1), img, grid, [bound], [order], extrapolate)
+    return g + np.moveaxis(gi, 1, -1) + gg
+
+
+def svf_exp(vel, steps=8, bound=5, order=1, inverse=False, displacement=False):
+    """nitorch/spatial/_svf.py:47-98 (exp_forward): scale by 2^-steps, then
+    `steps` self-compositions; returns the transformation (id + u) unless
+    `displacement`.  vel: (N, *spatial, D)."""
+    u = (-1.0 if inverse else 1.0) * np.asarray(vel, np.float64) / 2 ** steps
+    for _ in range(steps):
+        u = svf_compose(u, bound, order)
+    return u if displacement else u + _identity_np(u.shape[1:-1])[None]
+
+
+def svf_exp_backward(vel, grad, steps=8, bound=5, order=1, inverse=False):
+    """Gradient of <grad, svf_exp(vel)> w.r.t. vel by the chain rule through
+    the compositions (what autograd computes on the reference's default
+    path)."""
+    u = (-1.0 if inverse else 1.0) * np.asarray(vel, np.float64) / 2 ** steps
+    states = []
+    for _ in range(steps):
+        states.append(u)
+        u = svf_compose(u, bound, order)
+    g = np.asarray(grad, np.float64)
+    for s in reversed(states):
+        g = svf_compose_backward(g, s, bound, order)
+    return (-1.0 if inverse else 1.0) * g / 2 ** steps

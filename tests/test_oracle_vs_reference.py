@@ -156,3 +156,37 @@ def test_float32_order0_bit_exact():
                 # several samples landing on one voxel; compare exactly on
                 # voxels hit once and to 1 ulp elsewhere
                 np.testing.assert_allclose(m, r, rtol=2e-7, atol=1e-7)
+
+
+def _ref_svf_exp(vel, steps, bound, order):
+    """nitorch/spatial/_svf.py:85-94 driven by the reference's own compiled
+    grid_pull (the _pull_vel wiring of :323-362: components moved to the
+    channel axis, dft bound, extrapolation on)."""
+    b, o = [ref.BoundType(bound)], [ref.InterpolationType(order)]
+    u = torch.as_tensor(vel) / 2 ** steps
+    shape = u.shape[1:-1]
+    idg = torch.stack(torch.meshgrid(*[torch.arange(s, dtype=torch.float64) for s in shape], indexing="ij"), -1)
+    for _ in range(steps):
+        pulled = ref.grid_pull(u.movedim(-1, 1).contiguous(), idg[None] + u, b, o, 1)
+        u = u + pulled.movedim(1, -1)
+    return (u + idg[None]).numpy()
+
+
+@pytest.mark.parametrize("bound", [5, 2])
+@pytest.mark.parametrize("order", [1, 3])
+def test_svf_exp_restatement(bound, order):
+    rng = np.random.default_rng(order * 10 + bound)
+    vel = rng.standard_normal((1, 7, 8, 6, 3)) * 2.0
+    mine = O.svf_exp(vel, steps=6, bound=bound, order=order)
+    theirs = _ref_svf_exp(vel, 6, bound, order)
+    assert np.abs(mine - theirs).max() / np.abs(theirs).max() < 1e-12
+
+
+def test_svf_backward_restatement_finite_differences():
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal((1, 5, 6, 4, 3)) * 0.7
+    g, d = rng.standard_normal(u.shape), rng.standard_normal(u.shape)
+    an = (O.svf_exp_backward(u, g, steps=3) * d).sum()
+    e = 1e-6
+    fd = ((O.svf_exp(u + e * d, steps=3) * g).sum() - (O.svf_exp(u - e * d, steps=3) * g).sum()) / (2 * e)
+    assert abs(an - fd) <= 1e-8 * abs(fd)
