@@ -16,7 +16,8 @@ roofline of the dominant kernel, the CPU baseline (the reference's own C++
 backend on a bounded sample), clocks and kernel-launch counts; `fused`
 reports the same step through the fused pull_push operator, and `batched`
 the config-4 workload (64 uneven volumes, float32 and bfloat16) as one
-captured batched step against the per-call loop.
+captured batched step against the per-call loop; `svf` times config-5
+registration iterations (velocity exponentiation, warp, MSE, backward).
 --impl reference times the reference's CPU implementation of the same step
 on the host cores (bounded sample) and prints the same metric.
 With N > 1 (torchrun), every rank runs an independent replica of the
@@ -464,6 +465,42 @@ def bf16_error(b):
             "bound": "2^-8 (one bf16 rounding of the pulled values; non-negative image) + 1e-5"}
 
 
+# ---------------------------------------------------------------------- #
+# config 5: registration iterations through the SVF exponentiation        #
+# ---------------------------------------------------------------------- #
+def run_svf(args, rank, world, device):
+    """Config 5: velocity 1x160x192x160x3 (N(0,1) smoothed sigma 3), moving
+    and fixed images 1x1x160x192x160; one iteration = exp(v) by 8 squarings
+    (linear, dft, extrapolate) -> pull of the moving image at order 3, dct2
+    -> MSE -> backward through every pull -> gradient step on v."""
+    import nitorch_b200 as nb
+    from nitorch_b200 import svf, workloads
+    v, mov, fix = workloads.config5()
+    v, mov, fix = v.float().to(device), mov.float().to(device), fix.float().to(device)
+    nvox = int(np.prod(v.shape[1:-1]))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def iteration():
+        vr = v.detach().requires_grad_(True)
+        phi = svf.exp(vr)
+        w = nb.grid_pull(mov, phi, 3, "dct2", False)
+        loss = ((w - fix) ** 2).mean()
+        loss.backward()
+        with torch.no_grad():
+            v.sub_(vr.grad, alpha=1.0)
+        return loss
+
+    for _ in range(args.warmup):
+        iteration()
+    torch.cuda.synchronize()
+    total_ms, launches, _ = timed_steps(iteration, args, world, device, flush, steps=args.svf_steps)
+    return {"workload": "cfg5: exp(v) by 8 squarings (linear, dft) -> pull moving (cubic, dct2) -> MSE -> "
+                        "backward -> step; 1x160x192x160",
+            "ms_per_iteration": round(total_ms / args.svf_steps, 3),
+            "value": round(world * nvox * args.svf_steps / (total_ms * 1e-3) / 1e9, 4), "unit": "Gvox/s",
+            "gpu_launches_per_iteration": round(launches / args.svf_steps, 1)}
+
+
 def run_all(args, rank, world, device):
     import gc
     line = run_b200(args, rank, world, device)
@@ -476,6 +513,12 @@ def run_all(args, rank, world, device):
         if line is not None:
             b["gpu_launches"] = _lib.kernel_launches() - l0
             line["batched"] = b
+        gc.collect()
+        torch.cuda.empty_cache()
+    if not args.no_svf:
+        r = run_svf(args, rank, world, device)
+        if line is not None:
+            line["svf"] = r
     return line
 
 
@@ -575,6 +618,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-volumes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--no-svf", action="store_true")
+    ap.add_argument("--svf-steps", type=int, default=5)
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")
     args = ap.parse_args()

@@ -3,7 +3,7 @@
 and this library's, on the same B200, the same inputs and the same chain --
 a measurement script, not a test (pytest does not collect it).
 
-    python tests/perf_reference_cuda.py [--size 192] [--steps 5] [--warmup 3]
+    python tests/perf_reference_cuda.py [--size 192] [--steps 5] [--warmup 3] [--svf]
 
 Workload: the config-2 chain without the prefilter (the reference's
 prefilter is Python code in a third-party package that is not present):
@@ -72,11 +72,67 @@ def timed(mod, x, g, w, steps, warmup, flush):
     return out, float(np.median(tot)), {k: round(float(np.median(v)), 4) for k, v in per.items()}
 
 
+def make_pull(mod):
+    """Autograd wrapper of a backend's native grid_pull, as nitorch/_C/grid.py
+    (GridPull, 192-230) wraps the reference's: the backward asks for the
+    gradients of the inputs that require them."""
+    class Pull(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, inp, grid, bound, order, ex):
+            ctx.opt = (bound, order, ex)
+            ctx.save_for_backward(inp, grid)
+            return mod.grid_pull(inp, grid, bound, order, ex)
+
+        @staticmethod
+        def backward(ctx, g):
+            inp, grid = ctx.saved_tensors
+            grads = list(mod.grid_pull_backward(g.contiguous(), inp, grid, *ctx.opt))
+            gi = grads.pop(0) if ctx.needs_input_grad[0] else None
+            gg = grads.pop(0) if ctx.needs_input_grad[1] else None
+            return gi, gg, None, None, None
+    return Pull.apply
+
+
+def svf_iteration(mod, v, mov, fix, idg):
+    """Config-5 iteration through one backend's native pull: exp(v) by 8
+    squarings u <- u + pull(u, id + u) (linear, dft, extrapolate; the
+    reference's exp_forward, nitorch/spatial/_svf.py:85-94), pull of the
+    moving image (cubic, dct2), MSE, backward."""
+    pull = make_pull(mod)
+    lin, dft = [mod.InterpolationType.linear], [mod.BoundType.dft]
+    cub, dct2 = [mod.InterpolationType.cubic], [mod.BoundType.dct2]
+    vr = v.detach().requires_grad_(True)
+    u = vr / 256.0
+    for _ in range(8):
+        u = u + pull(u.movedim(-1, 1).contiguous(), idg + u, dft, lin, 1).movedim(1, -1)
+    w = pull(mov, idg + u, dct2, cub, 0)
+    loss = ((w - fix) ** 2).mean()
+    loss.backward()
+    return loss.detach(), vr.grad
+
+
+def time_svf(mod, v, mov, fix, idg, steps, warmup):
+    for _ in range(warmup):
+        svf_iteration(mod, v, mov, fix, idg)
+    torch.cuda.synchronize()
+    ts = []
+    out = None
+    for _ in range(steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        out = svf_iteration(mod, v, mov, fix, idg)
+        e.record()
+        torch.cuda.synchronize()
+        ts.append(s.elapsed_time(e))
+    return out, float(np.median(ts))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--size", type=int, default=192)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--svf", action="store_true", help="also time a config-5 registration iteration")
     args = ap.parse_args()
     from nitorch_b200 import spatial, workloads
     from oracle.reference import load_compiled_cuda
@@ -103,6 +159,23 @@ def main():
     for k, a, b in zip(names, outs["b200"], outs["reference_cuda"]):
         a, b = a.double(), b.double()
         res["max_rel_diff"][k] = float((a - b).abs().max() / b.abs().max().clamp_min(1e-30))
+    if args.svf:
+        v5, mov, fix = workloads.config5()
+        v5, mov, fix = v5.float().to(dev), mov.float().to(dev), fix.float().to(dev)
+        shape = v5.shape[1:-1]
+        idg = torch.stack(torch.meshgrid(*[torch.arange(n, dtype=torch.float32, device=dev) for n in shape],
+                                         indexing="ij"), -1)[None]
+        sv = {"workload": "cfg5 iteration: exp(v) 8 squarings (linear, dft) -> pull moving (cubic, dct2) -> "
+                          "MSE -> backward, 1x160x192x160, both backends through the same autograd wiring"}
+        outs5 = {}
+        for name, mod in (("reference_cuda", ref), ("b200", spatial)):
+            out, ms = time_svf(mod, v5, mov, fix, idg, max(2, args.steps // 2), 2)
+            outs5[name] = out
+            sv[name] = {"ms_per_iteration": round(ms, 3)}
+        sv["speedup"] = round(sv["reference_cuda"]["ms_per_iteration"] / sv["b200"]["ms_per_iteration"], 2)
+        ga, gb = outs5["b200"][1].double(), outs5["reference_cuda"][1].double()
+        sv["grad_max_rel_diff"] = float((ga - gb).abs().max() / gb.abs().max().clamp_min(1e-30))
+        res["svf"] = sv
     print(json.dumps(res), flush=True)
 
 
