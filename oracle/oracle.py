@@ -354,3 +354,60 @@ def svf_exp_backward(vel, grad, steps=8, bound=5, order=1, inverse=False):
     for s in reversed(states):
         g = svf_compose_backward(g, s, bound, order)
     return (-1.0 if inverse else 1.0) * g / 2 ** steps
+
+
+# --------------------------------------------------------------------- #
+# Jacobians of transformation fields (FP64)                             #
+# --------------------------------------------------------------------- #
+
+def _central_diff1d(x, axis, bound, vs):
+    """nitorch/spatial/_finite_differences.py:32-222, order 1, side 'c':
+    (x[i+1] - x[i-1]) / (2 vs) with the bound's value beyond each end; a
+    singleton axis returns x itself (:87-91)."""
+    x = np.moveaxis(np.asarray(x, np.float64), axis, 0)
+    n = x.shape[0]
+    if n == 1:
+        return np.moveaxis(x.copy(), 0, axis)
+    d = np.empty_like(x)
+    d[1:-1] = x[2:] - x[:-2]
+    if bound in ("dct2", "replicate"):
+        d[0] = x[1] - x[0]
+        d[-1] = x[-1] - x[-2]
+    elif bound == "dct1":
+        d[0] = 0
+        d[-1] = 0
+    elif bound == "dst2":
+        d[0] = x[1] + x[0]
+        d[-1] = -(x[-1] + x[-2])
+    elif bound in ("dst1", "zero"):
+        d[0] = x[1]
+        d[-1] = -x[-2]
+    elif bound == "dft":
+        d[0] = x[1] - x[-1]
+        d[-1] = x[0] - x[-2]
+    else:
+        raise ValueError(bound)
+    d /= 2 * vs
+    return np.moveaxis(d, 0, axis)
+
+
+def grid_jacobian(grid, bound="dft", voxel_size=1, type="grid", add_identity=True):
+    """nitorch/spatial/_grid.py:917-969 without `sample`: central finite
+    differences of the displacement; jac[..., i, j] = d psi_i / d x_j.
+    grid: (N, *spatial, D)."""
+    g = np.asarray(grid, np.float64)
+    D = g.shape[-1]
+    spatial = g.shape[1:-1]
+    vs = list(voxel_size) if isinstance(voxel_size, (list, tuple)) else [voxel_size] * D
+    if type == "grid":
+        g = g - _identity_np(spatial)[None]
+    jac = np.stack([_central_diff1d(g, 1 + j, bound, vs[j]) for j in range(D)], -1)
+    if add_identity:
+        for i in range(D):
+            jac[..., i, i] += 1
+    return jac
+
+
+def grid_jacdet(grid, bound="dft", voxel_size=1, type="grid", add_identity=True):
+    """nitorch/spatial/_grid.py:972-1013: det of grid_jacobian."""
+    return np.linalg.det(grid_jacobian(grid, bound, voxel_size, type, add_identity))

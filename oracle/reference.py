@@ -6,6 +6,10 @@
 * ``load_compiled_cuda()``: the same module built with the reference's CUDA
   backend for sm_100a by ``oracle/build_ref_cuda.py`` (``oracle/_ref/cuda/``),
   used to time the reference's own GPU kernels beside this library's.
+* ``load_spatial()``: the reference's own ``nitorch.spatial`` package,
+  imported from the reference tree with the compiled CPU backend as
+  ``nitorch._C.spatial`` and the vendored TorchScript package as
+  ``interpol`` (the import shim: only where the reference tree is present).
 * ``load_ts_coeff()``: the reference's vendored prefilter
   ``nitorch/_C/_ts/coeff.py`` imported from the reference tree, when that
   tree is present (only in the development container, never on a GPU box).
@@ -68,3 +72,35 @@ def load_ts_coeff():
         spec.loader.exec_module(pkg)
         _ts = sys.modules["_ref_interpol.coeff"]
     return _ts
+
+
+_spatial = None
+
+
+def load_spatial():
+    """The reference's nitorch.spatial (Python layer over its compiled CPU
+    backend), or None if the reference tree or the compiled backend is
+    absent."""
+    global _spatial
+    if _spatial is not None:
+        return _spatial
+    ref = load_compiled()
+    root = os.path.join(REFERENCE_ROOT, "nitorch", "_C", "_ts")
+    if ref is None or not os.path.isdir(root):
+        return None
+    os.environ.setdefault("NI_COMPILED_BACKEND", "C")
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        if "interpol" not in sys.modules:
+            spec = importlib.util.spec_from_file_location("interpol", os.path.join(root, "__init__.py"),
+                                                          submodule_search_locations=[root])
+            pkg = importlib.util.module_from_spec(spec)
+            sys.modules["interpol"] = pkg
+            spec.loader.exec_module(pkg)
+        sys.modules.setdefault("nitorch._C.spatial", ref)
+        if REFERENCE_ROOT not in sys.path:
+            sys.path.append(REFERENCE_ROOT)
+        import nitorch.spatial as S  # noqa: E402
+    _spatial = S
+    return S

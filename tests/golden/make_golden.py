@@ -15,6 +15,12 @@ Writes
                         spline_coeff_nd volumes.
   config1_golden.npz  : checksums of the reference's pull / push on the
                         seeded config-1 workload (1x1x64^3, order 1, dct2).
+  spatial_golden.npz  : outputs of the reference's nitorch.spatial callers of
+                        the path (grid_jacobian / grid_jacdet, resize,
+                        reslice, exp of a velocity field and its autograd
+                        gradient) on seeded float64 inputs.
+                        (`python tests/golden/make_golden.py spatial` writes
+                        this file alone.)
 
 Reference defects are handled as in tests/test_oracle_vs_reference.py: the
 grid_grad_backward target is laid out with a last-dimension stride > 1 (D2),
@@ -142,7 +148,69 @@ def config1(ref):
     return {k: np.asarray(v) for k, v in out.items()}
 
 
+def spatial(S):
+    """nitorch.spatial callers of the push/pull path, float64."""
+    out = {}
+    g = torch.Generator().manual_seed(77)
+    # Jacobians by central differences, all bounds, both field types
+    f3 = torch.randn((1, 7, 6, 5, 3), generator=g, dtype=torch.float64)
+    f2 = torch.randn((1, 8, 9, 2), generator=g, dtype=torch.float64)
+    f1s = torch.randn((1, 6, 1, 5, 3), generator=g, dtype=torch.float64)  # a singleton axis
+    out["jac_f3"], out["jac_f2"], out["jac_f1s"] = f3.numpy(), f2.numpy(), f1s.numpy()
+    for b in ("dft", "dct2", "dct1", "dst1", "dst2", "zero", "replicate"):
+        for typ in ("grid", "disp"):
+            out[f"jac3_{b}_{typ}"] = S.grid_jacobian(f3, bound=b, type=typ).numpy()
+            out[f"jacdet3_{b}_{typ}"] = S.grid_jacdet(f3, bound=b, type=typ).numpy()
+            out[f"jac2_{b}_{typ}"] = S.grid_jacobian(f2, bound=b, type=typ).numpy()
+        out[f"jac1s_{b}"] = S.grid_jacobian(f1s, bound=b, type="disp").numpy()
+    out["jac3_vs"] = S.grid_jacobian(f3, bound="dct2", voxel_size=[1.5, 2.0, 0.5], type="disp",
+                                     add_identity=False).numpy()
+    smp = torch.rand((1, 4, 5, 3, 3), generator=g, dtype=torch.float64) * 5
+    out["jac_sample"] = smp.numpy()
+    out["jac3_sampled"] = S.grid_jacobian(f3, sample=smp, bound="dft", type="disp").numpy()
+    # resize: anchors x factors, cubic dct2 (prefilter on by default)
+    x = torch.randn((1, 2, 9, 8, 7), generator=g, dtype=torch.float64)
+    out["resize_x"] = x.numpy()
+    for a in ("c", "e", "f", "l"):
+        for k, fct in enumerate((2.0, 0.5, 1.7)):
+            out[f"resize_{a}_{k}"] = S.resize(x, factor=fct, anchor=a, interpolation=3, bound="dct2").numpy()
+    out["resize_shape"] = S.resize(x, shape=(5, 11, 6), interpolation=1, bound="dct2").numpy()
+    aff = torch.eye(4, dtype=torch.float64)
+    aff[:3, :3] = torch.diag(torch.tensor([1.2, 0.9, 2.0], dtype=torch.float64))
+    aff[:3, 3] = torch.tensor([3.0, -1.0, 0.5], dtype=torch.float64)
+    rz, raff = S.resize(x, factor=1.5, affine=aff, anchor="c", interpolation=1, bound="dct2")
+    out["resize_aff_in"], out["resize_aff_out"], out["resize_aff_img"] = aff.numpy(), raff.numpy(), rz.numpy()
+    # reslice: linear, zero bound (defaults), shape_to given
+    y = torch.randn((1, 1, 10, 9, 8), generator=g, dtype=torch.float64)
+    a_from = torch.eye(4, dtype=torch.float64)
+    a_from[:3, :3] *= 1.5
+    a_to = torch.eye(4, dtype=torch.float64)
+    a_to[:3, :3] += 0.1 * torch.randn((3, 3), generator=g, dtype=torch.float64)
+    a_to[:3, 3] = torch.tensor([1.0, 2.0, -0.5], dtype=torch.float64)
+    out["reslice_x"], out["reslice_from"], out["reslice_to"] = y.numpy(), a_from.numpy(), a_to.numpy()
+    out["reslice_out"] = S.reslice(y, a_from, a_to, (7, 8, 9)).numpy()
+    # velocity exponentiation, forward and autograd gradient
+    v = torch.randn((1, 8, 9, 7, 3), generator=g, dtype=torch.float64)
+    v = torch.nn.functional.avg_pool3d(v.movedim(-1, 1), 3, 1, 1).movedim(1, -1) * 3
+    w = torch.randn(v.shape, generator=g, dtype=torch.float64)
+    out["exp_v"], out["exp_w"] = v.numpy(), w.numpy()
+    out["exp_fwd"] = S.exp(v).numpy()
+    out["exp_inv_disp"] = S.exp(v, inverse=True, displacement=True).numpy()
+    vr = v.clone().requires_grad_(True)
+    (S.exp(vr) * w).sum().backward()
+    out["exp_grad"] = vr.grad.numpy()
+    return {k: np.asarray(v) for k, v in out.items()}
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "spatial":
+        S = R.load_spatial()
+        if S is None:
+            raise SystemExit("reference tree / compiled backend not found")
+        torch.set_num_threads(1)
+        np.savez_compressed(os.path.join(HERE, "spatial_golden.npz"), **spatial(S))
+        print("spatial_golden.npz", os.path.getsize(os.path.join(HERE, "spatial_golden.npz")))
+        return
     ref = R.load_compiled()
     if ref is None:
         raise SystemExit("build the reference first: python oracle/build_ref.py")

@@ -114,3 +114,36 @@ def test_config1_checksums():
     a, b = (p * y).sum(), (x * q).sum()
     assert abs(a - b) <= 1e-12 * abs(a)
     np.testing.assert_allclose(a, C1["inner_pull_y"], rtol=1e-12)
+
+
+SPATIAL = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "spatial_golden.npz"))
+JAC_BOUNDS = ("dft", "dct2", "dct1", "dst1", "dst2", "zero", "replicate")
+
+
+@pytest.mark.parametrize("bound", JAC_BOUNDS)
+@pytest.mark.parametrize("typ", ["grid", "disp"])
+def test_oracle_jacobian_vs_reference_golden(bound, typ):
+    f3, f2 = SPATIAL["jac_f3"], SPATIAL["jac_f2"]
+    np.testing.assert_allclose(O.grid_jacobian(f3, bound, type=typ), SPATIAL[f"jac3_{bound}_{typ}"],
+                               rtol=0, atol=1e-12)
+    np.testing.assert_allclose(O.grid_jacdet(f3, bound, type=typ), SPATIAL[f"jacdet3_{bound}_{typ}"],
+                               rtol=1e-10, atol=1e-10)
+    np.testing.assert_allclose(O.grid_jacobian(f2, bound, type=typ), SPATIAL[f"jac2_{bound}_{typ}"],
+                               rtol=0, atol=1e-12)
+    np.testing.assert_allclose(O.grid_jacobian(SPATIAL["jac_f1s"], bound, type="disp"),
+                               SPATIAL[f"jac1s_{bound}"], rtol=0, atol=1e-12)
+
+
+def test_oracle_jacobian_voxel_size_vs_reference_golden():
+    np.testing.assert_allclose(O.grid_jacobian(SPATIAL["jac_f3"], "dct2", [1.5, 2.0, 0.5], "disp", False),
+                               SPATIAL["jac3_vs"], rtol=0, atol=1e-12)
+
+
+def test_oracle_svf_vs_reference_golden():
+    v, w = SPATIAL["exp_v"], SPATIAL["exp_w"]
+    ref = SPATIAL["exp_fwd"]
+    assert np.abs(O.svf_exp(v) - ref).max() <= 1e-11 * np.abs(ref).max()
+    ref = SPATIAL["exp_inv_disp"]
+    assert np.abs(O.svf_exp(v, inverse=True, displacement=True) - ref).max() <= 1e-11 * np.abs(ref).max()
+    ref = SPATIAL["exp_grad"]
+    assert np.abs(O.svf_exp_backward(v, w) - ref).max() <= 1e-10 * np.abs(ref).max()
