@@ -214,6 +214,33 @@ PP_API int pp_affine_grad_matrix(const pp_tensor* grad, const pp_tensor* input, 
                                  const pp_tensor* grad_mat, const pp_options* opt, void* stream,
                                  void* workspace, size_t workspace_bytes);
 
+/* ---- Jacobians of transformation / displacement fields ----------------
+ * nitorch.spatial.grid_jacobian / grid_jacdet (nitorch/spatial/_grid.py:
+ * 917-1013) without `sample`: central finite differences of the
+ * displacement (nitorch/spatial/_finite_differences.py:32-222, order 1,
+ * side 'c'; the bound code gives the values beyond each end; a singleton
+ * axis yields the values themselves, as there), plus the identity.
+ * field: (N, *spatial, D) float32 / float64, components last (a
+ * transformation if is_grid, else a displacement); jac: (N, *spatial, D, D)
+ * with jac[..., i, j] = d psi_i / d x_j, and / or det: (N, *spatial); either
+ * may be NULL.  voxel_size: D doubles (NULL: 1). */
+PP_API int pp_grid_jacobian(const pp_tensor* field, const pp_tensor* jac, const pp_tensor* det, int32_t bound,
+                            const double* voxel_size, int32_t is_grid, int32_t add_identity, void* stream);
+
+/* Adjoint of pp_grid_jacobian: grad_field (field's shape, zero-filled by
+ * the call) = gradient of <grad_jac, jac> + <grad_det, det> w.r.t. the field;
+ * grad_jac or grad_det may be NULL. */
+PP_API int pp_grid_jacobian_backward(const pp_tensor* grad_jac, const pp_tensor* grad_det,
+                                     const pp_tensor* field, const pp_tensor* grad_field, int32_t bound,
+                                     const double* voxel_size, int32_t is_grid, int32_t add_identity,
+                                     void* stream);
+
+/* Determinants of (M, D, D) matrices (torch.det in nitorch's grid_jacdet
+ * with `sample`): det (M) forward, or grad_jac = grad_det * cofactor(jac)
+ * backward (det = NULL). */
+PP_API int pp_jacobian_det(const pp_tensor* jac, const pp_tensor* det, const pp_tensor* grad_det,
+                           const pp_tensor* grad_jac, void* stream);
+
 /* Source-sorted processing order of a grid's sampling points (no
  * counterpart in the reference; a scheduling aid for rough deformations):
  * writes to `perm` (int32, N*prod(grid spatial) entries) the sample indices

@@ -12,6 +12,7 @@ Entry points:
   nitorch_b200.resize / reslice / affine_pull / affine_push   affine sampling,
                             coordinates computed in the kernel (no grid)
   nitorch_b200.svf.exp      velocity exponentiation (scaling and squaring)
+  nitorch_b200.grid_jacobian / grid_jacdet   Jacobians of transformation fields
   nitorch_b200.spatial      drop-in for the ``nitorch._C.spatial`` module
   nitorch_b200.coeff        drop-in for ``interpol.coeff``
   nitorch_b200.batch        many uneven volumes in one persistent launch
@@ -20,12 +21,13 @@ Entry points:
 from .api import (affine_grid, affine_pull, affine_push, grid_count, grid_grad, grid_pull, grid_push,
                   identity_grid, pull_push, reslice, resize, spline_coeff, spline_coeff_nd)
 from .enums import BoundType, InterpolationType
+from .jacobian import grid_jacdet, grid_jacobian
 from .spatial import get_deterministic, set_deterministic
 from . import spatial, coeff, grid, svf
 from .integration import install
 
 __all__ = ["grid_pull", "grid_push", "grid_count", "grid_grad", "pull_push", "affine_grid", "affine_pull",
-           "affine_push", "resize", "reslice", "svf", "spline_coeff",
+           "affine_push", "resize", "reslice", "svf", "grid_jacobian", "grid_jacdet", "spline_coeff",
            "spline_coeff_nd", "identity_grid", "BoundType", "InterpolationType",
            "set_deterministic", "get_deterministic", "spatial", "coeff", "grid",
            "install"]

@@ -72,6 +72,7 @@ EXPORTS = (
     "pp_batch_plan_bytes", "pp_batch_scratch_bytes", "pp_batch_plan", "pp_batch_run",
     "pp_svf_compose", "pp_svf_compose_backward", "pp_affine_pull", "pp_affine_push",
     "pp_affine_grad_workspace_bytes", "pp_affine_grad_matrix",
+    "pp_grid_jacobian", "pp_grid_jacobian_backward", "pp_jacobian_det",
 )
 
 PP_BATCH_PULL, PP_BATCH_PUSH, PP_BATCH_PUSH_BACKWARD = 0, 2, 4
@@ -99,6 +100,11 @@ def _declare(L):
     L.pp_grid_grad_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
     L.pp_grid_pull_push.argtypes = [T, T, T, O, vp, vp, sz]
     L.pp_grid_pull_push_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
+    DP = ctypes.POINTER(ctypes.c_double)
+    i32 = ctypes.c_int32
+    L.pp_grid_jacobian.argtypes = [T, T, T, i32, DP, i32, i32, vp]
+    L.pp_grid_jacobian_backward.argtypes = [T, T, T, T, i32, DP, i32, i32, vp]
+    L.pp_jacobian_det.argtypes = [T, T, T, T, vp]
     L.pp_svf_compose.argtypes = [T, T, O, vp]
     L.pp_svf_compose_backward.argtypes = [T, T, T, O, vp]
     L.pp_affine_pull.argtypes = [T, T, T, O, vp]

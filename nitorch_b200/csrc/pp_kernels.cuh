@@ -392,7 +392,6 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
           PP_CB acc[cb] = fma(az.w[k], accy[cb], acc[cb]);
         }
       }
-#pragma unroll
       if (a.flags & F_ADDSELF) {
         // self-composition: add the field's own value at the point
         int64_t so = 0;
