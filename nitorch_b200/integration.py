@@ -54,3 +54,46 @@ def install(set_env=True):
         sys.modules["interpol"] = pkg
         del BoundType
     return spatial
+
+
+# nitorch.spatial callers of the push/pull path that this package also
+# provides as fused CUDA implementations: name -> "module:function"
+_CALLERS = {
+    "exp": "svf:exp",
+    "resize": "api:resize",
+    "reslice": "api:reslice",
+    "grid_jacobian": "jacobian:grid_jacobian",
+    "grid_jacdet": "jacobian:grid_jacdet",
+}
+
+
+def patch_callers(spatial_module):
+    """After ``install()`` and ``import nitorch.spatial as S``, route
+    ``S.exp``, ``S.resize``, ``S.reslice``, ``S.grid_jacobian`` and
+    ``S.grid_jacdet`` to this package's fused versions for CUDA tensors
+    (velocity exponentiation with one kernel per squaring, affine sampling
+    without a materialised grid, Jacobians in one pass).  Tensors on other
+    devices keep nitorch's own functions (which, after ``install()``, still
+    call this backend for their CUDA pulls).  Returns the patched names."""
+    import importlib
+
+    import torch
+
+    patched = []
+    for name, target in _CALLERS.items():
+        original = getattr(spatial_module, name, None)
+        if original is None or getattr(original, "_nitorch_b200", False):
+            continue
+        mod, fn = target.split(":")
+        fast = getattr(importlib.import_module(f"{__package__}.{mod}"), fn)
+
+        def dispatch(x, *args, _fast=fast, _orig=original, **kwargs):
+            if isinstance(x, torch.Tensor) and x.is_cuda:
+                return _fast(x, *args, **kwargs)
+            return _orig(x, *args, **kwargs)
+        dispatch.__name__ = name
+        dispatch.__doc__ = (original.__doc__ or "") + f"\n(CUDA tensors: nitorch_b200.{mod}.{fn})"
+        dispatch._nitorch_b200 = True
+        setattr(spatial_module, name, dispatch)
+        patched.append(name)
+    return patched

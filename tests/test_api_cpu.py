@@ -103,3 +103,22 @@ def test_install_registers_backend_module():
                 sys.modules.pop(k, None)
             else:
                 sys.modules[k] = v
+
+
+def test_patch_callers_dispatches_by_device():
+    """patch_callers replaces nitorch.spatial's callers by dispatchers: CUDA
+    tensors go to this package, other tensors to the original function."""
+    import types
+
+    import torch
+
+    from nitorch_b200 import integration
+    calls = []
+    fake = types.ModuleType("fake_spatial")
+    for name in ("exp", "resize", "reslice", "grid_jacobian", "grid_jacdet"):
+        setattr(fake, name, (lambda n: (lambda x, *a, **k: calls.append(n) or n))(name))
+    patched = integration.patch_callers(fake)
+    assert sorted(patched) == sorted(["exp", "resize", "reslice", "grid_jacobian", "grid_jacdet"])
+    assert fake.exp(torch.zeros(2, 2, 1)) == "exp" and calls == ["exp"]
+    assert fake.grid_jacdet(torch.zeros(1, 2, 2, 2)) == "grid_jacdet"
+    assert integration.patch_callers(fake) == []  # idempotent
