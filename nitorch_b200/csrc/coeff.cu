@@ -143,12 +143,16 @@ __global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int64_t
   __shared__ int64_t bin[LINES], bout[LINES];
   for (int l = threadIdx.x; l < nl; l += blockDim.x) line_base(a, l0 + l, bin[l], bout[l]);
   __syncthreads();
-  const int64_t total = static_cast<int64_t>(nl) * a.n;
-  for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-    int l; int64_t i;
-    if (a.line_major) { l = static_cast<int>(e / a.n); i = e - static_cast<int64_t>(l) * a.n; }
-    else { i = e / nl; l = static_cast<int>(e - i * nl); }
-    sm[l * row + i] = ppk::to_acc(in[bin[l] + i * a.in_st]);
+  // element loops in 32-bit arithmetic (a CTA holds at most LINES lines of
+  // the shared-memory budget): consecutive threads take consecutive
+  // elements along the line (line-major) or across the lines
+  const int n32 = static_cast<int>(a.n);
+  const int total = nl * n32;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    int l, i;
+    if (a.line_major) { l = e / n32; i = e - l * n32; }
+    else { i = e / nl; l = e - i * nl; }
+    sm[l * row + i] = ppk::to_acc(in[bin[l] + static_cast<int64_t>(i) * a.in_st]);
   }
   __syncthreads();
   if (threadIdx.x < nl) {
@@ -156,11 +160,11 @@ __global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int64_t
     filter_line(L, a.n, a);
   }
   __syncthreads();
-  for (int64_t e = threadIdx.x; e < total; e += blockDim.x) {
-    int l; int64_t i;
-    if (a.line_major) { l = static_cast<int>(e / a.n); i = e - static_cast<int64_t>(l) * a.n; }
-    else { i = e / nl; l = static_cast<int>(e - i * nl); }
-    out[bout[l] + i * a.out_st] = ppk::from_acc<S>(sm[l * row + i]);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    int l, i;
+    if (a.line_major) { l = e / n32; i = e - l * n32; }
+    else { i = e / nl; l = e - i * nl; }
+    out[bout[l] + static_cast<int64_t>(i) * a.out_st] = ppk::from_acc<S>(sm[l * row + i]);
   }
 }
 
