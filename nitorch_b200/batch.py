@@ -26,6 +26,7 @@ import ctypes
 import gc
 import json
 import os
+import threading
 import time
 
 import torch
@@ -243,6 +244,8 @@ class Autotuner:
     # (persistent CTAs per SM, 0 = one CTA per work item) x sample order
     CANDIDATES = [(ctas_per_sm, srt) for srt in (True, False) for ctas_per_sm in (0, 4)]
 
+    _lock = threading.Lock()  # one tuning / cache write at a time per process
+
     def __init__(self, path=None):
         self.path = path or os.environ.get("PP_AUTOTUNE_CACHE") or os.path.join(
             os.path.expanduser("~"), ".cache", "nitorch_b200", "autotune.json")
@@ -264,6 +267,10 @@ class Autotuner:
                extrapolate=False, reps=3, init=None, fused=True):
         """Returns (ctas, sorted_order, timings).  `init(batch)` fills the
         input arenas of a candidate batch before it is timed."""
+        with Autotuner._lock:
+            return self._choose(shapes, channels, orders, dtype, device, bound, extrapolate, reps, init, fused)
+
+    def _choose(self, shapes, channels, orders, dtype, device, bound, extrapolate, reps, init, fused):
         device = torch.device(device or "cuda")
         k = self.key(shapes, channels, orders, dtype, device, fused)
         if k in self.cache:
@@ -293,9 +300,12 @@ class Autotuner:
             torch.cuda.empty_cache()
         self.cache[k] = {"ctas": best[1], "sorted": best[2], "ms": timings}
         try:
+            # write-then-rename: a concurrent reader never sees a partial file
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            with open(self.path, "w") as f:
+            tmp = f"{self.path}.{os.getpid()}.tmp"
+            with open(tmp, "w") as f:
                 json.dump(self.cache, f, indent=1)
+            os.replace(tmp, self.path)
         except OSError:
             pass
         return best[1], best[2], timings

@@ -28,6 +28,7 @@ Argument errors raise ``RuntimeError`` with the reference's "(): expected
 """
 import ctypes
 import os
+import threading
 import weakref
 
 import torch
@@ -65,6 +66,7 @@ class _OrderCache:
     def __init__(self, size=4):
         self.size = size
         self.entries = []
+        self.lock = threading.Lock()  # callers may run on several host threads
 
     @staticmethod
     def _key(grid, src):
@@ -73,19 +75,22 @@ class _OrderCache:
 
     def get(self, grid, src):
         key = self._key(grid, src)
-        for i, (ref, k, perm) in enumerate(self.entries):
-            if ref() is not None and k == key:
-                if i:
-                    self.entries.insert(0, self.entries.pop(i))
-                return perm
+        with self.lock:
+            for i, (ref, k, perm) in enumerate(self.entries):
+                if ref() is not None and k == key:
+                    if i:
+                        self.entries.insert(0, self.entries.pop(i))
+                    return perm
         return None
 
     def put(self, grid, src, perm):
-        self.entries = [e for e in self.entries if e[0]() is not None][: self.size - 1]
-        self.entries.insert(0, (weakref.ref(grid), self._key(grid, src), perm))
+        with self.lock:
+            self.entries = [e for e in self.entries if e[0]() is not None][: self.size - 1]
+            self.entries.insert(0, (weakref.ref(grid), self._key(grid, src), perm))
 
     def clear(self):
-        self.entries = []
+        with self.lock:
+            self.entries = []
 
 
 _orders = _OrderCache()
