@@ -14,6 +14,7 @@ Entry points:
   nitorch_b200.svf.exp      velocity exponentiation (scaling and squaring)
   nitorch_b200.grid_jacobian / grid_jacdet   Jacobians of transformation fields
   nitorch_b200.spatial      drop-in for the ``nitorch._C.spatial`` module
+  nitorch_b200.ops          the same as torch.library operators (torch.ops.nitorch_b200.*)
   nitorch_b200.coeff        drop-in for ``interpol.coeff``
   nitorch_b200.batch        many uneven volumes in one persistent launch
   nitorch_b200.install()    route an installed nitorch through this backend
@@ -23,7 +24,7 @@ from .api import (affine_grid, affine_pull, affine_push, grid_count, grid_grad, 
 from .enums import BoundType, InterpolationType
 from .jacobian import grid_jacdet, grid_jacobian
 from .spatial import get_deterministic, set_deterministic
-from . import spatial, coeff, grid, svf
+from . import spatial, coeff, grid, svf, ops
 from .integration import install
 
 __all__ = ["grid_pull", "grid_push", "grid_count", "grid_grad", "pull_push", "affine_grid", "affine_pull",

@@ -122,3 +122,24 @@ def test_patch_callers_dispatches_by_device():
     assert fake.exp(torch.zeros(2, 2, 1)) == "exp" and calls == ["exp"]
     assert fake.grid_jacdet(torch.zeros(1, 2, 2, 2)) == "grid_jacdet"
     assert integration.patch_callers(fake) == []  # idempotent
+
+
+def test_torch_library_ops_fake_shapes():
+    """The custom operators are registered and propagate shapes on fake
+    tensors (what torch.compile traces with), no GPU needed."""
+    import torch
+    from torch._subclasses.fake_tensor import FakeTensorMode
+
+    import nitorch_b200.ops  # noqa: F401  (registers the operators)
+    with FakeTensorMode():
+        x = torch.empty(2, 3, 8, 9, 10)
+        g = torch.empty(2, 5, 6, 7, 3)
+        y = torch.ops.nitorch_b200.grid_pull(x, g, [2], [3], 0)
+        assert y.shape == (2, 3, 5, 6, 7)
+        assert torch.ops.nitorch_b200.grid_push(y, g, [8, 9, 10], [2], [3], 0).shape == x.shape
+        assert torch.ops.nitorch_b200.grid_push(y, g, [], [2], [3], 0).shape == y.shape
+        assert torch.ops.nitorch_b200.grid_count(g, [], [2], [1], 0).shape == (2, 1, 5, 6, 7)
+        assert torch.ops.nitorch_b200.grid_grad(x, g, [2], [1], 0).shape == (2, 3, 5, 6, 7, 3)
+        gi, gg = torch.ops.nitorch_b200.grid_pull_backward(y, x, g, [2], [3], 0, True, True)
+        assert gi.shape == x.shape and gg.shape == g.shape
+        assert torch.ops.nitorch_b200.spline_coeff_nd(x, [3], [3], 3).shape == x.shape
