@@ -16,8 +16,9 @@
 
 namespace {
 
-constexpr int LINES = 32;
+constexpr int LINES = 128;    // lines per CTA: one per thread in the recursions
 constexpr int THREADS = 128;
+constexpr int UNROLL = 4;     // global loads in flight per thread while staging
 
 struct LineArgs {
   const void* in;
@@ -115,9 +116,10 @@ __device__ double final_value(const LineRef<C>& L, int64_t n, int kind, double z
 }
 
 template <class C>
-__device__ void filter_line(const LineRef<C>& L, int64_t n, const LineArgs& a) {
+__device__ void filter_line(const LineRef<C>& L, int64_t n, const LineArgs& a, bool apply_gain = true) {
   const C gain = static_cast<C>(a.gain);
-  for (int64_t i = 0; i < n; ++i) L[i] *= gain;
+  if (apply_gain)
+    for (int64_t i = 0; i < n; ++i) L[i] *= gain;
   for (int q = 0; q < a.npoles; ++q) {
     const double zd = a.z[q];
     const C z = static_cast<C>(zd);
@@ -130,7 +132,11 @@ __device__ void filter_line(const LineRef<C>& L, int64_t n, const LineArgs& a) {
   }
 }
 
-// Shared-memory line kernel: LINES lines per CTA.
+// Shared-memory line kernel: up to LINES lines per CTA, one per thread in
+// the recursions.  Staging: each warp copies whole lines (line-major: the
+// filtered axis is the fastest) or one element of 32 adjacent lines (the
+// lines are adjacent in memory) per step, UNROLL loads in flight per thread,
+// the gain folded into the staging multiply.
 template <class S>
 __global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int64_t row, int lines) {
   using C = typename ppk::Acc<S>::type;
@@ -143,28 +149,39 @@ __global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int64_t
   __shared__ int64_t bin[LINES], bout[LINES];
   for (int l = threadIdx.x; l < nl; l += blockDim.x) line_base(a, l0 + l, bin[l], bout[l]);
   __syncthreads();
-  // element loops in 32-bit arithmetic (a CTA holds at most LINES lines of
-  // the shared-memory budget): consecutive threads take consecutive
-  // elements along the line (line-major) or across the lines
   const int n32 = static_cast<int>(a.n);
-  const int total = nl * n32;
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    int l, i;
-    if (a.line_major) { l = e / n32; i = e - l * n32; }
-    else { i = e / nl; l = e - i * nl; }
-    sm[l * row + i] = ppk::to_acc(in[bin[l] + static_cast<int64_t>(i) * a.in_st]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const C gain = static_cast<C>(a.gain);
+  // (outer, inner) walks: inner = 32 lanes, UNROLL steps per batch
+  const int outer_n = a.line_major ? nl : n32, inner_n = a.line_major ? n32 : nl;
+  for (int o = warp; o < outer_n; o += nwarps) {
+    for (int j0 = 0; j0 < inner_n; j0 += 32 * UNROLL) {
+      C v[UNROLL];
+#pragma unroll
+      for (int u = 0; u < UNROLL; ++u) {
+        const int j = j0 + u * 32 + lane;
+        const int l = a.line_major ? o : j, i = a.line_major ? j : o;
+        v[u] = j < inner_n ? ppk::to_acc(in[bin[l] + static_cast<int64_t>(i) * a.in_st]) : C(0);
+      }
+#pragma unroll
+      for (int u = 0; u < UNROLL; ++u) {
+        const int j = j0 + u * 32 + lane;
+        const int l = a.line_major ? o : j, i = a.line_major ? j : o;
+        if (j < inner_n) sm[l * row + i] = v[u] * gain;
+      }
+    }
   }
   __syncthreads();
   if (threadIdx.x < nl) {
     LineRef<C> L{sm + threadIdx.x * row, 1};
-    filter_line(L, a.n, a);
+    filter_line(L, a.n, a, false);
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < total; e += blockDim.x) {
-    int l, i;
-    if (a.line_major) { l = e / n32; i = e - l * n32; }
-    else { i = e / nl; l = e - i * nl; }
-    out[bout[l] + static_cast<int64_t>(i) * a.out_st] = ppk::from_acc<S>(sm[l * row + i]);
+  for (int o = warp; o < outer_n; o += nwarps) {
+    for (int j = lane; j < inner_n; j += 32) {
+      const int l = a.line_major ? o : j, i = a.line_major ? j : o;
+      out[bout[l] + static_cast<int64_t>(i) * a.out_st] = ppk::from_acc<S>(sm[l * row + i]);
+    }
   }
 }
 
@@ -244,8 +261,13 @@ int run_axis(LineArgs& a, cudaStream_t st) {
   using C = typename ppk::Acc<S>::type;
   if (a.nlines == 0) return PP_OK;
   const int64_t row = a.n | 1;  // odd row pitch: conflict-free per-thread walks
-  const size_t budget = 200 * 1024;
+  // two CTAs per SM where the lines allow; one long line per CTA otherwise
+  size_t budget = 110 * 1024;
   int lines = static_cast<int>(budget / (row * sizeof(C)));
+  if (lines < 1) {
+    budget = 200 * 1024;
+    lines = static_cast<int>(budget / (row * sizeof(C)));
+  }
   if (lines > LINES) lines = LINES;
   if (lines >= 1) {
     const size_t smem = static_cast<size_t>(lines) * row * sizeof(C);
