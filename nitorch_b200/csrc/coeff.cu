@@ -18,7 +18,7 @@ namespace {
 
 constexpr int LINES = 128;    // lines per CTA: one per thread in the recursions
 constexpr int THREADS = 128;
-constexpr int UNROLL = 4;     // global loads in flight per thread while staging
+constexpr int UNROLL = 8;     // 16-bit storage: loads in flight per thread while staging
 
 struct LineArgs {
   const void* in;
@@ -52,60 +52,75 @@ __device__ __forceinline__ int64_t trunc_iter(double z) {
   return static_cast<int64_t>(ceil(-30.0 / log(fabs(z))));
 }
 
-// Accessor over a line held in shared or global memory.
+// Accessors over one line: in global memory (any stride) or in the shared
+// tile (element-major, one column per line, pitch = lines per CTA | 1).
 template <class C>
 struct LineRef {
+  using value_type = C;
+  using index_type = int64_t;
   C* p;
   int64_t st;
   __device__ __forceinline__ C& operator[](int64_t i) const { return p[i * st]; }
 };
 
-// Initial causal coefficient (coeff.py:69-170), double accumulation.
 template <class C>
-__device__ double initial(const LineRef<C>& L, int64_t n, int kind, double z) {
+struct TileLine {
+  using value_type = C;
+  using index_type = int;
+  C* p;
+  int pitch;
+  __device__ __forceinline__ C& operator[](int i) const { return p[i * pitch]; }
+};
+
+// Initial causal coefficient (coeff.py:69-170), double accumulation.  The
+// samples are read as L[k] * g (g: the filter gain on the first pole's pass,
+// 1 afterwards), so the gain pass costs no separate sweep.
+template <class R, class C = typename R::value_type>
+__device__ double initial(const R& L, int64_t n, int kind, double z, C g) {
+  auto x = [&](int64_t k) { return static_cast<double>(L[k] * g); };
   if (kind == 2) {  // dct2 / replicate (coeff.py:137-170)
     const double zn = pow(z, static_cast<double>(n));
     const double zlast = zn * (1.0 + 1.0 / (z + zn * zn));
-    double acc = static_cast<double>(L[0]) + zlast * static_cast<double>(L[n - 1]);
+    double acc = x(0) + zlast * x(n - 1);
     // sum_{k=1}^{n-2} (z^k + z^(2n-1-k)) L[k]; both power series decay
     // geometrically, terms below 2^-64 of the leading one are dropped.
     const int64_t K = static_cast<int64_t>(ceil(-44.4 / log(fabs(z)))) + 1;
     const int64_t k1 = n - 2 < K ? n - 2 : K;
     double zk = z;
-    for (int64_t k = 1; k <= k1; ++k, zk *= z) acc += zk * static_cast<double>(L[k]);
+    for (int64_t k = 1; k <= k1; ++k, zk *= z) acc += zk * x(k);
     int64_t k2 = 2 * n - 1 - K;
     if (k2 < 1) k2 = 1;
     if (k2 <= n - 2) {
       double zq = pow(z, static_cast<double>(2 * n - 1 - k2));
       const double iz = 1.0 / z;
-      for (int64_t k = k2; k <= n - 2; ++k, zq *= iz) acc += zq * static_cast<double>(L[k]);
+      for (int64_t k = k2; k <= n - 2; ++k, zq *= iz) acc += zq * x(k);
     }
-    return acc * (z / (1.0 - zn * zn)) + static_cast<double>(L[0]);
+    return acc * (z / (1.0 - zn * zn)) + x(0);
   }
   if (kind == 1) {  // dct1 / zero (coeff.py:94-134)
     const int64_t m = trunc_iter(z);
     if (m < n) {
-      double acc = static_cast<double>(L[0]), zk = z;
-      for (int64_t k = 1; k < m; ++k, zk *= z) acc += zk * static_cast<double>(L[k]);
+      double acc = x(0), zk = z;
+      for (int64_t k = 1; k < m; ++k, zk *= z) acc += zk * x(k);
       return acc;
     }
     const double zn = pow(z, static_cast<double>(n - 1));
-    double acc = static_cast<double>(L[0]) + zn * static_cast<double>(L[n - 1]);
+    double acc = x(0) + zn * x(n - 1);
     double zk = z;
-    for (int64_t k = 1; k < n - 1; ++k, zk *= z) acc += (zk + zn * zn / zk) * static_cast<double>(L[k]);
+    for (int64_t k = 1; k < n - 1; ++k, zk *= z) acc += (zk + zn * zn / zk) * x(k);
     return acc / (1.0 - zn * zn);
   }
   // dft (coeff.py:69-91)
   int64_t m = trunc_iter(z);
   if (m > n) m = n;
-  double acc = static_cast<double>(L[0]), zj = z;
-  for (int64_t j = 1; j < m; ++j, zj *= z) acc += zj * static_cast<double>(L[n - j]);
+  double acc = x(0), zj = z;
+  for (int64_t j = 1; j < m; ++j, zj *= z) acc += zj * x(n - j);
   return acc / (1.0 - pow(z, static_cast<double>(m)));
 }
 
 // Final anti-causal coefficient (coeff.py:173-215).
-template <class C>
-__device__ double final_value(const LineRef<C>& L, int64_t n, int kind, double z) {
+template <class R>
+__device__ double final_value(const R& L, int64_t n, int kind, double z) {
   if (kind == 2) return static_cast<double>(L[n - 1]) * (z / (z - 1.0));
   if (kind == 1) return (z * static_cast<double>(L[n - 2]) + static_cast<double>(L[n - 1])) * (z / (z * z - 1.0));
   int64_t m = trunc_iter(z);
@@ -115,30 +130,46 @@ __device__ double final_value(const LineRef<C>& L, int64_t n, int kind, double z
   return acc / (pow(z, static_cast<double>(m)) - 1.0);
 }
 
-template <class C>
-__device__ void filter_line(const LineRef<C>& L, int64_t n, const LineArgs& a, bool apply_gain = true) {
-  const C gain = static_cast<C>(a.gain);
-  if (apply_gain)
-    for (int64_t i = 0; i < n; ++i) L[i] *= gain;
+// Gain (coeff.py:61-65) folded into the first causal pass, then one causal
+// and one anti-causal recursion per pole (coeff.py:254-281).
+template <class R>
+__device__ void filter_line(const R& L, typename R::index_type n, const LineArgs& a) {
+  using C = typename R::value_type;
+  using I = typename R::index_type;
+  C g = static_cast<C>(a.gain);
   for (int q = 0; q < a.npoles; ++q) {
     const double zd = a.z[q];
     const C z = static_cast<C>(zd);
-    C prev = static_cast<C>(initial(L, n, a.kind, zd));
+    C prev = static_cast<C>(initial(L, n, a.kind, zd, g));
     L[0] = prev;
-    for (int64_t i = 1; i < n; ++i) { prev = fma(z, prev, L[i]); L[i] = prev; }
+    for (I i = 1; i < n; ++i) { prev = fma(z, prev, L[i] * g); L[i] = prev; }
     prev = static_cast<C>(final_value(L, n, a.kind, zd));
     L[n - 1] = prev;
-    for (int64_t i = n - 2; i >= 0; --i) { prev = z * (prev - L[i]); L[i] = prev; }
+    for (I i = n - 2; i >= 0; --i) { prev = z * (prev - L[i]); L[i] = prev; }
+    g = C(1);
   }
 }
 
+// Asynchronous 4- / 8-byte global -> shared copy (no register round trip).
+template <int B>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (B == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+
 // Shared-memory line kernel: up to LINES lines per CTA, one per thread in
-// the recursions.  Staging: each warp copies whole lines (line-major: the
-// filtered axis is the fastest) or one element of 32 adjacent lines (the
-// lines are adjacent in memory) per step, UNROLL loads in flight per thread,
-// the gain folded into the staging multiply.
+// the recursions, held element-major in shared memory (tile[i * pitch + l],
+// odd pitch: conflict-free both for the per-thread walks along a line and
+// for warps that stage whole lines).  Staging walks the tile so that a warp
+// touches 32 consecutive addresses of global memory: 32 elements of one line
+// when the filtered axis is the fastest, else element i of 32 adjacent
+// lines.  float / double storage stage with asynchronous copies -- every
+// element of the tile is in flight at once, which is what it takes to keep
+// HBM busy with two CTAs per SM; 16-bit storage converts through registers,
+// UNROLL loads in flight per thread.
 template <class S>
-__global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int64_t row, int lines) {
+__global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int pitch, int lines) {
   using C = typename ppk::Acc<S>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
@@ -151,36 +182,40 @@ __global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int64_t
   __syncthreads();
   const int n32 = static_cast<int>(a.n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const C gain = static_cast<C>(a.gain);
-  // (outer, inner) walks: inner = 32 lanes, UNROLL steps per batch
   const int outer_n = a.line_major ? nl : n32, inner_n = a.line_major ? n32 : nl;
-  for (int o = warp; o < outer_n; o += nwarps) {
-    for (int j0 = 0; j0 < inner_n; j0 += 32 * UNROLL) {
-      C v[UNROLL];
-#pragma unroll
-      for (int u = 0; u < UNROLL; ++u) {
-        const int j = j0 + u * 32 + lane;
+  if constexpr (sizeof(S) == sizeof(C)) {
+    for (int o = warp; o < outer_n; o += nwarps)
+      for (int j = lane; j < inner_n; j += 32) {
         const int l = a.line_major ? o : j, i = a.line_major ? j : o;
-        v[u] = j < inner_n ? ppk::to_acc(in[bin[l] + static_cast<int64_t>(i) * a.in_st]) : C(0);
+        cp_async<sizeof(C)>(sm + i * pitch + l, in + bin[l] + static_cast<int64_t>(i) * a.in_st);
       }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+  } else {
+    for (int o = warp; o < outer_n; o += nwarps) {
+      for (int j0 = 0; j0 < inner_n; j0 += 32 * UNROLL) {
+        C v[UNROLL];
 #pragma unroll
-      for (int u = 0; u < UNROLL; ++u) {
-        const int j = j0 + u * 32 + lane;
-        const int l = a.line_major ? o : j, i = a.line_major ? j : o;
-        if (j < inner_n) sm[l * row + i] = v[u] * gain;
+        for (int u = 0; u < UNROLL; ++u) {
+          const int j = j0 + u * 32 + lane;
+          const int l = a.line_major ? o : j, i = a.line_major ? j : o;
+          v[u] = j < inner_n ? ppk::to_acc(in[bin[l] + static_cast<int64_t>(i) * a.in_st]) : C(0);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          const int j = j0 + u * 32 + lane;
+          const int l = a.line_major ? o : j, i = a.line_major ? j : o;
+          if (j < inner_n) sm[i * pitch + l] = v[u];
+        }
       }
     }
   }
   __syncthreads();
-  if (threadIdx.x < nl) {
-    LineRef<C> L{sm + threadIdx.x * row, 1};
-    filter_line(L, a.n, a, false);
-  }
+  if (threadIdx.x < nl) filter_line(TileLine<C>{sm + threadIdx.x, pitch}, n32, a);
   __syncthreads();
   for (int o = warp; o < outer_n; o += nwarps) {
     for (int j = lane; j < inner_n; j += 32) {
       const int l = a.line_major ? o : j, i = a.line_major ? j : o;
-      out[bout[l] + static_cast<int64_t>(i) * a.out_st] = ppk::from_acc<S>(sm[l * row + i]);
+      out[bout[l] + static_cast<int64_t>(i) * a.out_st] = ppk::from_acc<S>(sm[i * pitch + l]);
     }
   }
 }
@@ -260,24 +295,24 @@ template <class S>
 int run_axis(LineArgs& a, cudaStream_t st) {
   using C = typename ppk::Acc<S>::type;
   if (a.nlines == 0) return PP_OK;
-  const int64_t row = a.n | 1;  // odd row pitch: conflict-free per-thread walks
-  // two CTAs per SM where the lines allow; one long line per CTA otherwise
+  // two CTAs per SM where the lines allow; fewer, longer lines otherwise
   size_t budget = 110 * 1024;
-  int lines = static_cast<int>(budget / (row * sizeof(C)));
-  if (lines < 1) {
-    budget = 200 * 1024;
-    lines = static_cast<int>(budget / (row * sizeof(C)));
+  int lines = 0, pitch = 0;
+  for (int pass = 0; pass < 2 && lines < 1; ++pass, budget = 200 * 1024) {
+    const int64_t fit = static_cast<int64_t>(budget / (static_cast<size_t>(a.n) * sizeof(C)));
+    lines = static_cast<int>(fit < LINES ? fit : LINES);
+    pitch = lines | 1;
+    if (static_cast<int64_t>(pitch) > fit) pitch = --lines;  // lines was even: drop one
   }
-  if (lines > LINES) lines = LINES;
   if (lines >= 1) {
-    const size_t smem = static_cast<size_t>(lines) * row * sizeof(C);
+    const size_t smem = static_cast<size_t>(a.n) * pitch * sizeof(C);
     auto k = coeff_smem_kernel<S>;
     if (smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e != cudaSuccess) return ppc::cuda_check(e, "prefilter smem attribute");
     }
     const int64_t blocks = (a.nlines + lines - 1) / lines;
-    k<<<static_cast<unsigned>(blocks), THREADS, smem, st>>>(a, row, lines);
+    k<<<static_cast<unsigned>(blocks), THREADS, smem, st>>>(a, pitch, lines);
     ppc::count_launch();
   } else {
     if constexpr (sizeof(S) < 4) {
