@@ -12,12 +12,15 @@
 // run in float (double for double storage); the initial / final condition
 // sums are evaluated in double.  Lines longer than the shared-memory budget
 // fall back to the same recursion directly on global memory.
+#include <algorithm>
+#include <cmath>
+
 #include "pp_capi_internal.cuh"
 
 namespace {
 
 constexpr int LINES = 128;    // lines per CTA: one per thread in the recursions
-constexpr int THREADS = 128;
+constexpr int THREADS = 256;  // all stage and store; the first LINES recurse
 constexpr int UNROLL = 8;     // 16-bit storage: loads in flight per thread while staging
 
 struct LineArgs {
@@ -34,7 +37,11 @@ struct LineArgs {
   int npoles;
   double z[3];
   double gain;
-  int line_major;     // 1: load element-major within a line (axis is the fastest)
+  // per-pole boundary constants, the same for every line (host-computed):
+  int64_t hz[3];      // dct2: series length K; dct1: truncation m; dft: min(m, n)
+  double zp[3];       // dct2: z^n; dct1: z^(n-1); dft: z^hz
+  double zq[3];       // dct2: z^(2n-1-k2), k2 = max(1, 2n-1-K): the mirrored tail's first weight
+  int line_major;     // 1: the filtered axis is the fastest (warps stage whole lines)
 };
 
 __device__ __forceinline__ void line_base(const LineArgs& a, int64_t l, int64_t& bi, int64_t& bo) {
@@ -46,10 +53,6 @@ __device__ __forceinline__ void line_base(const LineArgs& a, int64_t l, int64_t&
     bo += r * a.ost[d];
     l = q;
   }
-}
-
-__device__ __forceinline__ int64_t trunc_iter(double z) {
-  return static_cast<int64_t>(ceil(-30.0 / log(fabs(z))));
 }
 
 // Accessors over one line: in global memory (any stride) or in the shared
@@ -76,62 +79,68 @@ struct TileLine {
 // samples are read as L[k] * g (g: the filter gain on the first pole's pass,
 // 1 afterwards), so the gain pass costs no separate sweep.
 template <class R, class C = typename R::value_type>
-__device__ double initial(const R& L, int64_t n, int kind, double z, C g) {
+__device__ double initial(const R& L, int64_t n, const LineArgs& a, int q, C g) {
+  const double z = a.z[q];
   auto x = [&](int64_t k) { return static_cast<double>(L[k] * g); };
-  if (kind == 2) {  // dct2 / replicate (coeff.py:137-170)
-    const double zn = pow(z, static_cast<double>(n));
+  if (a.kind == 2) {  // dct2 / replicate (coeff.py:137-170)
+    const double zn = a.zp[q];
     const double zlast = zn * (1.0 + 1.0 / (z + zn * zn));
     double acc = x(0) + zlast * x(n - 1);
     // sum_{k=1}^{n-2} (z^k + z^(2n-1-k)) L[k]; both power series decay
     // geometrically, terms below 2^-64 of the leading one are dropped.
-    const int64_t K = static_cast<int64_t>(ceil(-44.4 / log(fabs(z)))) + 1;
+    const int64_t K = a.hz[q];
     const int64_t k1 = n - 2 < K ? n - 2 : K;
     double zk = z;
     for (int64_t k = 1; k <= k1; ++k, zk *= z) acc += zk * x(k);
     int64_t k2 = 2 * n - 1 - K;
     if (k2 < 1) k2 = 1;
     if (k2 <= n - 2) {
-      double zq = pow(z, static_cast<double>(2 * n - 1 - k2));
+      double zq = a.zq[q];
       const double iz = 1.0 / z;
       for (int64_t k = k2; k <= n - 2; ++k, zq *= iz) acc += zq * x(k);
     }
     return acc * (z / (1.0 - zn * zn)) + x(0);
   }
-  if (kind == 1) {  // dct1 / zero (coeff.py:94-134)
-    const int64_t m = trunc_iter(z);
+  if (a.kind == 1) {  // dct1 / zero (coeff.py:94-134)
+    const int64_t m = a.hz[q];
     if (m < n) {
       double acc = x(0), zk = z;
       for (int64_t k = 1; k < m; ++k, zk *= z) acc += zk * x(k);
       return acc;
     }
-    const double zn = pow(z, static_cast<double>(n - 1));
+    const double zn = a.zp[q];
     double acc = x(0) + zn * x(n - 1);
     double zk = z;
     for (int64_t k = 1; k < n - 1; ++k, zk *= z) acc += (zk + zn * zn / zk) * x(k);
     return acc / (1.0 - zn * zn);
   }
   // dft (coeff.py:69-91)
-  int64_t m = trunc_iter(z);
-  if (m > n) m = n;
+  const int64_t m = a.hz[q];
   double acc = x(0), zj = z;
   for (int64_t j = 1; j < m; ++j, zj *= z) acc += zj * x(n - j);
-  return acc / (1.0 - pow(z, static_cast<double>(m)));
+  return acc / (1.0 - a.zp[q]);
 }
 
 // Final anti-causal coefficient (coeff.py:173-215).
 template <class R>
-__device__ double final_value(const R& L, int64_t n, int kind, double z) {
-  if (kind == 2) return static_cast<double>(L[n - 1]) * (z / (z - 1.0));
-  if (kind == 1) return (z * static_cast<double>(L[n - 2]) + static_cast<double>(L[n - 1])) * (z / (z * z - 1.0));
-  int64_t m = trunc_iter(z);
-  if (m > n) m = n;
+__device__ double final_value(const R& L, int64_t n, const LineArgs& a, int q) {
+  const double z = a.z[q];
+  if (a.kind == 2) return static_cast<double>(L[n - 1]) * (z / (z - 1.0));
+  if (a.kind == 1) return (z * static_cast<double>(L[n - 2]) + static_cast<double>(L[n - 1])) * (z / (z * z - 1.0));
+  const int64_t m = a.hz[q];
   double acc = z * static_cast<double>(L[n - 1]), zj = z * z;
   for (int64_t j = 0; j < m - 1; ++j, zj *= z) acc += zj * static_cast<double>(L[j]);
-  return acc / (pow(z, static_cast<double>(m)) - 1.0);
+  return acc / (a.zp[q] - 1.0);
 }
 
 // Gain (coeff.py:61-65) folded into the first causal pass, then one causal
-// and one anti-causal recursion per pole (coeff.py:254-281).
+// and one anti-causal recursion per pole (coeff.py:254-281).  The walks go
+// in chunks of RU samples held in registers, the next chunk loaded before the
+// current one is filtered, so that the memory latency leaves the dependency
+// chain (one FMA per sample); the accessor's stride is a runtime value, which
+// keeps the compiler from reordering the loads past the stores by itself.
+constexpr int RU = 8;
+
 template <class R>
 __device__ void filter_line(const R& L, typename R::index_type n, const LineArgs& a) {
   using C = typename R::value_type;
@@ -140,37 +149,95 @@ __device__ void filter_line(const R& L, typename R::index_type n, const LineArgs
   for (int q = 0; q < a.npoles; ++q) {
     const double zd = a.z[q];
     const C z = static_cast<C>(zd);
-    C prev = static_cast<C>(initial(L, n, a.kind, zd, g));
+    C prev = static_cast<C>(initial(L, n, a, q, g));
     L[0] = prev;
-    for (I i = 1; i < n; ++i) { prev = fma(z, prev, L[i] * g); L[i] = prev; }
-    prev = static_cast<C>(final_value(L, n, a.kind, zd));
+    I i = 1;  // causal: i = 1 .. n-1
+    if (n - 1 >= RU) {
+      C x[RU];
+#pragma unroll
+      for (int u = 0; u < RU; ++u) x[u] = L[i + u];
+      for (;;) {
+        const bool more = i + 2 * RU <= n;
+        C y[RU];
+        if (more) {
+#pragma unroll
+          for (int u = 0; u < RU; ++u) y[u] = L[i + RU + u];
+        }
+#pragma unroll
+        for (int u = 0; u < RU; ++u) { prev = fma(z, prev, x[u] * g); L[i + u] = prev; }
+        i += RU;
+        if (!more) break;
+#pragma unroll
+        for (int u = 0; u < RU; ++u) x[u] = y[u];
+      }
+    }
+    for (; i < n; ++i) { prev = fma(z, prev, L[i] * g); L[i] = prev; }
+    prev = static_cast<C>(final_value(L, n, a, q));
     L[n - 1] = prev;
-    for (I i = n - 2; i >= 0; --i) { prev = z * (prev - L[i]); L[i] = prev; }
+    i = n - 2;  // anti-causal: i = n-2 .. 0
+    if (i + 1 >= RU) {
+      C x[RU];
+#pragma unroll
+      for (int u = 0; u < RU; ++u) x[u] = L[i - u];
+      for (;;) {
+        const bool more = i + 1 >= 2 * RU;
+        C y[RU];
+        if (more) {
+#pragma unroll
+          for (int u = 0; u < RU; ++u) y[u] = L[i - RU - u];
+        }
+#pragma unroll
+        for (int u = 0; u < RU; ++u) { prev = z * (prev - x[u]); L[i - u] = prev; }
+        i -= RU;
+        if (!more) break;
+#pragma unroll
+        for (int u = 0; u < RU; ++u) x[u] = y[u];
+      }
+    }
+    for (; i >= 0; --i) { prev = z * (prev - L[i]); L[i] = prev; }
     g = C(1);
   }
 }
 
-// Asynchronous 4- / 8-byte global -> shared copy (no register round trip).
+// Asynchronous global -> shared copies (no register round trip).
 template <int B>
 __device__ __forceinline__ void cp_async(void* dst, const void* src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   if constexpr (B == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+  else if constexpr (B == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+  else asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+
+// G adjacent samples of 16-bit storage <-> G floats (one 8-byte access).
+template <class S, class C>
+__device__ __forceinline__ void load_group(C* dst, const S* src) {
+  static_assert(sizeof(S) == 2 && sizeof(C) == 4, "16-bit storage, float arithmetic");
+  const uint2 r = *reinterpret_cast<const uint2*>(src);
+  const S* v = reinterpret_cast<const S*>(&r);
+  *reinterpret_cast<float4*>(dst) = make_float4(ppk::to_acc(v[0]), ppk::to_acc(v[1]), ppk::to_acc(v[2]),
+                                                ppk::to_acc(v[3]));
 }
 
 // Shared-memory line kernel: up to LINES lines per CTA, one per thread in
-// the recursions, held element-major in shared memory (tile[i * pitch + l],
-// odd pitch: conflict-free both for the per-thread walks along a line and
-// for warps that stage whole lines).  Staging walks the tile so that a warp
-// touches 32 consecutive addresses of global memory: 32 elements of one line
-// when the filtered axis is the fastest, else element i of 32 adjacent
-// lines.  float / double storage stage with asynchronous copies -- every
-// element of the tile is in flight at once, which is what it takes to keep
-// HBM busy with two CTAs per SM; 16-bit storage converts through registers,
-// UNROLL loads in flight per thread.
+// the recursions, held element-major in shared memory (tile[i * pitch + l]).
+// Staging walks the tile so that a warp touches consecutive addresses of
+// global memory:
+//  * filtered axis the fastest (line_major): a warp per line, lanes over
+//    consecutive samples; odd pitch, so the lanes' column writes are
+//    conflict-free;
+//  * otherwise a warp per sample row, each lane a group of G = 16 / sizeof(C)
+//    adjacent lines moved as one 16-byte copy (8-byte load for 16-bit
+//    storage) when the G lines are adjacent and aligned in memory, else G
+//    scalar copies; pitch a multiple of G.
+// float / double storage stage with asynchronous copies, so that the whole
+// tile is in flight at once (what it takes to keep HBM busy at two CTAs per
+// SM); 16-bit storage converts through registers.  Per-lane pointers are
+// formed once per line / group: the sample loops are an add and a copy.
 template <class S>
-__global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int pitch, int lines) {
+__global__ void __launch_bounds__(THREADS, 2) coeff_smem_kernel(LineArgs a, int pitch, int lines) {
   using C = typename ppk::Acc<S>::type;
+  constexpr int G = 16 / static_cast<int>(sizeof(C));
+  constexpr bool kAsync = sizeof(S) == sizeof(C);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
   const int64_t l0 = static_cast<int64_t>(blockIdx.x) * lines;
@@ -182,40 +249,96 @@ __global__ void __launch_bounds__(THREADS) coeff_smem_kernel(LineArgs a, int pit
   __syncthreads();
   const int n32 = static_cast<int>(a.n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int outer_n = a.line_major ? nl : n32, inner_n = a.line_major ? n32 : nl;
-  if constexpr (sizeof(S) == sizeof(C)) {
-    for (int o = warp; o < outer_n; o += nwarps)
-      for (int j = lane; j < inner_n; j += 32) {
-        const int l = a.line_major ? o : j, i = a.line_major ? j : o;
-        cp_async<sizeof(C)>(sm + i * pitch + l, in + bin[l] + static_cast<int64_t>(i) * a.in_st);
-      }
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-  } else {
-    for (int o = warp; o < outer_n; o += nwarps) {
-      for (int j0 = 0; j0 < inner_n; j0 += 32 * UNROLL) {
-        C v[UNROLL];
+  const int ngroups = (nl + G - 1) / G;
+  // vector eligibility of group g: G lines present, adjacent, aligned rows
+  auto group_vec = [&](const int64_t* base, const void* ptr, int64_t st, int g, int bytes) {
+    const int l = g * G;
+    if (l + G > nl || (pitch % G) != 0) return false;
+    for (int k = 1; k < G; ++k)
+      if (base[l + k] != base[l] + k) return false;
+    const uintptr_t p = reinterpret_cast<uintptr_t>(ptr) + static_cast<uintptr_t>(base[l]) * sizeof(S);
+    return (p % bytes) == 0 && ((st * static_cast<int64_t>(sizeof(S))) % bytes) == 0;
+  };
+  if (a.line_major) {
+    for (int l = warp; l < nl; l += nwarps) {
+      const S* src = in + bin[l];
+      C* dst = sm + l;
+      if constexpr (kAsync) {
+        for (int i = lane; i < n32; i += 32) cp_async<sizeof(C)>(dst + i * pitch, src + i * a.in_st);
+      } else {
+        for (int i0 = 0; i0 < n32; i0 += 32 * UNROLL) {
+          C v[UNROLL];
 #pragma unroll
-        for (int u = 0; u < UNROLL; ++u) {
-          const int j = j0 + u * 32 + lane;
-          const int l = a.line_major ? o : j, i = a.line_major ? j : o;
-          v[u] = j < inner_n ? ppk::to_acc(in[bin[l] + static_cast<int64_t>(i) * a.in_st]) : C(0);
+          for (int u = 0; u < UNROLL; ++u) {
+            const int i = i0 + u * 32 + lane;
+            v[u] = i < n32 ? ppk::to_acc(src[i * a.in_st]) : C(0);
+          }
+#pragma unroll
+          for (int u = 0; u < UNROLL; ++u) {
+            const int i = i0 + u * 32 + lane;
+            if (i < n32) dst[i * pitch] = v[u];
+          }
         }
-#pragma unroll
-        for (int u = 0; u < UNROLL; ++u) {
-          const int j = j0 + u * 32 + lane;
-          const int l = a.line_major ? o : j, i = a.line_major ? j : o;
-          if (j < inner_n) sm[i * pitch + l] = v[u];
+      }
+    }
+  } else {
+    for (int g = lane; g < ngroups; g += 32) {
+      const int l = g * G;
+      const bool vec = group_vec(bin, in, a.in_st, g, G * static_cast<int>(sizeof(S)));
+      const S* src = in + bin[l];
+      if constexpr (kAsync) {
+        for (int i = warp; i < n32; i += nwarps) {
+          C* dst = sm + i * pitch + l;
+          const int64_t off = i * a.in_st;
+          if (vec) {
+            cp_async<16>(dst, src + off);
+          } else {
+            for (int k = 0; k < G && l + k < nl; ++k) cp_async<sizeof(C)>(dst + k, in + bin[l + k] + off);
+          }
+        }
+      } else {
+        for (int i = warp; i < n32; i += nwarps) {
+          C* dst = sm + i * pitch + l;
+          const int64_t off = i * a.in_st;
+          if (vec) {
+            load_group(dst, src + off);
+          } else {
+            for (int k = 0; k < G && l + k < nl; ++k) dst[k] = ppk::to_acc(in[bin[l + k] + off]);
+          }
         }
       }
     }
   }
+  if constexpr (kAsync) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   if (threadIdx.x < nl) filter_line(TileLine<C>{sm + threadIdx.x, pitch}, n32, a);
   __syncthreads();
-  for (int o = warp; o < outer_n; o += nwarps) {
-    for (int j = lane; j < inner_n; j += 32) {
-      const int l = a.line_major ? o : j, i = a.line_major ? j : o;
-      out[bout[l] + static_cast<int64_t>(i) * a.out_st] = ppk::from_acc<S>(sm[i * pitch + l]);
+  if (a.line_major) {
+    for (int l = warp; l < nl; l += nwarps) {
+      S* dst = out + bout[l];
+      const C* src = sm + l;
+      for (int i = lane; i < n32; i += 32) dst[i * a.out_st] = ppk::from_acc<S>(src[i * pitch]);
+    }
+  } else {
+    for (int g = lane; g < ngroups; g += 32) {
+      const int l = g * G;
+      const bool vec = group_vec(bout, out, a.out_st, g, G * static_cast<int>(sizeof(S)));
+      S* dst = out + bout[l];
+      for (int i = warp; i < n32; i += nwarps) {
+        const C* src = sm + i * pitch + l;
+        const int64_t off = i * a.out_st;
+        if (vec) {
+          if constexpr (kAsync) {
+            *reinterpret_cast<uint4*>(dst + off) = *reinterpret_cast<const uint4*>(src);
+          } else {
+            const float4 f = *reinterpret_cast<const float4*>(src);
+            S v[4] = {ppk::from_acc<S>(f.x), ppk::from_acc<S>(f.y), ppk::from_acc<S>(f.z), ppk::from_acc<S>(f.w)};
+            *reinterpret_cast<uint2*>(dst + off) = *reinterpret_cast<const uint2*>(v);
+          }
+        } else {
+          for (int k = 0; k < G && l + k < nl; ++k) out[bout[l + k] + off] = ppk::from_acc<S>(src[k]);
+        }
+      }
     }
   }
 }
@@ -295,14 +418,22 @@ template <class S>
 int run_axis(LineArgs& a, cudaStream_t st) {
   using C = typename ppk::Acc<S>::type;
   if (a.nlines == 0) return PP_OK;
-  // two CTAs per SM where the lines allow; fewer, longer lines otherwise
+  // two CTAs per SM where the lines allow; fewer, longer lines otherwise.
+  // pitch: odd when warps stage whole lines (conflict-free column writes),
+  // else a multiple of the 16-byte group width.
+  constexpr int G = 16 / static_cast<int>(sizeof(C));
   size_t budget = 110 * 1024;
   int lines = 0, pitch = 0;
   for (int pass = 0; pass < 2 && lines < 1; ++pass, budget = 200 * 1024) {
     const int64_t fit = static_cast<int64_t>(budget / (static_cast<size_t>(a.n) * sizeof(C)));
     lines = static_cast<int>(fit < LINES ? fit : LINES);
-    pitch = lines | 1;
-    if (static_cast<int64_t>(pitch) > fit) pitch = --lines;  // lines was even: drop one
+    if (a.line_major) {
+      pitch = lines | 1;
+      if (static_cast<int64_t>(pitch) > fit) pitch = --lines;  // lines was even: drop one
+    } else {
+      if (lines >= G) lines -= lines % G;
+      pitch = lines;
+    }
   }
   if (lines >= 1) {
     const size_t smem = static_cast<size_t>(a.n) * pitch * sizeof(C);
@@ -345,7 +476,27 @@ int coeff_axis(const pp_tensor* in, const pp_tensor* out, int bound, int order, 
                         "(only zero, replicate, dct1, dct2 and dft)", bound);
   if (a.n == 1) return copy_any(in, out, st);
   a.gain = 1.0;
-  for (int q = 0; q < a.npoles; ++q) a.gain *= (1.0 - a.z[q]) * (1.0 - 1.0 / a.z[q]);
+  for (int q = 0; q < a.npoles; ++q) {
+    const double z = a.z[q];
+    a.gain *= (1.0 - z) * (1.0 - 1.0 / z);
+    // truncation of the causal initial sums (coeff.py:75, :100): |z|^m < 1e-13
+    const int64_t m = static_cast<int64_t>(std::ceil(-30.0 / std::log(std::fabs(z))));
+    if (a.kind == 2) {
+      const int64_t K = static_cast<int64_t>(std::ceil(-44.4 / std::log(std::fabs(z)))) + 1;
+      const int64_t k2 = std::max<int64_t>(1, 2 * a.n - 1 - K);
+      a.hz[q] = K;
+      a.zp[q] = std::pow(z, static_cast<double>(a.n));
+      a.zq[q] = std::pow(z, static_cast<double>(2 * a.n - 1 - k2));
+    } else if (a.kind == 1) {
+      a.hz[q] = m;
+      a.zp[q] = std::pow(z, static_cast<double>(a.n - 1));
+      a.zq[q] = 0.0;
+    } else {
+      a.hz[q] = std::min<int64_t>(m, a.n);
+      a.zp[q] = std::pow(z, static_cast<double>(a.hz[q]));
+      a.zq[q] = 0.0;
+    }
+  }
   a.ndo = 0;
   a.nlines = 1;
   int64_t min_other = INT64_MAX;

@@ -58,6 +58,43 @@ def test_coeff_axes_and_layouts(bound, shape):
     assert relerr(nb.spline_coeff_nd(X.float(), 3, name, dim=3).double().cpu().numpy(), ref) < 1e-5
 
 
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16])
+@pytest.mark.parametrize("n", [8, 9, 15, 16, 17, 24, 25, 129])
+@pytest.mark.parametrize("bound", [2, 3, 6])
+def test_coeff_register_chunk_lengths(dtype, n, bound):
+    """Line lengths around the recursion's 8-sample register chunks, along
+    the fastest axis (warps stage whole lines) and a strided one (warps stage
+    one sample of 32 adjacent lines)."""
+    r = np.random.default_rng(n + bound)
+    tol = {torch.float64: 1e-11, torch.float32: 1e-5, torch.bfloat16: 1e-5}[dtype]
+    for order in (3, 7):
+        for shape, axis in (((3, 5, n), -1), ((3, n, 37), 1)):
+            x = torch.from_numpy(r.standard_normal(shape)).to(dtype)
+            ref = O.spline_coeff(x.double().numpy(), bound, order, dim=axis)
+            y = coeff.spline_coeff(x.cuda(), bound, order, dim=axis)
+            if dtype == torch.bfloat16:
+                # recursions in float, one bfloat16 rounding of the output
+                assert relerr(y.double().cpu().numpy(), ref) < 8e-3
+            else:
+                assert relerr(y.double().cpu().numpy(), ref) < tol
+
+
+@pytest.mark.parametrize("dtype,n", [(torch.float32, 30000), (torch.float32, 60000), (torch.float64, 30000)])
+def test_coeff_lines_beyond_tile_budget(dtype, n):
+    """Lines too long for two CTAs per SM (one wide tile per CTA), and lines
+    too long for shared memory altogether (recursion in global memory)."""
+    r = np.random.default_rng(n)
+    x = r.standard_normal((3, n))
+    ref = O.spline_coeff(x, 3, 3, dim=-1)
+    y = coeff.spline_coeff(torch.from_numpy(x).to(dtype).cuda(), 3, 3, dim=-1)
+    assert relerr(y.double().cpu().numpy(), ref) < (1e-11 if dtype == torch.float64 else 1e-5)
+
+
+def test_coeff_bf16_line_too_long_raises():
+    with pytest.raises(Exception):
+        coeff.spline_coeff(torch.zeros(2, 60000, device="cuda", dtype=torch.bfloat16), 3, 3, dim=-1)
+
+
 def test_coeff_interpolates_long_lines():
     x = torch.randn(1, 1, 96, 80, 72, dtype=torch.double, device="cuda")
     grid = nb.identity_grid(x.shape[2:], dtype=torch.double, device="cuda")[None]
