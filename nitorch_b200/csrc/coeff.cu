@@ -14,13 +14,12 @@
 // fall back to the same recursion directly on global memory.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "pp_capi_internal.cuh"
 
 namespace {
 
-constexpr int LINES = 128;    // lines per CTA: one per thread in the recursions
-constexpr int THREADS = 256;  // all stage and store; the first LINES recurse
 constexpr int UNROLL = 8;     // 16-bit storage: loads in flight per thread while staging
 
 struct LineArgs {
@@ -66,13 +65,13 @@ struct LineRef {
   __device__ __forceinline__ C& operator[](int64_t i) const { return p[i * st]; }
 };
 
-template <class C>
+template <class C, int P>  // P: compile-time pitch, 0 = runtime
 struct TileLine {
   using value_type = C;
   using index_type = int;
   C* p;
   int pitch;
-  __device__ __forceinline__ C& operator[](int i) const { return p[i * pitch]; }
+  __device__ __forceinline__ C& operator[](int i) const { return p[i * (P ? P : pitch)]; }
 };
 
 // Initial causal coefficient (coeff.py:69-170), double accumulation.  The
@@ -218,47 +217,53 @@ __device__ __forceinline__ void load_group(C* dst, const S* src) {
                                                 ppk::to_acc(v[3]));
 }
 
-// Shared-memory line kernel: up to LINES lines per CTA, one per thread in
-// the recursions, held element-major in shared memory (tile[i * pitch + l]).
-// Staging walks the tile so that a warp touches consecutive addresses of
-// global memory:
+// Shared-memory line kernel: NL threads, up to NL lines per CTA, one per
+// thread, held element-major in shared memory (tile[i * pitch + l]).  Small
+// CTAs (a few warps) several to an SM: each loads its tile, recurses and
+// stores on its own schedule, so the loads of some overlap the recursions of
+// others.  Staging walks the tile so that a warp touches consecutive
+// addresses of global memory:
 //  * filtered axis the fastest (line_major): a warp per line, lanes over
 //    consecutive samples; odd pitch, so the lanes' column writes are
 //    conflict-free;
-//  * otherwise a warp per sample row, each lane a group of G = 16 / sizeof(C)
-//    adjacent lines moved as one 16-byte copy (8-byte load for 16-bit
-//    storage) when the G lines are adjacent and aligned in memory, else G
-//    scalar copies; pitch a multiple of G.
+//  * otherwise each thread a group of G = 16 / sizeof(C) adjacent lines on
+//    every G-th sample row, moved as one 16-byte copy (8-byte load for
+//    16-bit storage) when the G lines are adjacent and aligned in memory, else
+//    G scalar copies; pitch a multiple of G.
 // float / double storage stage with asynchronous copies, so that the whole
-// tile is in flight at once (what it takes to keep HBM busy at two CTAs per
-// SM); 16-bit storage converts through registers.  Per-lane pointers are
-// formed once per line / group: the sample loops are an add and a copy.
-template <class S>
-__global__ void __launch_bounds__(THREADS, 2) coeff_smem_kernel(LineArgs a, int pitch, int lines) {
+// tile is in flight at once; 16-bit storage converts through registers.
+// P: the pitch as a compile-time constant for full tiles (NL + 1 for
+// line_major, NL otherwise), 0 for the runtime pitch of long-line tiles.
+template <class S, int NL, int P>
+__global__ void __launch_bounds__(NL) coeff_smem_kernel(LineArgs a, int pitch_rt, int lines) {
   using C = typename ppk::Acc<S>::type;
   constexpr int G = 16 / static_cast<int>(sizeof(C));
+  constexpr int GPR = NL / G;  // groups per sample row
   constexpr bool kAsync = sizeof(S) == sizeof(C);
+  static_assert(NL % 32 == 0 && NL % G == 0, "tile of whole warps and groups");
+  const int pitch = P ? P : pitch_rt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
   const int64_t l0 = static_cast<int64_t>(blockIdx.x) * lines;
   const int nl = static_cast<int>(a.nlines - l0 < lines ? a.nlines - l0 : lines);
   const S* in = static_cast<const S*>(a.in);
   S* out = static_cast<S*>(a.out);
-  __shared__ int64_t bin[LINES], bout[LINES];
-  for (int l = threadIdx.x; l < nl; l += blockDim.x) line_base(a, l0 + l, bin[l], bout[l]);
+  __shared__ int64_t bin[NL], bout[NL];
+  for (int l = threadIdx.x; l < nl; l += NL) line_base(a, l0 + l, bin[l], bout[l]);
   __syncthreads();
   const int n32 = static_cast<int>(a.n);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int ngroups = (nl + G - 1) / G;
-  // vector eligibility of group g: G lines present, adjacent, aligned rows
-  auto group_vec = [&](const int64_t* base, const void* ptr, int64_t st, int g, int bytes) {
-    const int l = g * G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int nwarps = NL / 32;
+  // vector eligibility of the group at line l: G lines present, adjacent,
+  // every row aligned
+  auto group_vec = [&](const int64_t* base, const void* ptr, int64_t st, int l, int bytes) {
     if (l + G > nl || (pitch % G) != 0) return false;
     for (int k = 1; k < G; ++k)
       if (base[l + k] != base[l] + k) return false;
     const uintptr_t p = reinterpret_cast<uintptr_t>(ptr) + static_cast<uintptr_t>(base[l]) * sizeof(S);
     return (p % bytes) == 0 && ((st * static_cast<int64_t>(sizeof(S))) % bytes) == 0;
   };
+  const int gl = (threadIdx.x % GPR) * G, r0 = threadIdx.x / GPR;  // strided: group line, first row
   if (a.line_major) {
     for (int l = warp; l < nl; l += nwarps) {
       const S* src = in + bin[l];
@@ -281,37 +286,26 @@ __global__ void __launch_bounds__(THREADS, 2) coeff_smem_kernel(LineArgs a, int 
         }
       }
     }
-  } else {
-    for (int g = lane; g < ngroups; g += 32) {
-      const int l = g * G;
-      const bool vec = group_vec(bin, in, a.in_st, g, G * static_cast<int>(sizeof(S)));
-      const S* src = in + bin[l];
-      if constexpr (kAsync) {
-        for (int i = warp; i < n32; i += nwarps) {
-          C* dst = sm + i * pitch + l;
-          const int64_t off = i * a.in_st;
-          if (vec) {
-            cp_async<16>(dst, src + off);
-          } else {
-            for (int k = 0; k < G && l + k < nl; ++k) cp_async<sizeof(C)>(dst + k, in + bin[l + k] + off);
-          }
-        }
+  } else if (gl < nl) {
+    const bool vec = group_vec(bin, in, a.in_st, gl, G * static_cast<int>(sizeof(S)));
+    const S* src = in + bin[gl];
+    for (int i = r0; i < n32; i += G) {
+      C* dst = sm + i * pitch + gl;
+      const int64_t off = i * a.in_st;
+      if (vec) {
+        if constexpr (kAsync) cp_async<16>(dst, src + off);
+        else load_group(dst, src + off);
       } else {
-        for (int i = warp; i < n32; i += nwarps) {
-          C* dst = sm + i * pitch + l;
-          const int64_t off = i * a.in_st;
-          if (vec) {
-            load_group(dst, src + off);
-          } else {
-            for (int k = 0; k < G && l + k < nl; ++k) dst[k] = ppk::to_acc(in[bin[l + k] + off]);
-          }
+        for (int k = 0; k < G && gl + k < nl; ++k) {
+          if constexpr (kAsync) cp_async<sizeof(C)>(dst + k, in + bin[gl + k] + off);
+          else dst[k] = ppk::to_acc(in[bin[gl + k] + off]);
         }
       }
     }
   }
   if constexpr (kAsync) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
-  if (threadIdx.x < nl) filter_line(TileLine<C>{sm + threadIdx.x, pitch}, n32, a);
+  if (threadIdx.x < nl) filter_line(TileLine<C, P>{sm + threadIdx.x, pitch}, n32, a);
   __syncthreads();
   if (a.line_major) {
     for (int l = warp; l < nl; l += nwarps) {
@@ -319,25 +313,22 @@ __global__ void __launch_bounds__(THREADS, 2) coeff_smem_kernel(LineArgs a, int 
       const C* src = sm + l;
       for (int i = lane; i < n32; i += 32) dst[i * a.out_st] = ppk::from_acc<S>(src[i * pitch]);
     }
-  } else {
-    for (int g = lane; g < ngroups; g += 32) {
-      const int l = g * G;
-      const bool vec = group_vec(bout, out, a.out_st, g, G * static_cast<int>(sizeof(S)));
-      S* dst = out + bout[l];
-      for (int i = warp; i < n32; i += nwarps) {
-        const C* src = sm + i * pitch + l;
-        const int64_t off = i * a.out_st;
-        if (vec) {
-          if constexpr (kAsync) {
-            *reinterpret_cast<uint4*>(dst + off) = *reinterpret_cast<const uint4*>(src);
-          } else {
-            const float4 f = *reinterpret_cast<const float4*>(src);
-            S v[4] = {ppk::from_acc<S>(f.x), ppk::from_acc<S>(f.y), ppk::from_acc<S>(f.z), ppk::from_acc<S>(f.w)};
-            *reinterpret_cast<uint2*>(dst + off) = *reinterpret_cast<const uint2*>(v);
-          }
+  } else if (gl < nl) {
+    const bool vec = group_vec(bout, out, a.out_st, gl, G * static_cast<int>(sizeof(S)));
+    S* dst = out + bout[gl];
+    for (int i = r0; i < n32; i += G) {
+      const C* src = sm + i * pitch + gl;
+      const int64_t off = i * a.out_st;
+      if (vec) {
+        if constexpr (kAsync) {
+          *reinterpret_cast<uint4*>(dst + off) = *reinterpret_cast<const uint4*>(src);
         } else {
-          for (int k = 0; k < G && l + k < nl; ++k) out[bout[l + k] + off] = ppk::from_acc<S>(src[k]);
+          const float4 f = *reinterpret_cast<const float4*>(src);
+          S v[4] = {ppk::from_acc<S>(f.x), ppk::from_acc<S>(f.y), ppk::from_acc<S>(f.z), ppk::from_acc<S>(f.w)};
+          *reinterpret_cast<uint2*>(dst + off) = *reinterpret_cast<const uint2*>(v);
         }
+      } else {
+        for (int k = 0; k < G && gl + k < nl; ++k) out[bout[gl + k] + off] = ppk::from_acc<S>(src[k]);
       }
     }
   }
@@ -414,36 +405,44 @@ int copy_any(const pp_tensor* in, const pp_tensor* out, cudaStream_t st) {
   }
 }
 
-template <class S>
-int run_axis(LineArgs& a, cudaStream_t st) {
+// Lines per CTA (= threads): small CTAs, several per SM.
+int tile_lines() {
+  static const int nl = [] {
+    const char* e = std::getenv("PP_COEFF_LINES");
+    const int v = e ? std::atoi(e) : 64;
+    return (v == 32 || v == 64 || v == 128) ? v : 64;
+  }();
+  return nl;
+}
+
+template <class S, int NL>
+int run_tiles(LineArgs& a, cudaStream_t st) {
   using C = typename ppk::Acc<S>::type;
-  if (a.nlines == 0) return PP_OK;
-  // two CTAs per SM where the lines allow; fewer, longer lines otherwise.
-  // pitch: odd when warps stage whole lines (conflict-free column writes),
-  // else a multiple of the 16-byte group width.
   constexpr int G = 16 / static_cast<int>(sizeof(C));
-  size_t budget = 110 * 1024;
-  int lines = 0, pitch = 0;
-  for (int pass = 0; pass < 2 && lines < 1; ++pass, budget = 200 * 1024) {
-    const int64_t fit = static_cast<int64_t>(budget / (static_cast<size_t>(a.n) * sizeof(C)));
-    lines = static_cast<int>(fit < LINES ? fit : LINES);
-    if (a.line_major) {
-      pitch = lines | 1;
-      if (static_cast<int64_t>(pitch) > fit) pitch = --lines;  // lines was even: drop one
-    } else {
-      if (lines >= G) lines -= lines % G;
-      pitch = lines;
-    }
+  // pitch: odd when warps stage whole lines (conflict-free column writes),
+  // else a multiple of the 16-byte group width; long lines take fewer lines
+  // per CTA, up to 200 KB of shared memory.
+  const size_t budget = 200 * 1024;
+  const int64_t fit = static_cast<int64_t>(budget / (static_cast<size_t>(a.n) * sizeof(C)));
+  int lines = static_cast<int>(fit < NL ? fit : NL), pitch = 0;
+  if (a.line_major) {
+    pitch = lines | 1;
+    if (static_cast<int64_t>(pitch) > fit) pitch = --lines;  // lines was even: drop one
+  } else {
+    if (lines >= G) lines -= lines % G;
+    pitch = lines;
   }
   if (lines >= 1) {
     const size_t smem = static_cast<size_t>(a.n) * pitch * sizeof(C);
-    auto k = coeff_smem_kernel<S>;
+    const bool full = lines == NL && pitch == (a.line_major ? NL + 1 : NL);
+    auto k = !full ? coeff_smem_kernel<S, NL, 0>
+                   : (a.line_major ? coeff_smem_kernel<S, NL, NL + 1> : coeff_smem_kernel<S, NL, NL>);
     if (smem > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e != cudaSuccess) return ppc::cuda_check(e, "prefilter smem attribute");
     }
     const int64_t blocks = (a.nlines + lines - 1) / lines;
-    k<<<static_cast<unsigned>(blocks), THREADS, smem, st>>>(a, pitch, lines);
+    k<<<static_cast<unsigned>(blocks), NL, smem, st>>>(a, pitch, lines);
     ppc::count_launch();
   } else {
     if constexpr (sizeof(S) < 4) {
@@ -456,6 +455,16 @@ int run_axis(LineArgs& a, cudaStream_t st) {
     }
   }
   return ppc::cuda_check(cudaGetLastError(), "prefilter launch");
+}
+
+template <class S>
+int run_axis(LineArgs& a, cudaStream_t st) {
+  if (a.nlines == 0) return PP_OK;
+  switch (tile_lines()) {
+    case 32: return run_tiles<S, 32>(a, st);
+    case 128: return run_tiles<S, 128>(a, st);
+    default: return run_tiles<S, 64>(a, st);
+  }
 }
 
 int coeff_axis(const pp_tensor* in, const pp_tensor* out, int bound, int order, int axis,
