@@ -437,7 +437,8 @@ int run_tiles(LineArgs& a, cudaStream_t st) {
     const bool full = lines == NL && pitch == (a.line_major ? NL + 1 : NL);
     auto k = !full ? coeff_smem_kernel<S, NL, 0>
                    : (a.line_major ? coeff_smem_kernel<S, NL, NL + 1> : coeff_smem_kernel<S, NL, NL>);
-    if (smem > 48 * 1024) {
+    // the 48 KB default covers static (line bases) plus dynamic shared memory
+    if (smem + 2 * NL * sizeof(int64_t) > 48 * 1024) {
       cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e != cudaSuccess) return ppc::cuda_check(e, "prefilter smem attribute");
     }

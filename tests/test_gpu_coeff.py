@@ -59,16 +59,17 @@ def test_coeff_axes_and_layouts(bound, shape):
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16])
-@pytest.mark.parametrize("n", [8, 9, 15, 16, 17, 24, 25, 129])
+@pytest.mark.parametrize("n", [8, 9, 15, 16, 17, 24, 25, 96, 129, 192, 384])
 @pytest.mark.parametrize("bound", [2, 3, 6])
 def test_coeff_register_chunk_lengths(dtype, n, bound):
-    """Line lengths around the recursion's 8-sample register chunks, along
-    the fastest axis (warps stage whole lines) and a strided one (warps stage
-    one sample of 32 adjacent lines)."""
+    """Line lengths around the recursion's 8-sample register chunks and tiles
+    at the 48 KB default shared-memory limit (96 / 192 / 384 samples), along
+    the fastest axis (warps stage whole lines) and a strided one (threads
+    stage groups of adjacent lines)."""
     r = np.random.default_rng(n + bound)
     tol = {torch.float64: 1e-11, torch.float32: 1e-5, torch.bfloat16: 1e-5}[dtype]
     for order in (3, 7):
-        for shape, axis in (((3, 5, n), -1), ((3, n, 37), 1)):
+        for shape, axis in (((3, 5, n), -1), ((3, n, 37), 1), ((140, n), -1), ((n, 140), 0)):
             x = torch.from_numpy(r.standard_normal(shape)).to(dtype)
             ref = O.spline_coeff(x.double().numpy(), bound, order, dim=axis)
             y = coeff.spline_coeff(x.cuda(), bound, order, dim=axis)
