@@ -14,7 +14,6 @@
 // fall back to the same recursion directly on global memory.
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 
 #include "pp_capi_internal.cuh"
 
@@ -54,146 +53,267 @@ __device__ __forceinline__ void line_base(const LineArgs& a, int64_t l, int64_t&
   }
 }
 
-// Accessors over one line: in global memory (any stride) or in the shared
-// tile (element-major, one column per line, pitch = lines per CTA | 1).
+// Accessors over V adjacent lines (V = 1: one line); load / store move
+// sample i of the V lines.
 template <class C>
-struct LineRef {
+struct LineRef {  // one line in global memory, any stride
+  static constexpr int V = 1;
   using value_type = C;
   using index_type = int64_t;
   C* p;
   int64_t st;
-  __device__ __forceinline__ C& operator[](int64_t i) const { return p[i * st]; }
+  __device__ __forceinline__ void load(int64_t i, C (&x)[1]) const { x[0] = p[i * st]; }
+  __device__ __forceinline__ void store(int64_t i, const C (&x)[1]) const { p[i * st] = x[0]; }
 };
 
-template <class C, int P>  // P: compile-time pitch, 0 = runtime
-struct TileLine {
+template <class C>
+struct TileLine {  // one column of a shared tile, runtime pitch
+  static constexpr int V = 1;
   using value_type = C;
   using index_type = int;
   C* p;
   int pitch;
-  __device__ __forceinline__ C& operator[](int i) const { return p[i * (P ? P : pitch)]; }
+  __device__ __forceinline__ void load(int i, C (&x)[1]) const { x[0] = p[i * pitch]; }
+  __device__ __forceinline__ void store(int i, const C (&x)[1]) const { p[i * pitch] = x[0]; }
 };
 
-// Initial causal coefficient (coeff.py:69-170), double accumulation.  The
-// samples are read as L[k] * g (g: the filter gain on the first pole's pass,
-// 1 afterwards), so the gain pass costs no separate sweep.
-template <class R, class C = typename R::value_type>
-__device__ double initial(const R& L, int64_t n, const LineArgs& a, int q, C g) {
+template <class C, int P>
+struct TileCols {  // 16 / sizeof(C) adjacent columns of a shared tile, one 16-byte access
+  static constexpr int V = 16 / static_cast<int>(sizeof(C));
+  using value_type = C;
+  using index_type = int;
+  C* p;
+  __device__ __forceinline__ void load(int i, C (&x)[V]) const {
+    if constexpr (V == 4) {
+      const float4 t = *reinterpret_cast<const float4*>(p + i * P);
+      x[0] = t.x; x[1] = t.y; x[2] = t.z; x[3] = t.w;
+    } else {
+      const double2 t = *reinterpret_cast<const double2*>(p + i * P);
+      x[0] = t.x; x[1] = t.y;
+    }
+  }
+  __device__ __forceinline__ void store(int i, const C (&x)[V]) const {
+    if constexpr (V == 4) *reinterpret_cast<float4*>(p + i * P) = make_float4(x[0], x[1], x[2], x[3]);
+    else *reinterpret_cast<double2*>(p + i * P) = make_double2(x[0], x[1]);
+  }
+};
+
+// Initial causal coefficient (coeff.py:69-170) of each of the V lines,
+// double accumulation.  The samples are read as L[k] * g (g: the filter gain
+// on the first pole's pass, 1 afterwards), so the gain costs no separate
+// sweep.
+template <class R, int V = R::V, class C = typename R::value_type>
+__device__ void initial(const R& L, int64_t n, const LineArgs& a, int q, C g, double (&out)[V]) {
   const double z = a.z[q];
-  auto x = [&](int64_t k) { return static_cast<double>(L[k] * g); };
+  C t[V];
+  double xv[V], x0[V], acc[V];
+  auto x = [&](int64_t k) {
+    L.load(k, t);
+#pragma unroll
+    for (int c = 0; c < V; ++c) xv[c] = static_cast<double>(t[c] * g);
+  };
+  x(0);
+#pragma unroll
+  for (int c = 0; c < V; ++c) x0[c] = acc[c] = xv[c];
   if (a.kind == 2) {  // dct2 / replicate (coeff.py:137-170)
     const double zn = a.zp[q];
     const double zlast = zn * (1.0 + 1.0 / (z + zn * zn));
-    double acc = x(0) + zlast * x(n - 1);
+    x(n - 1);
+#pragma unroll
+    for (int c = 0; c < V; ++c) acc[c] += zlast * xv[c];
     // sum_{k=1}^{n-2} (z^k + z^(2n-1-k)) L[k]; both power series decay
     // geometrically, terms below 2^-64 of the leading one are dropped.
     const int64_t K = a.hz[q];
     const int64_t k1 = n - 2 < K ? n - 2 : K;
     double zk = z;
-    for (int64_t k = 1; k <= k1; ++k, zk *= z) acc += zk * x(k);
+    for (int64_t k = 1; k <= k1; ++k, zk *= z) {
+      x(k);
+#pragma unroll
+      for (int c = 0; c < V; ++c) acc[c] += zk * xv[c];
+    }
     int64_t k2 = 2 * n - 1 - K;
     if (k2 < 1) k2 = 1;
     if (k2 <= n - 2) {
       double zq = a.zq[q];
       const double iz = 1.0 / z;
-      for (int64_t k = k2; k <= n - 2; ++k, zq *= iz) acc += zq * x(k);
+      for (int64_t k = k2; k <= n - 2; ++k, zq *= iz) {
+        x(k);
+#pragma unroll
+        for (int c = 0; c < V; ++c) acc[c] += zq * xv[c];
+      }
     }
-    return acc * (z / (1.0 - zn * zn)) + x(0);
+    const double s = z / (1.0 - zn * zn);
+#pragma unroll
+    for (int c = 0; c < V; ++c) out[c] = acc[c] * s + x0[c];
+    return;
   }
   if (a.kind == 1) {  // dct1 / zero (coeff.py:94-134)
     const int64_t m = a.hz[q];
     if (m < n) {
-      double acc = x(0), zk = z;
-      for (int64_t k = 1; k < m; ++k, zk *= z) acc += zk * x(k);
-      return acc;
+      double zk = z;
+      for (int64_t k = 1; k < m; ++k, zk *= z) {
+        x(k);
+#pragma unroll
+        for (int c = 0; c < V; ++c) acc[c] += zk * xv[c];
+      }
+#pragma unroll
+      for (int c = 0; c < V; ++c) out[c] = acc[c];
+      return;
     }
     const double zn = a.zp[q];
-    double acc = x(0) + zn * x(n - 1);
+    x(n - 1);
+#pragma unroll
+    for (int c = 0; c < V; ++c) acc[c] += zn * xv[c];
     double zk = z;
-    for (int64_t k = 1; k < n - 1; ++k, zk *= z) acc += (zk + zn * zn / zk) * x(k);
-    return acc / (1.0 - zn * zn);
+    for (int64_t k = 1; k < n - 1; ++k, zk *= z) {
+      x(k);
+      const double w = zk + zn * zn / zk;
+#pragma unroll
+      for (int c = 0; c < V; ++c) acc[c] += w * xv[c];
+    }
+    const double s = 1.0 / (1.0 - zn * zn);
+#pragma unroll
+    for (int c = 0; c < V; ++c) out[c] = acc[c] * s;
+    return;
   }
   // dft (coeff.py:69-91)
   const int64_t m = a.hz[q];
-  double acc = x(0), zj = z;
-  for (int64_t j = 1; j < m; ++j, zj *= z) acc += zj * x(n - j);
-  return acc / (1.0 - a.zp[q]);
+  double zj = z;
+  for (int64_t j = 1; j < m; ++j, zj *= z) {
+    x(n - j);
+#pragma unroll
+    for (int c = 0; c < V; ++c) acc[c] += zj * xv[c];
+  }
+  const double s = 1.0 / (1.0 - a.zp[q]);
+#pragma unroll
+  for (int c = 0; c < V; ++c) out[c] = acc[c] * s;
 }
 
-// Final anti-causal coefficient (coeff.py:173-215).
-template <class R>
-__device__ double final_value(const R& L, int64_t n, const LineArgs& a, int q) {
+// Final anti-causal coefficient (coeff.py:173-215) of each of the V lines.
+template <class R, int V = R::V, class C = typename R::value_type>
+__device__ void final_value(const R& L, int64_t n, const LineArgs& a, int q, double (&out)[V]) {
   const double z = a.z[q];
-  if (a.kind == 2) return static_cast<double>(L[n - 1]) * (z / (z - 1.0));
-  if (a.kind == 1) return (z * static_cast<double>(L[n - 2]) + static_cast<double>(L[n - 1])) * (z / (z * z - 1.0));
+  C t[V];
+  L.load(n - 1, t);
+  if (a.kind == 2) {
+    const double s = z / (z - 1.0);
+#pragma unroll
+    for (int c = 0; c < V; ++c) out[c] = static_cast<double>(t[c]) * s;
+    return;
+  }
+  if (a.kind == 1) {
+    C u[V];
+    L.load(n - 2, u);
+    const double s = z / (z * z - 1.0);
+#pragma unroll
+    for (int c = 0; c < V; ++c) out[c] = (z * static_cast<double>(u[c]) + static_cast<double>(t[c])) * s;
+    return;
+  }
   const int64_t m = a.hz[q];
-  double acc = z * static_cast<double>(L[n - 1]), zj = z * z;
-  for (int64_t j = 0; j < m - 1; ++j, zj *= z) acc += zj * static_cast<double>(L[j]);
-  return acc / (a.zp[q] - 1.0);
+  double acc[V];
+#pragma unroll
+  for (int c = 0; c < V; ++c) acc[c] = z * static_cast<double>(t[c]);
+  double zj = z * z;
+  for (int64_t j = 0; j < m - 1; ++j, zj *= z) {
+    L.load(j, t);
+#pragma unroll
+    for (int c = 0; c < V; ++c) acc[c] += zj * static_cast<double>(t[c]);
+  }
+  const double s = 1.0 / (a.zp[q] - 1.0);
+#pragma unroll
+  for (int c = 0; c < V; ++c) out[c] = acc[c] * s;
 }
 
 // Gain (coeff.py:61-65) folded into the first causal pass, then one causal
-// and one anti-causal recursion per pole (coeff.py:254-281).  The walks go
-// in chunks of RU samples held in registers, the next chunk loaded before the
-// current one is filtered, so that the memory latency leaves the dependency
-// chain (one FMA per sample); the accessor's stride is a runtime value, which
-// keeps the compiler from reordering the loads past the stores by itself.
-constexpr int RU = 8;
-
+// and one anti-causal recursion per pole (coeff.py:254-281), on V lines at
+// once (independent dependency chains).  The walks go in chunks of U samples
+// held in registers, the next chunk loaded before the current one is
+// filtered, so that the memory latency leaves the dependency chains.
 template <class R>
 __device__ void filter_line(const R& L, typename R::index_type n, const LineArgs& a) {
   using C = typename R::value_type;
   using I = typename R::index_type;
+  constexpr int V = R::V;
+  constexpr int U = V == 1 ? 8 : 4;
   C g = static_cast<C>(a.gain);
   for (int q = 0; q < a.npoles; ++q) {
-    const double zd = a.z[q];
-    const C z = static_cast<C>(zd);
-    C prev = static_cast<C>(initial(L, n, a, q, g));
-    L[0] = prev;
+    const C z = static_cast<C>(a.z[q]);
+    double d[V];
+    C prev[V];
+    initial(L, n, a, q, g, d);
+#pragma unroll
+    for (int c = 0; c < V; ++c) prev[c] = static_cast<C>(d[c]);
+    L.store(0, prev);
     I i = 1;  // causal: i = 1 .. n-1
-    if (n - 1 >= RU) {
-      C x[RU];
+    if (n - 1 >= U) {
+      C x[U][V];
 #pragma unroll
-      for (int u = 0; u < RU; ++u) x[u] = L[i + u];
+      for (int u = 0; u < U; ++u) L.load(i + u, x[u]);
       for (;;) {
-        const bool more = i + 2 * RU <= n;
-        C y[RU];
+        const bool more = i + 2 * U <= n;
+        C y[U][V];
         if (more) {
 #pragma unroll
-          for (int u = 0; u < RU; ++u) y[u] = L[i + RU + u];
+          for (int u = 0; u < U; ++u) L.load(i + U + u, y[u]);
         }
 #pragma unroll
-        for (int u = 0; u < RU; ++u) { prev = fma(z, prev, x[u] * g); L[i + u] = prev; }
-        i += RU;
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+          for (int c = 0; c < V; ++c) prev[c] = fma(z, prev[c], x[u][c] * g);
+          L.store(i + u, prev);
+        }
+        i += U;
         if (!more) break;
 #pragma unroll
-        for (int u = 0; u < RU; ++u) x[u] = y[u];
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+          for (int c = 0; c < V; ++c) x[u][c] = y[u][c];
       }
     }
-    for (; i < n; ++i) { prev = fma(z, prev, L[i] * g); L[i] = prev; }
-    prev = static_cast<C>(final_value(L, n, a, q));
-    L[n - 1] = prev;
+    for (; i < n; ++i) {
+      C x[V];
+      L.load(i, x);
+#pragma unroll
+      for (int c = 0; c < V; ++c) prev[c] = fma(z, prev[c], x[c] * g);
+      L.store(i, prev);
+    }
+    final_value(L, n, a, q, d);
+#pragma unroll
+    for (int c = 0; c < V; ++c) prev[c] = static_cast<C>(d[c]);
+    L.store(n - 1, prev);
     i = n - 2;  // anti-causal: i = n-2 .. 0
-    if (i + 1 >= RU) {
-      C x[RU];
+    if (i + 1 >= U) {
+      C x[U][V];
 #pragma unroll
-      for (int u = 0; u < RU; ++u) x[u] = L[i - u];
+      for (int u = 0; u < U; ++u) L.load(i - u, x[u]);
       for (;;) {
-        const bool more = i + 1 >= 2 * RU;
-        C y[RU];
+        const bool more = i + 1 >= 2 * U;
+        C y[U][V];
         if (more) {
 #pragma unroll
-          for (int u = 0; u < RU; ++u) y[u] = L[i - RU - u];
+          for (int u = 0; u < U; ++u) L.load(i - U - u, y[u]);
         }
 #pragma unroll
-        for (int u = 0; u < RU; ++u) { prev = z * (prev - x[u]); L[i - u] = prev; }
-        i -= RU;
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+          for (int c = 0; c < V; ++c) prev[c] = z * (prev[c] - x[u][c]);
+          L.store(i - u, prev);
+        }
+        i -= U;
         if (!more) break;
 #pragma unroll
-        for (int u = 0; u < RU; ++u) x[u] = y[u];
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+          for (int c = 0; c < V; ++c) x[u][c] = y[u][c];
       }
     }
-    for (; i >= 0; --i) { prev = z * (prev - L[i]); L[i] = prev; }
+    for (; i >= 0; --i) {
+      C x[V];
+      L.load(i, x);
+#pragma unroll
+      for (int c = 0; c < V; ++c) prev[c] = z * (prev[c] - x[c]);
+      L.store(i, prev);
+    }
     g = C(1);
   }
 }
@@ -217,77 +337,171 @@ __device__ __forceinline__ void load_group(C* dst, const S* src) {
                                                 ppk::to_acc(v[3]));
 }
 
-// Shared-memory line kernel: NL threads, up to NL lines per CTA, one per
-// thread, held element-major in shared memory (tile[i * pitch + l]).  Small
-// CTAs (a few warps) several to an SM: each loads its tile, recurses and
-// stores on its own schedule, so the loads of some overlap the recursions of
-// others.  Staging walks the tile so that a warp touches consecutive
-// addresses of global memory:
-//  * filtered axis the fastest (line_major): a warp per line, lanes over
-//    consecutive samples; odd pitch, so the lanes' column writes are
-//    conflict-free;
-//  * otherwise each thread a group of G = 16 / sizeof(C) adjacent lines on
-//    every G-th sample row, moved as one 16-byte copy (8-byte load for
-//    16-bit storage) when the G lines are adjacent and aligned in memory, else
-//    G scalar copies; pitch a multiple of G.
-// float / double storage stage with asynchronous copies, so that the whole
-// tile is in flight at once; 16-bit storage converts through registers.
-// P: the pitch as a compile-time constant for full tiles (NL + 1 for
-// line_major, NL otherwise), 0 for the runtime pitch of long-line tiles.
-template <class S, int NL, int P>
-__global__ void __launch_bounds__(NL) coeff_smem_kernel(LineArgs a, int pitch_rt, int lines) {
+// Vector eligibility of the group of G adjacent lines starting at tile line
+// l: all present, adjacent in memory, every sample row aligned to the group
+// width in bytes.
+template <class S, int G>
+__device__ __forceinline__ bool group_vec(const int64_t* base, const void* ptr, int64_t st, int l, int nl) {
+  constexpr int bytes = G * static_cast<int>(sizeof(S));
+  if (l + G > nl) return false;
+  for (int k = 1; k < G; ++k)
+    if (base[l + k] != base[l] + k) return false;
+  const uintptr_t p = reinterpret_cast<uintptr_t>(ptr) + static_cast<uintptr_t>(base[l]) * sizeof(S);
+  return (p % bytes) == 0 && ((st * static_cast<int64_t>(sizeof(S))) % bytes) == 0;
+}
+
+// Full-tile kernel (lines up to ~390 samples): NT = 32 * V lines per CTA,
+// V = 16 / sizeof(C) (128 lines for float arithmetic, 64 for double), held
+// element-major in shared memory: tile[i * P + l], P = NT + V (16-byte rows).
+// Four warps stage and store; warp 0 runs the recursions, each lane on V
+// adjacent lines read and written as one 16-byte vector (V independent
+// dependency chains, a quarter of the shared-memory instructions of one line
+// per thread).  Staging keeps warps on consecutive global addresses:
+//  * filtered axis the fastest (line_major): a warp instruction covers 8
+//    consecutive samples of 4 lines (32-byte segments); with P = 4 mod 32
+//    words the 32 shared-memory writes fall in 32 distinct banks;
+//  * otherwise each lane a group of V adjacent lines on every 4th sample row,
+//    moved as one 16-byte copy (8-byte load for 16-bit storage) when the lines
+//    are adjacent and aligned in memory, else V scalar copies.
+// float / double storage stage with asynchronous copies, the whole tile in
+// flight at once; 16-bit storage converts through registers.  Two CTAs fit
+// an SM for lines up to ~200 samples, so one's transfers overlap the other's
+// recursions.
+constexpr int TILE_THREADS = 128;
+
+template <class S>
+__global__ void __launch_bounds__(TILE_THREADS) coeff_tile_kernel(LineArgs a) {
+  using C = typename ppk::Acc<S>::type;
+  constexpr int V = 16 / static_cast<int>(sizeof(C));
+  constexpr int NT = 32 * V;
+  constexpr int P = NT + V;
+  constexpr int NW = TILE_THREADS / 32;
+  constexpr bool kAsync = sizeof(S) == sizeof(C);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  const int64_t l0 = static_cast<int64_t>(blockIdx.x) * NT;
+  const int nl = static_cast<int>(a.nlines - l0 < NT ? a.nlines - l0 : NT);
+  const S* in = static_cast<const S*>(a.in);
+  S* out = static_cast<S*>(a.out);
+  __shared__ int64_t bin[NT], bout[NT];
+  for (int l = threadIdx.x; l < nl; l += TILE_THREADS) line_base(a, l0 + l, bin[l], bout[l]);
+  __syncthreads();
+  const int n32 = static_cast<int>(a.n);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int qs = lane >> 3, qj = lane & 7;  // line_major: line in the quad, first sample
+  const int gl = lane * V;                   // strided: the lane's group of V lines
+  if (a.line_major) {
+    for (int qd = warp; qd * 4 < nl; qd += NW) {
+      const int l = qd * 4 + qs;
+      if (l >= nl) continue;
+      const S* src = in + bin[l];
+      C* dst = sm + l;
+      if constexpr (kAsync) {
+        for (int i = qj; i < n32; i += 8) cp_async<sizeof(C)>(dst + i * P, src + i * a.in_st);
+      } else {
+        for (int i0 = qj; i0 < n32; i0 += 8 * UNROLL) {
+          C v[UNROLL];
+#pragma unroll
+          for (int u = 0; u < UNROLL; ++u) {
+            const int i = i0 + 8 * u;
+            v[u] = i < n32 ? ppk::to_acc(src[i * a.in_st]) : C(0);
+          }
+#pragma unroll
+          for (int u = 0; u < UNROLL; ++u) {
+            const int i = i0 + 8 * u;
+            if (i < n32) dst[i * P] = v[u];
+          }
+        }
+      }
+    }
+  } else if (gl < nl) {
+    const bool vec = group_vec<S, V>(bin, in, a.in_st, gl, nl);
+    const S* src = in + bin[gl];
+    for (int i = warp; i < n32; i += NW) {
+      C* dst = sm + i * P + gl;
+      const int64_t off = i * a.in_st;
+      if (vec) {
+        if constexpr (kAsync) cp_async<16>(dst, src + off);
+        else load_group(dst, src + off);
+      } else {
+        for (int k = 0; k < V && gl + k < nl; ++k) {
+          if constexpr (kAsync) cp_async<sizeof(C)>(dst + k, in + bin[gl + k] + off);
+          else dst[k] = ppk::to_acc(in[bin[gl + k] + off]);
+        }
+      }
+    }
+  }
+  if constexpr (kAsync) asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+  // columns past nl (last tile) hold stale shared memory: filtered, never stored
+  if (warp == 0) filter_line(TileCols<C, P>{sm + gl}, n32, a);
+  __syncthreads();
+  if (a.line_major) {
+    for (int qd = warp; qd * 4 < nl; qd += NW) {
+      const int l = qd * 4 + qs;
+      if (l >= nl) continue;
+      S* dst = out + bout[l];
+      const C* src = sm + l;
+      for (int i = qj; i < n32; i += 8) dst[i * a.out_st] = ppk::from_acc<S>(src[i * P]);
+    }
+  } else if (gl < nl) {
+    const bool vec = group_vec<S, V>(bout, out, a.out_st, gl, nl);
+    S* dst = out + bout[gl];
+    for (int i = warp; i < n32; i += NW) {
+      const C* src = sm + i * P + gl;
+      const int64_t off = i * a.out_st;
+      if (vec) {
+        if constexpr (kAsync) {
+          *reinterpret_cast<uint4*>(dst + off) = *reinterpret_cast<const uint4*>(src);
+        } else {
+          const float4 f = *reinterpret_cast<const float4*>(src);
+          S v[4] = {ppk::from_acc<S>(f.x), ppk::from_acc<S>(f.y), ppk::from_acc<S>(f.z), ppk::from_acc<S>(f.w)};
+          *reinterpret_cast<uint2*>(dst + off) = *reinterpret_cast<const uint2*>(v);
+        }
+      } else {
+        for (int k = 0; k < V && gl + k < nl; ++k) out[bout[gl + k] + off] = ppk::from_acc<S>(src[k]);
+      }
+    }
+  }
+}
+
+// Long-line kernel: LL threads, up to LL lines per CTA, one per thread, with
+// a runtime pitch (fewer lines for longer lines, up to 200 KB of shared
+// memory): odd when warps stage whole lines (conflict-free column writes),
+// else a multiple of G = 16 / sizeof(C) for the group copies.
+constexpr int LL = 64;
+
+template <class S>
+__global__ void __launch_bounds__(LL) coeff_smem_kernel(LineArgs a, int pitch, int lines) {
   using C = typename ppk::Acc<S>::type;
   constexpr int G = 16 / static_cast<int>(sizeof(C));
-  constexpr int GPR = NL / G;  // groups per sample row
+  constexpr int GPR = LL / G;  // groups per sample row
+  constexpr int NW = LL / 32;
   constexpr bool kAsync = sizeof(S) == sizeof(C);
-  static_assert(NL % 32 == 0 && NL % G == 0, "tile of whole warps and groups");
-  const int pitch = P ? P : pitch_rt;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
   const int64_t l0 = static_cast<int64_t>(blockIdx.x) * lines;
   const int nl = static_cast<int>(a.nlines - l0 < lines ? a.nlines - l0 : lines);
   const S* in = static_cast<const S*>(a.in);
   S* out = static_cast<S*>(a.out);
-  __shared__ int64_t bin[NL], bout[NL];
-  for (int l = threadIdx.x; l < nl; l += NL) line_base(a, l0 + l, bin[l], bout[l]);
+  __shared__ int64_t bin[LL], bout[LL];
+  for (int l = threadIdx.x; l < nl; l += LL) line_base(a, l0 + l, bin[l], bout[l]);
   __syncthreads();
   const int n32 = static_cast<int>(a.n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int nwarps = NL / 32;
-  // vector eligibility of the group at line l: G lines present, adjacent,
-  // every row aligned
-  auto group_vec = [&](const int64_t* base, const void* ptr, int64_t st, int l, int bytes) {
-    if (l + G > nl || (pitch % G) != 0) return false;
-    for (int k = 1; k < G; ++k)
-      if (base[l + k] != base[l] + k) return false;
-    const uintptr_t p = reinterpret_cast<uintptr_t>(ptr) + static_cast<uintptr_t>(base[l]) * sizeof(S);
-    return (p % bytes) == 0 && ((st * static_cast<int64_t>(sizeof(S))) % bytes) == 0;
-  };
+  const bool gvec_ok = (pitch % G) == 0;
   const int gl = (threadIdx.x % GPR) * G, r0 = threadIdx.x / GPR;  // strided: group line, first row
   if (a.line_major) {
-    for (int l = warp; l < nl; l += nwarps) {
+    for (int l = warp; l < nl; l += NW) {
       const S* src = in + bin[l];
       C* dst = sm + l;
-      if constexpr (kAsync) {
-        for (int i = lane; i < n32; i += 32) cp_async<sizeof(C)>(dst + i * pitch, src + i * a.in_st);
-      } else {
-        for (int i0 = 0; i0 < n32; i0 += 32 * UNROLL) {
-          C v[UNROLL];
-#pragma unroll
-          for (int u = 0; u < UNROLL; ++u) {
-            const int i = i0 + u * 32 + lane;
-            v[u] = i < n32 ? ppk::to_acc(src[i * a.in_st]) : C(0);
-          }
-#pragma unroll
-          for (int u = 0; u < UNROLL; ++u) {
-            const int i = i0 + u * 32 + lane;
-            if (i < n32) dst[i * pitch] = v[u];
-          }
-        }
+      for (int i = lane; i < n32; i += 32) {
+        if constexpr (kAsync) cp_async<sizeof(C)>(dst + i * pitch, src + i * a.in_st);
+        else dst[i * pitch] = ppk::to_acc(src[i * a.in_st]);
       }
     }
   } else if (gl < nl) {
-    const bool vec = group_vec(bin, in, a.in_st, gl, G * static_cast<int>(sizeof(S)));
+    const bool vec = gvec_ok && group_vec<S, G>(bin, in, a.in_st, gl, nl);
     const S* src = in + bin[gl];
     for (int i = r0; i < n32; i += G) {
       C* dst = sm + i * pitch + gl;
@@ -305,16 +519,16 @@ __global__ void __launch_bounds__(NL) coeff_smem_kernel(LineArgs a, int pitch_rt
   }
   if constexpr (kAsync) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
-  if (threadIdx.x < nl) filter_line(TileLine<C, P>{sm + threadIdx.x, pitch}, n32, a);
+  if (threadIdx.x < nl) filter_line(TileLine<C>{sm + threadIdx.x, pitch}, n32, a);
   __syncthreads();
   if (a.line_major) {
-    for (int l = warp; l < nl; l += nwarps) {
+    for (int l = warp; l < nl; l += NW) {
       S* dst = out + bout[l];
       const C* src = sm + l;
       for (int i = lane; i < n32; i += 32) dst[i * a.out_st] = ppk::from_acc<S>(src[i * pitch]);
     }
   } else if (gl < nl) {
-    const bool vec = group_vec(bout, out, a.out_st, gl, G * static_cast<int>(sizeof(S)));
+    const bool vec = gvec_ok && group_vec<S, G>(bout, out, a.out_st, gl, nl);
     S* dst = out + bout[gl];
     for (int i = r0; i < n32; i += G) {
       const C* src = sm + i * pitch + gl;
@@ -405,26 +619,36 @@ int copy_any(const pp_tensor* in, const pp_tensor* out, cudaStream_t st) {
   }
 }
 
-// Lines per CTA (= threads): small CTAs, several per SM.
-int tile_lines() {
-  static const int nl = [] {
-    const char* e = std::getenv("PP_COEFF_LINES");
-    const int v = e ? std::atoi(e) : 64;
-    return (v == 32 || v == 64 || v == 128) ? v : 64;
-  }();
-  return nl;
+template <class K>
+int allow_smem(K k, size_t smem, size_t static_bytes) {
+  // the 48 KB default covers static (line bases) plus dynamic shared memory
+  if (smem + static_bytes <= 48 * 1024) return PP_OK;
+  return ppc::cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                         "prefilter smem attribute");
 }
 
-template <class S, int NL>
-int run_tiles(LineArgs& a, cudaStream_t st) {
+template <class S>
+int run_axis(LineArgs& a, cudaStream_t st) {
   using C = typename ppk::Acc<S>::type;
   constexpr int G = 16 / static_cast<int>(sizeof(C));
-  // pitch: odd when warps stage whole lines (conflict-free column writes),
-  // else a multiple of the 16-byte group width; long lines take fewer lines
-  // per CTA, up to 200 KB of shared memory.
+  if (a.nlines == 0) return PP_OK;
   const size_t budget = 200 * 1024;
+  // full tiles: NT lines of the vectorised kernel
+  {
+    constexpr int NT = 32 * G, P = NT + G;
+    const size_t smem = static_cast<size_t>(a.n) * P * sizeof(C);
+    if (smem <= budget) {
+      auto k = coeff_tile_kernel<S>;
+      if (int rc = allow_smem(k, smem, 2 * NT * sizeof(int64_t))) return rc;
+      const int64_t blocks = (a.nlines + NT - 1) / NT;
+      k<<<static_cast<unsigned>(blocks), TILE_THREADS, smem, st>>>(a);
+      ppc::count_launch();
+      return ppc::cuda_check(cudaGetLastError(), "prefilter launch");
+    }
+  }
+  // longer lines: fewer per CTA, one per thread
   const int64_t fit = static_cast<int64_t>(budget / (static_cast<size_t>(a.n) * sizeof(C)));
-  int lines = static_cast<int>(fit < NL ? fit : NL), pitch = 0;
+  int lines = static_cast<int>(fit < LL ? fit : LL), pitch = 0;
   if (a.line_major) {
     pitch = lines | 1;
     if (static_cast<int64_t>(pitch) > fit) pitch = --lines;  // lines was even: drop one
@@ -434,16 +658,10 @@ int run_tiles(LineArgs& a, cudaStream_t st) {
   }
   if (lines >= 1) {
     const size_t smem = static_cast<size_t>(a.n) * pitch * sizeof(C);
-    const bool full = lines == NL && pitch == (a.line_major ? NL + 1 : NL);
-    auto k = !full ? coeff_smem_kernel<S, NL, 0>
-                   : (a.line_major ? coeff_smem_kernel<S, NL, NL + 1> : coeff_smem_kernel<S, NL, NL>);
-    // the 48 KB default covers static (line bases) plus dynamic shared memory
-    if (smem + 2 * NL * sizeof(int64_t) > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-      if (e != cudaSuccess) return ppc::cuda_check(e, "prefilter smem attribute");
-    }
+    auto k = coeff_smem_kernel<S>;
+    if (int rc = allow_smem(k, smem, 2 * LL * sizeof(int64_t))) return rc;
     const int64_t blocks = (a.nlines + lines - 1) / lines;
-    k<<<static_cast<unsigned>(blocks), NL, smem, st>>>(a, pitch, lines);
+    k<<<static_cast<unsigned>(blocks), LL, smem, st>>>(a, pitch, lines);
     ppc::count_launch();
   } else {
     if constexpr (sizeof(S) < 4) {
@@ -456,16 +674,6 @@ int run_tiles(LineArgs& a, cudaStream_t st) {
     }
   }
   return ppc::cuda_check(cudaGetLastError(), "prefilter launch");
-}
-
-template <class S>
-int run_axis(LineArgs& a, cudaStream_t st) {
-  if (a.nlines == 0) return PP_OK;
-  switch (tile_lines()) {
-    case 32: return run_tiles<S, 32>(a, st);
-    case 128: return run_tiles<S, 128>(a, st);
-    default: return run_tiles<S, 64>(a, st);
-  }
 }
 
 int coeff_axis(const pp_tensor* in, const pp_tensor* out, int bound, int order, int axis,

@@ -59,13 +59,14 @@ def test_coeff_axes_and_layouts(bound, shape):
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16])
-@pytest.mark.parametrize("n", [8, 9, 15, 16, 17, 24, 25, 96, 129, 192, 384])
+@pytest.mark.parametrize("n", [8, 9, 15, 16, 17, 24, 25, 96, 129, 192, 384, 388, 500])
 @pytest.mark.parametrize("bound", [2, 3, 6])
 def test_coeff_register_chunk_lengths(dtype, n, bound):
-    """Line lengths around the recursion's 8-sample register chunks and tiles
-    at the 48 KB default shared-memory limit (96 / 192 / 384 samples), along
+    """Line lengths around the recursions' register chunks, tiles at the 48 KB
+    default shared-memory limit (96 / 192 / 384 samples), either side of the
+    longest full tile (387 samples) and in the long-line kernel (500), along
     the fastest axis (warps stage whole lines) and a strided one (threads
-    stage groups of adjacent lines)."""
+    stage groups of adjacent lines), with full and partial last tiles."""
     r = np.random.default_rng(n + bound)
     tol = {torch.float64: 1e-11, torch.float32: 1e-5, torch.bfloat16: 1e-5}[dtype]
     for order in (3, 7):
