@@ -14,6 +14,7 @@
 // fall back to the same recursion directly on global memory.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "pp_capi_internal.cuh"
 
@@ -77,24 +78,40 @@ struct TileLine {  // one column of a shared tile, runtime pitch
   __device__ __forceinline__ void store(int i, const C (&x)[1]) const { p[i * pitch] = x[0]; }
 };
 
-template <class C, int P>
-struct TileCols {  // 16 / sizeof(C) adjacent columns of a shared tile, one 16-byte access
-  static constexpr int V = 16 / static_cast<int>(sizeof(C));
+template <class C, int P, int V_>
+struct TileCols {  // V_ adjacent columns of a shared tile (compile-time pitch), one access
+  static constexpr int V = V_;
   using value_type = C;
   using index_type = int;
   C* p;
   __device__ __forceinline__ void load(int i, C (&x)[V]) const {
-    if constexpr (V == 4) {
-      const float4 t = *reinterpret_cast<const float4*>(p + i * P);
+    const C* q = p + i * P;
+    if constexpr (V == 4 && sizeof(C) == 4) {
+      const float4 t = *reinterpret_cast<const float4*>(q);
       x[0] = t.x; x[1] = t.y; x[2] = t.z; x[3] = t.w;
-    } else {
-      const double2 t = *reinterpret_cast<const double2*>(p + i * P);
+    } else if constexpr (V == 2 && sizeof(C) == 4) {
+      const float2 t = *reinterpret_cast<const float2*>(q);
       x[0] = t.x; x[1] = t.y;
+    } else if constexpr (V == 2 && sizeof(C) == 8) {
+      const double2 t = *reinterpret_cast<const double2*>(q);
+      x[0] = t.x; x[1] = t.y;
+    } else {
+#pragma unroll
+      for (int c = 0; c < V; ++c) x[c] = q[c];
     }
   }
   __device__ __forceinline__ void store(int i, const C (&x)[V]) const {
-    if constexpr (V == 4) *reinterpret_cast<float4*>(p + i * P) = make_float4(x[0], x[1], x[2], x[3]);
-    else *reinterpret_cast<double2*>(p + i * P) = make_double2(x[0], x[1]);
+    C* q = p + i * P;
+    if constexpr (V == 4 && sizeof(C) == 4) {
+      *reinterpret_cast<float4*>(q) = make_float4(x[0], x[1], x[2], x[3]);
+    } else if constexpr (V == 2 && sizeof(C) == 4) {
+      *reinterpret_cast<float2*>(q) = make_float2(x[0], x[1]);
+    } else if constexpr (V == 2 && sizeof(C) == 8) {
+      *reinterpret_cast<double2*>(q) = make_double2(x[0], x[1]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < V; ++c) q[c] = x[c];
+    }
   }
 };
 
@@ -350,33 +367,33 @@ __device__ __forceinline__ bool group_vec(const int64_t* base, const void* ptr, 
   return (p % bytes) == 0 && ((st * static_cast<int64_t>(sizeof(S))) % bytes) == 0;
 }
 
-// Full-tile kernel (lines up to ~390 samples): NT = 32 * V lines per CTA,
-// V = 16 / sizeof(C) (128 lines for float arithmetic, 64 for double), held
-// element-major in shared memory: tile[i * P + l], P = NT + V (16-byte rows).
-// Four warps stage and store; warp 0 runs the recursions, each lane on V
-// adjacent lines read and written as one 16-byte vector (V independent
-// dependency chains, a quarter of the shared-memory instructions of one line
-// per thread).  Staging keeps warps on consecutive global addresses:
+// Full-tile kernel: NT lines per CTA (32, 64 or 128, sized to the line
+// length so that two CTAs or more fit an SM and one's transfers overlap the
+// other's recursions), held element-major in shared memory: tile[i * P + l],
+// P = NT + 4 (16-byte rows; 4 mod 32 words).  TILE_THREADS stage and store;
+// NT / V threads run the recursions, V adjacent lines each, read and written
+// as one access.  Staging keeps warps on consecutive global addresses:
 //  * filtered axis the fastest (line_major): a warp instruction covers 8
 //    consecutive samples of 4 lines (32-byte segments); with P = 4 mod 32
 //    words the 32 shared-memory writes fall in 32 distinct banks;
-//  * otherwise each lane a group of V adjacent lines on every 4th sample row,
-//    moved as one 16-byte copy (8-byte load for 16-bit storage) when the lines
-//    are adjacent and aligned in memory, else V scalar copies.
+//  * otherwise each thread a group of G = 16 / sizeof(C) adjacent lines on
+//    every few sample rows, moved as one 16-byte copy (8-byte load for 16-bit
+//    storage) when the lines are adjacent and aligned in memory, else G
+//    scalar copies.
 // float / double storage stage with asynchronous copies, the whole tile in
-// flight at once; 16-bit storage converts through registers.  Two CTAs fit
-// an SM for lines up to ~200 samples, so one's transfers overlap the other's
-// recursions.
-constexpr int TILE_THREADS = 128;
+// flight at once; 16-bit storage converts through registers.
+constexpr int TILE_THREADS = 256;
 
-template <class S>
-__global__ void __launch_bounds__(TILE_THREADS) coeff_tile_kernel(LineArgs a) {
+template <class S, int NT, int V>
+__global__ void __launch_bounds__(TILE_THREADS, 2) coeff_tile_kernel(LineArgs a) {
   using C = typename ppk::Acc<S>::type;
-  constexpr int V = 16 / static_cast<int>(sizeof(C));
-  constexpr int NT = 32 * V;
-  constexpr int P = NT + V;
+  constexpr int G = 16 / static_cast<int>(sizeof(C));
+  constexpr int P = NT + 4;
   constexpr int NW = TILE_THREADS / 32;
+  constexpr int GPR = NT / G;                 // strided: groups per sample row
+  constexpr int RS = TILE_THREADS / GPR;      // strided: rows per step
   constexpr bool kAsync = sizeof(S) == sizeof(C);
+  static_assert(NT % 32 == 0 && TILE_THREADS % GPR == 0 && NT / V <= TILE_THREADS, "tile shape");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
   const int64_t l0 = static_cast<int64_t>(blockIdx.x) * NT;
@@ -389,7 +406,7 @@ __global__ void __launch_bounds__(TILE_THREADS) coeff_tile_kernel(LineArgs a) {
   const int n32 = static_cast<int>(a.n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int qs = lane >> 3, qj = lane & 7;  // line_major: line in the quad, first sample
-  const int gl = lane * V;                   // strided: the lane's group of V lines
+  const int gl = (threadIdx.x % GPR) * G, r0 = threadIdx.x / GPR;  // strided: group, first row
   if (a.line_major) {
     for (int qd = warp; qd * 4 < nl; qd += NW) {
       const int l = qd * 4 + qs;
@@ -415,16 +432,16 @@ __global__ void __launch_bounds__(TILE_THREADS) coeff_tile_kernel(LineArgs a) {
       }
     }
   } else if (gl < nl) {
-    const bool vec = group_vec<S, V>(bin, in, a.in_st, gl, nl);
+    const bool vec = group_vec<S, G>(bin, in, a.in_st, gl, nl);
     const S* src = in + bin[gl];
-    for (int i = warp; i < n32; i += NW) {
+    for (int i = r0; i < n32; i += RS) {
       C* dst = sm + i * P + gl;
       const int64_t off = i * a.in_st;
       if (vec) {
         if constexpr (kAsync) cp_async<16>(dst, src + off);
         else load_group(dst, src + off);
       } else {
-        for (int k = 0; k < V && gl + k < nl; ++k) {
+        for (int k = 0; k < G && gl + k < nl; ++k) {
           if constexpr (kAsync) cp_async<sizeof(C)>(dst + k, in + bin[gl + k] + off);
           else dst[k] = ppk::to_acc(in[bin[gl + k] + off]);
         }
@@ -434,7 +451,7 @@ __global__ void __launch_bounds__(TILE_THREADS) coeff_tile_kernel(LineArgs a) {
   if constexpr (kAsync) asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   // columns past nl (last tile) hold stale shared memory: filtered, never stored
-  if (warp == 0) filter_line(TileCols<C, P>{sm + gl}, n32, a);
+  if (threadIdx.x * V < nl) filter_line(TileCols<C, P, V>{sm + threadIdx.x * V}, n32, a);
   __syncthreads();
   if (a.line_major) {
     for (int qd = warp; qd * 4 < nl; qd += NW) {
@@ -445,9 +462,9 @@ __global__ void __launch_bounds__(TILE_THREADS) coeff_tile_kernel(LineArgs a) {
       for (int i = qj; i < n32; i += 8) dst[i * a.out_st] = ppk::from_acc<S>(src[i * P]);
     }
   } else if (gl < nl) {
-    const bool vec = group_vec<S, V>(bout, out, a.out_st, gl, nl);
+    const bool vec = group_vec<S, G>(bout, out, a.out_st, gl, nl);
     S* dst = out + bout[gl];
-    for (int i = warp; i < n32; i += NW) {
+    for (int i = r0; i < n32; i += RS) {
       const C* src = sm + i * P + gl;
       const int64_t off = i * a.out_st;
       if (vec) {
@@ -459,7 +476,7 @@ __global__ void __launch_bounds__(TILE_THREADS) coeff_tile_kernel(LineArgs a) {
           *reinterpret_cast<uint2*>(dst + off) = *reinterpret_cast<const uint2*>(v);
         }
       } else {
-        for (int k = 0; k < V && gl + k < nl; ++k) out[bout[gl + k] + off] = ppk::from_acc<S>(src[k]);
+        for (int k = 0; k < G && gl + k < nl; ++k) out[bout[gl + k] + off] = ppk::from_acc<S>(src[k]);
       }
     }
   }
@@ -627,23 +644,66 @@ int allow_smem(K k, size_t smem, size_t static_bytes) {
                          "prefilter smem attribute");
 }
 
+int tile_v() {  // lines per recursion thread in full tiles
+  static const int v = [] {
+    const char* e = std::getenv("PP_COEFF_V");
+    const int x = e ? std::atoi(e) : 1;
+    return (x == 1 || x == 2 || x == 4) ? x : 1;
+  }();
+  return v;
+}
+
+int tile_cap() {  // widest full tile
+  static const int v = [] {
+    const char* e = std::getenv("PP_COEFF_NT");
+    return e ? std::atoi(e) : 128;
+  }();
+  return v;
+}
+
+template <class S, int NT, int V>
+int launch_tile(const LineArgs& a, size_t smem, cudaStream_t st) {
+  auto k = coeff_tile_kernel<S, NT, V>;
+  if (int rc = allow_smem(k, smem, 2 * NT * sizeof(int64_t))) return rc;
+  const int64_t blocks = (a.nlines + NT - 1) / NT;
+  k<<<static_cast<unsigned>(blocks), TILE_THREADS, smem, st>>>(a);
+  ppc::count_launch();
+  return ppc::cuda_check(cudaGetLastError(), "prefilter launch");
+}
+
+template <class S, int NT>
+int launch_tile_v(const LineArgs& a, size_t smem, cudaStream_t st) {
+  using C = typename ppk::Acc<S>::type;
+  const int v = tile_v();
+  if (v == 4 && sizeof(C) == 4) return launch_tile<S, NT, 4>(a, smem, st);
+  if (v >= 2) return launch_tile<S, NT, 2>(a, smem, st);
+  return launch_tile<S, NT, 1>(a, smem, st);
+}
+
+template <class S>
+int launch_tiles(const LineArgs& a, int NT, size_t smem, cudaStream_t st) {
+  switch (NT) {
+    case 128: return launch_tile_v<S, 128>(a, smem, st);
+    case 64: return launch_tile_v<S, 64>(a, smem, st);
+    default: return launch_tile_v<S, 32>(a, smem, st);
+  }
+}
+
 template <class S>
 int run_axis(LineArgs& a, cudaStream_t st) {
   using C = typename ppk::Acc<S>::type;
   constexpr int G = 16 / static_cast<int>(sizeof(C));
   if (a.nlines == 0) return PP_OK;
   const size_t budget = 200 * 1024;
-  // full tiles: NT lines of the vectorised kernel
+  // full tiles: the widest NT (multiple of 32, at most 128) whose tile
+  // leaves room for two CTAs per SM
   {
-    constexpr int NT = 32 * G, P = NT + G;
-    const size_t smem = static_cast<size_t>(a.n) * P * sizeof(C);
-    if (smem <= budget) {
-      auto k = coeff_tile_kernel<S>;
-      if (int rc = allow_smem(k, smem, 2 * NT * sizeof(int64_t))) return rc;
-      const int64_t blocks = (a.nlines + NT - 1) / NT;
-      k<<<static_cast<unsigned>(blocks), TILE_THREADS, smem, st>>>(a);
-      ppc::count_launch();
-      return ppc::cuda_check(cudaGetLastError(), "prefilter launch");
+    const int64_t fit = static_cast<int64_t>(113 * 1024 / (static_cast<size_t>(a.n) * sizeof(C))) - 4;
+    const int cap = tile_cap();
+    const int NT = (fit >= 128 && cap >= 128) ? 128 : (fit >= 64 && cap >= 64) ? 64 : fit >= 32 ? 32 : 0;
+    if (NT > 0) {
+      const size_t smem = static_cast<size_t>(a.n) * (NT + 4) * sizeof(C);
+      return launch_tiles<S>(a, NT, smem, st);
     }
   }
   // longer lines: fewer per CTA, one per thread
