@@ -367,8 +367,8 @@ __device__ __forceinline__ bool group_vec(const int64_t* base, const void* ptr, 
   return (p % bytes) == 0 && ((st * static_cast<int64_t>(sizeof(S))) % bytes) == 0;
 }
 
-// Full-tile kernel: NT lines per CTA (32, 64 or 128, sized to the line
-// length so that two CTAs or more fit an SM and one's transfers overlap the
+// Full-tile kernel: NT lines per CTA (32, 64, 96 or 128: the widest that
+// leaves room for two CTAs per SM and one's transfers overlap the
 // other's recursions), held element-major in shared memory: tile[i * P + l],
 // P = NT + 4 (16-byte rows; 4 mod 32 words).  TILE_THREADS stage and store;
 // NT / V threads run the recursions, V adjacent lines each, read and written
@@ -391,9 +391,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) coeff_tile_kernel(LineArgs a)
   constexpr int P = NT + 4;
   constexpr int NW = TILE_THREADS / 32;
   constexpr int GPR = NT / G;                 // strided: groups per sample row
-  constexpr int RS = TILE_THREADS / GPR;      // strided: rows per step
+  constexpr int RS = TILE_THREADS / GPR;      // strided: rows per step (threads past RS * GPR idle)
   constexpr bool kAsync = sizeof(S) == sizeof(C);
-  static_assert(NT % 32 == 0 && TILE_THREADS % GPR == 0 && NT / V <= TILE_THREADS, "tile shape");
+  static_assert(NT % 32 == 0 && NT % G == 0 && RS >= 1 && NT / V <= TILE_THREADS, "tile shape");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
   const int64_t l0 = static_cast<int64_t>(blockIdx.x) * NT;
@@ -406,7 +406,8 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) coeff_tile_kernel(LineArgs a)
   const int n32 = static_cast<int>(a.n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int qs = lane >> 3, qj = lane & 7;  // line_major: line in the quad, first sample
-  const int gl = (threadIdx.x % GPR) * G, r0 = threadIdx.x / GPR;  // strided: group, first row
+  const int gl = threadIdx.x < RS * GPR ? (threadIdx.x % GPR) * G : NT;  // strided: group (NT: idle)
+  const int r0 = threadIdx.x / GPR;                                       // strided: first row
   if (a.line_major) {
     for (int qd = warp; qd * 4 < nl; qd += NW) {
       const int l = qd * 4 + qs;
@@ -647,7 +648,7 @@ int allow_smem(K k, size_t smem, size_t static_bytes) {
 int tile_v() {  // lines per recursion thread in full tiles
   static const int v = [] {
     const char* e = std::getenv("PP_COEFF_V");
-    const int x = e ? std::atoi(e) : 1;
+    const int x = e ? std::atoi(e) : 2;
     return (x == 1 || x == 2 || x == 4) ? x : 1;
   }();
   return v;
@@ -684,6 +685,7 @@ template <class S>
 int launch_tiles(const LineArgs& a, int NT, size_t smem, cudaStream_t st) {
   switch (NT) {
     case 128: return launch_tile_v<S, 128>(a, smem, st);
+    case 96: return launch_tile_v<S, 96>(a, smem, st);
     case 64: return launch_tile_v<S, 64>(a, smem, st);
     default: return launch_tile_v<S, 32>(a, smem, st);
   }
@@ -700,7 +702,8 @@ int run_axis(LineArgs& a, cudaStream_t st) {
   {
     const int64_t fit = static_cast<int64_t>(113 * 1024 / (static_cast<size_t>(a.n) * sizeof(C))) - 4;
     const int cap = tile_cap();
-    const int NT = (fit >= 128 && cap >= 128) ? 128 : (fit >= 64 && cap >= 64) ? 64 : fit >= 32 ? 32 : 0;
+    const int NT = (fit >= 128 && cap >= 128) ? 128 : (fit >= 96 && cap >= 96) ? 96
+                 : (fit >= 64 && cap >= 64) ? 64 : fit >= 32 ? 32 : 0;
     if (NT > 0) {
       const size_t smem = static_cast<size_t>(a.n) * (NT + 4) * sizeof(C);
       return launch_tiles<S>(a, NT, smem, st);

@@ -59,7 +59,7 @@ def test_coeff_axes_and_layouts(bound, shape):
 
 
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16])
-@pytest.mark.parametrize("n", [8, 9, 15, 16, 17, 24, 25, 96, 129, 192, 384, 388, 500])
+@pytest.mark.parametrize("n", [8, 9, 15, 16, 17, 24, 25, 96, 129, 192, 256, 384, 388, 500])
 @pytest.mark.parametrize("bound", [2, 3, 6])
 def test_coeff_register_chunk_lengths(dtype, n, bound):
     """Line lengths around the recursions' register chunks, tiles at the 48 KB
