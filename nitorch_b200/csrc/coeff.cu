@@ -5,16 +5,19 @@
 // causal and one anti-causal first-order recursion per pole (coeff.py:
 // 254-281), initial / final conditions per boundary (coeff.py:69-251).
 //
-// B200 mapping: one line per thread, LINES lines per CTA staged in shared
-// memory through a cooperative, coalesced load (whichever axis is filtered),
-// so that the sequential recursions run out of shared memory and the global
-// traffic is one read and one write of the volume per axis.  The recursions
-// run in float (double for double storage); the initial / final condition
-// sums are evaluated in double.  Lines longer than the shared-memory budget
-// fall back to the same recursion directly on global memory.
+// B200 mapping: one line per thread, a tile of lines per CTA staged in
+// shared memory (element-major: warps of recursing threads read one sample of
+// 32 adjacent lines per access) by asynchronous copies issued for the whole
+// tile at once, 16 bytes at a time across adjacent lines when the filtered
+// axis is strided.  The sequential recursions run out of shared memory and
+// the global traffic is one read and one write of the volume per axis.  Tile
+// widths are chosen per line length so that two CTAs share an SM, one's
+// transfers overlapping the other's recursions.  The recursions run in float
+// (double for double storage); the initial / final condition sums in double
+// with per-pole constants computed on the host.  Lines too long for a shared
+// tile fall back to the same recursion directly on global memory.
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 
 #include "pp_capi_internal.cuh"
 
@@ -383,6 +386,10 @@ __device__ __forceinline__ bool group_vec(const int64_t* base, const void* ptr, 
 // float / double storage stage with asynchronous copies, the whole tile in
 // flight at once; 16-bit storage converts through registers.
 constexpr int TILE_THREADS = 256;
+// lines per recursion thread: 1, 2 and 4 (one 4-, 8- or 16-byte access per
+// sample) measured within noise of each other on 3 x 192^3 and 3 x 256^3
+// float volumes; one line per thread keeps the most warps in the recursions
+constexpr int TILE_V = 1;
 
 template <class S, int NT, int V>
 __global__ void __launch_bounds__(TILE_THREADS, 2) coeff_tile_kernel(LineArgs a) {
@@ -645,23 +652,6 @@ int allow_smem(K k, size_t smem, size_t static_bytes) {
                          "prefilter smem attribute");
 }
 
-int tile_v() {  // lines per recursion thread in full tiles
-  static const int v = [] {
-    const char* e = std::getenv("PP_COEFF_V");
-    const int x = e ? std::atoi(e) : 2;
-    return (x == 1 || x == 2 || x == 4) ? x : 1;
-  }();
-  return v;
-}
-
-int tile_cap() {  // widest full tile
-  static const int v = [] {
-    const char* e = std::getenv("PP_COEFF_NT");
-    return e ? std::atoi(e) : 128;
-  }();
-  return v;
-}
-
 template <class S, int NT, int V>
 int launch_tile(const LineArgs& a, size_t smem, cudaStream_t st) {
   auto k = coeff_tile_kernel<S, NT, V>;
@@ -672,22 +662,13 @@ int launch_tile(const LineArgs& a, size_t smem, cudaStream_t st) {
   return ppc::cuda_check(cudaGetLastError(), "prefilter launch");
 }
 
-template <class S, int NT>
-int launch_tile_v(const LineArgs& a, size_t smem, cudaStream_t st) {
-  using C = typename ppk::Acc<S>::type;
-  const int v = tile_v();
-  if (v == 4 && sizeof(C) == 4) return launch_tile<S, NT, 4>(a, smem, st);
-  if (v >= 2) return launch_tile<S, NT, 2>(a, smem, st);
-  return launch_tile<S, NT, 1>(a, smem, st);
-}
-
 template <class S>
 int launch_tiles(const LineArgs& a, int NT, size_t smem, cudaStream_t st) {
   switch (NT) {
-    case 128: return launch_tile_v<S, 128>(a, smem, st);
-    case 96: return launch_tile_v<S, 96>(a, smem, st);
-    case 64: return launch_tile_v<S, 64>(a, smem, st);
-    default: return launch_tile_v<S, 32>(a, smem, st);
+    case 128: return launch_tile<S, 128, TILE_V>(a, smem, st);
+    case 96: return launch_tile<S, 96, TILE_V>(a, smem, st);
+    case 64: return launch_tile<S, 64, TILE_V>(a, smem, st);
+    default: return launch_tile<S, 32, TILE_V>(a, smem, st);
   }
 }
 
@@ -701,9 +682,7 @@ int run_axis(LineArgs& a, cudaStream_t st) {
   // leaves room for two CTAs per SM
   {
     const int64_t fit = static_cast<int64_t>(113 * 1024 / (static_cast<size_t>(a.n) * sizeof(C))) - 4;
-    const int cap = tile_cap();
-    const int NT = (fit >= 128 && cap >= 128) ? 128 : (fit >= 96 && cap >= 96) ? 96
-                 : (fit >= 64 && cap >= 64) ? 64 : fit >= 32 ? 32 : 0;
+    const int NT = fit >= 128 ? 128 : fit >= 96 ? 96 : fit >= 64 ? 64 : fit >= 32 ? 32 : 0;
     if (NT > 0) {
       const size_t smem = static_cast<size_t>(a.n) * (NT + 4) * sizeof(C);
       return launch_tiles<S>(a, NT, smem, st);
