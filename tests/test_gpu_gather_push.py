@@ -14,7 +14,7 @@ import pytest
 import torch
 
 import nitorch_b200 as nb
-from nitorch_b200 import spatial
+from nitorch_b200 import _lib, spatial
 from nitorch_b200.enums import BoundType, InterpolationType
 from oracle import oracle as O
 from tests._gpu_ops import relerr
@@ -101,21 +101,22 @@ def test_gather_push_collapsed_grid(order):
     assert relerr(y.double().cpu().numpy(), ref) < 1e-5
 
 
-def test_gather_push_options_carry_cells():
-    """With the gather push on, the call options carry the sorted order and
-    its cell offsets (N * prod(source) + 1 of them, ending at the number of
-    points); off, only the order."""
+def test_gather_push_runs_gather_kernel():
+    """With the cell offsets cached, a gather push is two launches (gather,
+    residual scatter); the scatter-only push is one."""
     x, grid = data(1, 3, (16, 16, 16), (16, 16, 16), seed=7)
-    G = torch.from_numpy(grid).float().cuda()
+    X, G = torch.from_numpy(x).float().cuda(), torch.from_numpy(grid).float().cuda()
+    L = _lib.load()
     with path(True):
-        o = spatial._opts([BoundType(2)], [InterpolationType(3)], 1, G, (16, 16, 16))
-        assert o.sample_order and o.sample_cells
-        perm, cells = o._keep
-        assert cells.numel() == 16 ** 3 + 1 and int(cells[-1]) == perm.numel() == 16 ** 3
-        assert bool((cells[1:] >= cells[:-1]).all())
+        push(X, G, (16, 16, 16), 2, 3, 1)  # computes and caches the order
+        n0 = L.pp_kernel_launches()
+        push(X, G, (16, 16, 16), 2, 3, 1)
+        n1 = L.pp_kernel_launches()
     with path(False):
-        o = spatial._opts([BoundType(2)], [InterpolationType(3)], 1, G, (16, 16, 16))
-        assert o.sample_order and not o.sample_cells
+        push(X, G, (16, 16, 16), 2, 3, 1)
+        n2 = L.pp_kernel_launches()
+    assert n1 - n0 == 2
+    assert n2 - n1 == 1
 
 
 def test_gather_push_large_identity_like():
