@@ -93,18 +93,6 @@ typedef struct pp_options {
                                     from pp_sample_order); NULL = natural.
                                     Results do not depend on it beyond
                                     floating-point summation order.        */
-  const int32_t* sample_cells;   /* optional device array that goes with a
-                                    sorted sample_order: the sorted position
-                                    of the first point of every source cell,
-                                    N*prod(source spatial) + 1 entries (from
-                                    pp_sample_order_cells).  With it, 3-D
-                                    pushes of orders 1 and 3 into float32
-                                    outputs run in gather form (each output
-                                    voxel sums the points of its cells; the
-                                    points near the faces or outside are
-                                    scattered) instead of as atomics.  The
-                                    source is the pushed-to volume.  NULL =
-                                    scatter only.                          */
 } pp_options;
 
 /* Version of this ABI (major * 100 + minor). */
@@ -262,14 +250,6 @@ PP_API int pp_jacobian_det(const pp_tensor* jac, const pp_tensor* det, const pp_
 PP_API size_t pp_sample_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size);
 PP_API int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
                            void* workspace, size_t workspace_bytes, void* stream);
-
-/* pp_sample_order that also returns the sort's per-cell offsets: cells
- * (N*prod(src_size) + 1 int32) receives the position in `perm` of the first
- * sampling point of every source cell (batch item, then source voxel, last
- * axis fastest), and cells[N*prod(src_size)] = the number of points.  Same
- * workspace as pp_sample_order.  No counterpart in the reference. */
-PP_API int pp_sample_order_cells(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
-                                 int32_t* cells, void* workspace, size_t workspace_bytes, void* stream);
 
 /* pp_sample_order without any device allocation or caller workspace (no
  * counterpart in the reference).  For callers that cannot allocate device

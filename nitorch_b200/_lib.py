@@ -52,7 +52,6 @@ class PPOptions(ctypes.Structure):
         ("extrapolate", ctypes.c_int32),
         ("flags", ctypes.c_int32),
         ("sample_order", ctypes.c_void_p),
-        ("sample_cells", ctypes.c_void_p),
     ]
 
 
@@ -69,7 +68,7 @@ EXPORTS = (
     "pp_grid_push_backward", "pp_grid_count", "pp_grid_count_backward",
     "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
     "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
-    "pp_sample_order_noalloc", "pp_sample_order_cells", "pp_grid_pull_push", "pp_grid_pull_push_backward",
+    "pp_sample_order_noalloc", "pp_grid_pull_push", "pp_grid_pull_push_backward",
     "pp_batch_plan_bytes", "pp_batch_scratch_bytes", "pp_batch_plan", "pp_batch_run",
     "pp_svf_compose", "pp_svf_compose_backward", "pp_affine_pull", "pp_affine_push",
     "pp_affine_grad_workspace_bytes", "pp_affine_grad_matrix",
@@ -129,7 +128,6 @@ def _declare(L):
     L.pp_sample_order_workspace_bytes.restype = sz
     L.pp_sample_order.argtypes = [T, I64P, vp, vp, sz, vp]
     L.pp_sample_order_noalloc.argtypes = [T, I64P, vp, vp]
-    L.pp_sample_order_cells.argtypes = [T, I64P, vp, vp, vp, sz, vp]
     for name in EXPORTS:
         if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches",
                         "pp_sample_order_workspace_bytes", "pp_batch_plan_bytes", "pp_batch_scratch_bytes",
@@ -186,10 +184,9 @@ def ref(d):
     return None if d is None else ctypes.byref(d)
 
 
-def options(bound, order, extrapolate, flags=0, sample_order=None, sample_cells=None):
+def options(bound, order, extrapolate, flags=0, sample_order=None):
     o = PPOptions()
     o.sample_order = sample_order
-    o.sample_cells = sample_cells if sample_order else None
     b = [int(x) for x in bound][:3]
     i = [int(x) for x in order][:3]
     o.nbound = len(b)

@@ -200,15 +200,8 @@ size_t pp_sample_order_workspace_bytes(const pp_tensor* grid, const int64_t* src
   return layout(nvox, nsrc * grid->sizes[0]).total;
 }
 
-}  // extern "C"
-
-namespace {
-
-__global__ void set_cells_end(int32_t* cells, int64_t nsrc_total, int32_t nvox) { cells[nsrc_total] = nvox; }
-
-// The counting sort; with `cells`, the per-key offsets are kept there.
-int sample_order_impl(const pp_tensor* grid, const int64_t* src_size, int32_t* perm, int32_t* cells,
-                      void* workspace, size_t workspace_bytes, void* stream) {
+int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
+                    void* workspace, size_t workspace_bytes, void* stream) {
   int D;
   int64_t nvox, nsrc;
   int rc = sizes_of(grid, src_size, D, nvox, nsrc);
@@ -218,13 +211,10 @@ int sample_order_impl(const pp_tensor* grid, const int64_t* src_size, int32_t* p
   const Layout L = layout(nvox, nsrc_total);
   if (!workspace || workspace_bytes < L.total)
     return ppc::fail(PP_ERR_WORKSPACE, "(): sample ordering needs %zu bytes of workspace", L.total);
-  if (nvox == 0)
-    return cells ? ppc::cuda_check(cudaMemsetAsync(cells, 0, static_cast<size_t>(nsrc_total + 1) * 4,
-                                                   static_cast<cudaStream_t>(stream)), "order clear")
-                 : PP_OK;
+  if (nvox == 0) return PP_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   unsigned char* ws = static_cast<unsigned char*>(workspace);
-  int32_t* count = cells ? cells : reinterpret_cast<int32_t*>(ws + L.count);
+  int32_t* count = reinterpret_cast<int32_t*>(ws + L.count);
   int32_t* keys = reinterpret_cast<int32_t*>(ws + L.keys);
   int32_t* ranks = reinterpret_cast<int32_t*>(ws + L.ranks);
   int32_t* partial = reinterpret_cast<int32_t*>(ws + L.partial);
@@ -251,26 +241,7 @@ int sample_order_impl(const pp_tensor* grid, const int64_t* src_size, int32_t* p
   scan_apply<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, nsrc_total, partial);
   order_scatter<<<nb, 256, 0, st>>>(keys, ranks, count, nvox, perm);
   ppc::count_launch(5);
-  if (cells) {
-    set_cells_end<<<1, 1, 0, st>>>(cells, nsrc_total, static_cast<int32_t>(nvox));
-    ppc::count_launch();
-  }
   return ppc::cuda_check(cudaGetLastError(), "sample order launch");
-}
-
-}  // namespace
-
-extern "C" {
-
-int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
-                    void* workspace, size_t workspace_bytes, void* stream) {
-  return sample_order_impl(grid, src_size, perm, nullptr, workspace, workspace_bytes, stream);
-}
-
-int pp_sample_order_cells(const pp_tensor* grid, const int64_t* src_size, int32_t* perm, int32_t* cells,
-                          void* workspace, size_t workspace_bytes, void* stream) {
-  if (!cells) return ppc::fail(PP_ERR_ARG, "(): expected an output cell-offset array");
-  return sample_order_impl(grid, src_size, perm, cells, workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

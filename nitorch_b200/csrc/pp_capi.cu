@@ -54,8 +54,6 @@ bool lanes_enabled() {
   }();
   return on;
 }
-// gather_push.cu
-int gather_push(const PPArgs& a, int order, int trgt_dtype, const int32_t* cells, cudaStream_t st);
 }  // namespace ppk
 
 
@@ -162,7 +160,6 @@ namespace {
 // Core dispatcher shared by the entry points.
 struct Call {
   int D = 0;
-  const int32_t* cells = nullptr;  // per-cell offsets of a sorted sample order (gather push)
   int bound[3] = {0, 0, 0}, order[3] = {1, 1, 1};
   int dtype = PP_FLOAT32;  // image storage dtype
   ppk::PPArgs a;
@@ -177,7 +174,6 @@ int prepare(Call& k, const pp_tensor* grid, const pp_options* opt) {
   for (int a = 0; a < 3; ++a) { k.a.bound[a] = k.bound[a]; k.a.order[a] = k.order[a]; }
   k.a.extrapolate = opt->extrapolate;
   k.a.perm = opt->sample_order;
-  k.cells = opt->sample_order ? opt->sample_cells : nullptr;
   k.a.grid = grid->data;
   set_grid(grid, k.D, k.a.grid_sN, k.a.grid_s, k.a.grid_sD);
   k.a.N = grid->sizes[0];
@@ -332,7 +328,7 @@ int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const u
 
 extern "C" {
 
-int pp_abi_version(void) { return 101; }
+int pp_abi_version(void) { return 100; }
 
 const char* pp_last_error(void) { return g_err.c_str(); }
 
@@ -429,23 +425,6 @@ static int scatter_into(Call& k, int mode, const pp_tensor* out, const pp_tensor
     for (int a = 0; a < 3; ++a) k.a.out_s[a] = a < k.D ? cs[2 + a] : 0;
     if ((rc = run(k, mode, wide, st))) return rc;
     return det_finalize_to(acc, out, mx, k.a.det_bound, st);
-  }
-  // Gather-form push (gather_push.cu): 3-D, orders 1 / 3, float32 output
-  // (float32 / bfloat16 values, so a float32 grid), the sorted order with its
-  // cell offsets, plain grids.  The
-  // interior points are summed per output voxel (every voxel written), the
-  // rest scattered on top with F_RESID in the grid's own order.
-  const int iso_g = iso_order(k.D, k.order);
-  if (mode == ppk::K_PUSH && k.cells && k.D == 3 && (iso_g == 1 || iso_g == 3) && out->dtype == PP_FLOAT32 &&
-      (k.dtype == PP_FLOAT32 || k.dtype == PP_BFLOAT16) && !wide && !det &&
-      !(k.a.flags & (ppk::F_IDGRID | ppk::F_AFFINE | ppk::F_ADDSELF | ppk::F_VEC)) && out->sizes[0] == k.a.N &&
-      k.a.trgt_sN != 0) {
-    k.a.out = out->data;
-    set_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
-    if ((rc = ppk::gather_push(k.a, iso_g, k.dtype, k.cells, st))) return rc;
-    k.a.perm = nullptr;
-    k.a.flags |= ppk::F_RESID;
-    return run(k, mode, wide, st);
   }
   // Vectorised scatter: 3-D, 2-4 channels, orders >= 2 with a compile-time
   // kernel (float32: all, bfloat16: cubic), 32-bit offsets, not

@@ -190,17 +190,6 @@ __device__ __forceinline__ I support_low(int order, T x) {
   }
 }
 
-// Interior point along one axis: all taps inside [0, n), so no boundary
-// condition applies.  The gather-form push takes these points and the
-// residual scatter the others; both decide with this one function on the
-// same coordinate values (clamped as in build_axis).
-template <class I, class T>
-__device__ __forceinline__ bool interior_axis(int order, T x, I n) {
-  x = fmin(fmax(x, T(-1073741824.0)), T(1073741824.0));
-  const I low = support_low<I, T>(order, x);
-  return low >= 0 && low + (order == 0 ? 0 : order) < n;
-}
-
 // Out-of-bound test of the compiled backend: inside [-tol, n-1+tol) with
 // tol = 0.05 (or 0.55 with the half-voxel flag), in the grid's precision.
 // nitorch/_C/src/impl/bounds_common.h:168-171, pushpull_common.cpp:58,895-918.

@@ -38,8 +38,7 @@ namespace ppk {
 
 enum Mode : int { K_PULL = 0, K_SGRAD, K_PUSH, K_COUNT, K_PULLGRAD, K_PUSHGRAD, K_KD,
                   K_PP, K_PP_BWD, K_NMODES };
-enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4, F_VEC = 8, F_IDGRID = 16, F_ADDSELF = 32, F_AFFINE = 64,
-                  F_RESID = 128 };
+enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4, F_VEC = 8, F_IDGRID = 16, F_ADDSELF = 32, F_AFFINE = 64 };
 // F_A: pull (PULLGRAD) / push (PUSHGRAD, KD)
 // F_VEC: `out` is a channel-interleaved float accumulator (pp_lanes_kernel)
 // F_IDGRID: the sampling coordinate is the point's own voxel plus the grid
@@ -51,8 +50,6 @@ enum Flag : int { F_A = 1, F_GRAD = 2, F_NOTRGT = 4, F_VEC = 8, F_IDGRID = 16, F
 // F_AFFINE: no grid tensor: the coordinate of grid point `sub` is
 //   A [sub; 1], A the D x (D+1) row-major matrix of batch item n at
 //   grid + n * grid_sN (resize / reslice without a materialised grid)
-// F_RESID (K_PUSH, 3-D): skip the interior points (interior_axis along
-//   every axis), whose contributions the gather-form push has written
 
 struct PPArgs {
   const void* src;   // gathered tensor (N, C, *src_size)
@@ -210,15 +207,6 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
   if (a.flags & F_IDGRID) {
 #pragma unroll
     for (int d = 0; d < D; ++d) coord[d] += static_cast<T>(sub[d]);
-  }
-  if constexpr (MODE == K_PUSH && D == 3) {
-    if (a.flags & F_RESID) {
-      bool inner = true;
-#pragma unroll
-      for (int d = 0; d < D; ++d)
-        inner = inner && interior_axis<I, T>(ORD >= 0 ? ORD : a.order[d], coord[d], static_cast<I>(a.src_size[d]));
-      if (inner) return;
-    }
   }
 
   const bool do_a = (a.flags & F_A) != 0;
@@ -1006,12 +994,6 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_lanes_k
     for (int d = 0; d < 3; ++d) gp += static_cast<int64_t>(sub[d]) * a.grid_s[d];
 #pragma unroll
     for (int d = 0; d < 3; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
-  }
-  if constexpr (MODE == K_PUSH) {
-    if ((a.flags & F_RESID) && interior_axis<I, T>(ORD, coord[0], static_cast<I>(a.src_size[0])) &&
-        interior_axis<I, T>(ORD, coord[1], static_cast<I>(a.src_size[1])) &&
-        interior_axis<I, T>(ORD, coord[2], static_cast<I>(a.src_size[2])))
-      return;
   }
   {
     const T tol = (a.extrapolate & 2) ? static_cast<T>(0.5 + 5e-2) : static_cast<T>(5e-2);

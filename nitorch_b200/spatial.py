@@ -27,7 +27,6 @@ Argument errors raise ``RuntimeError`` with the reference's "(): expected
     second axis' order for the third, ``pushpull_common.cpp:591``).
 """
 import ctypes
-import math
 import os
 import threading
 import weakref
@@ -40,13 +39,12 @@ from .enums import BoundType, InterpolationType
 __all__ = ["grid_pull", "grid_pull_backward", "grid_push", "grid_push_backward",
            "grid_count", "grid_count_backward", "grid_grad", "grid_grad_backward",
            "BoundType", "InterpolationType", "set_deterministic", "get_deterministic",
-           "set_sample_order", "sample_order", "set_gather_push", "grid_pull_push", "grid_pull_push_backward"]
+           "set_sample_order", "sample_order", "grid_pull_push", "grid_pull_push_backward"]
 
 _FLOATS = (torch.float32, torch.float64, torch.bfloat16, torch.float16)
 _deterministic = bool(int(os.environ.get("PP_DETERMINISTIC", "0") or "0"))
 _sample_order_mode = os.environ.get("PP_SAMPLE_ORDER", "auto")
 _SORT_MIN_SAMPLES = 1 << 18
-_gather_push = os.environ.get("PP_GATHER_PUSH", "1") != "0"
 
 
 def set_sample_order(mode="auto"):
@@ -78,17 +76,17 @@ class _OrderCache:
     def get(self, grid, src):
         key = self._key(grid, src)
         with self.lock:
-            for i, (ref, k, order) in enumerate(self.entries):
+            for i, (ref, k, perm) in enumerate(self.entries):
                 if ref() is not None and k == key:
                     if i:
                         self.entries.insert(0, self.entries.pop(i))
-                    return order
+                    return perm
         return None
 
-    def put(self, grid, src, order):
+    def put(self, grid, src, perm):
         with self.lock:
             self.entries = [e for e in self.entries if e[0]() is not None][: self.size - 1]
-            self.entries.insert(0, (weakref.ref(grid), self._key(grid, src), order))
+            self.entries.insert(0, (weakref.ref(grid), self._key(grid, src), perm))
 
     def clear(self):
         with self.lock:
@@ -98,12 +96,9 @@ class _OrderCache:
 _orders = _OrderCache()
 
 
-def sample_order(grid, src_size, with_cells=False):
+def sample_order(grid, src_size):
     """Source-sorted processing order of `grid`'s sampling points (int32
-    permutation) for a source of spatial size `src_size`.  With
-    `with_cells`, returns (perm, cells): cells[k] is the position in perm of
-    the first point of source cell k (batch item, then voxel, last axis
-    fastest), N * prod(src_size) + 1 entries."""
+    permutation) for a source of spatial size `src_size`."""
     L = _lib.load()
     src = (ctypes.c_int64 * len(src_size))(*[int(v) for v in src_size])
     d = _lib.desc(grid)
@@ -113,46 +108,26 @@ def sample_order(grid, src_size, with_cells=False):
     nvox = grid.numel() // grid.shape[-1]
     perm = torch.empty(nvox, dtype=torch.int32, device=grid.device)
     ws = torch.empty(nbytes, dtype=torch.uint8, device=grid.device)
-    cells = None
     with _On(grid):
-        if with_cells:
-            ncell = grid.shape[0] * math.prod(int(v) for v in src_size) + 1
-            cells = torch.empty(ncell, dtype=torch.int32, device=grid.device)
-            _lib.check(L.pp_sample_order_cells(ctypes.byref(d), src, ctypes.c_void_p(perm.data_ptr()),
-                                               ctypes.c_void_p(cells.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
-                                               nbytes, _lib.stream_of(grid)))
-        else:
-            _lib.check(L.pp_sample_order(ctypes.byref(d), src, ctypes.c_void_p(perm.data_ptr()),
-                                         ctypes.c_void_p(ws.data_ptr()), nbytes, _lib.stream_of(grid)))
-    return (perm, cells) if with_cells else perm
+        _lib.check(L.pp_sample_order(ctypes.byref(d), src, ctypes.c_void_p(perm.data_ptr()),
+                                     ctypes.c_void_p(ws.data_ptr()), nbytes, _lib.stream_of(grid)))
+    return perm
 
 
 def _order_for(grid, src_size):
-    """(perm, cells) of the cached source-sorted order, or None."""
     mode = _sample_order_mode
     if mode == "natural":
         return None
     nvox = grid.numel() // grid.shape[-1]
     if mode == "auto" and nvox < _SORT_MIN_SAMPLES:
         return None
-    if nvox >= (1 << 31) or grid.shape[0] * math.prod(int(v) for v in src_size) >= (1 << 31):
+    if nvox >= (1 << 31):
         return None
-    order = _orders.get(grid, src_size)
-    if order is None:
-        order = sample_order(grid, src_size, with_cells=True)
-        _orders.put(grid, src_size, order)
-    return order
-
-
-def set_gather_push(flag=True):
-    """Run 3-D pushes of orders 1 and 3 into float32 outputs (and the
-    input-gradient halves of pull backward passes) in gather form -- each
-    output voxel sums the sorted points of its cells, the points near the
-    faces are scattered -- when a sorted sample order is in use (the
-    default for large grids).  Off: the scatter (float atomics) everywhere.
-    Results agree to float32 rounding either way."""
-    global _gather_push
-    _gather_push = bool(flag)
+    perm = _orders.get(grid, src_size)
+    if perm is None:
+        perm = sample_order(grid, src_size)
+        _orders.put(grid, src_size, perm)
+    return perm
 
 
 def set_deterministic(flag=True):
@@ -245,12 +220,11 @@ def _grid32(grid):
 
 def _opts(bound, interpolation, extrapolate, grid=None, src_size=None):
     _check_opts(bound, interpolation)
-    order = _order_for(grid, src_size) if grid is not None and grid.is_cuda else None
+    perm = _order_for(grid, src_size) if grid is not None and grid.is_cuda else None
     o = _lib.options([int(b) for b in bound], [int(i) for i in interpolation],
                      int(extrapolate), _lib.PP_DETERMINISTIC if _deterministic else 0,
-                     None if order is None else order[0].data_ptr(),
-                     None if order is None or not _gather_push else order[1].data_ptr())
-    o._keep = order      # keep the permutation and cell offsets alive for the call
+                     None if perm is None else perm.data_ptr())
+    o._keep = perm       # keep the permutation alive for the call
     return o
 
 
