@@ -8,6 +8,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <string>
 
 #include "../../include/nitorch_b200.h"
@@ -243,11 +244,55 @@ __global__ void store_interleaved(const float* acc, S* dst, Strided s, int64_t V
   }
 }
 
+// Contiguous (N, C, *spatial) output: one thread per voxel, one vector load
+// of its CP accumulator slots, C coalesced stores.  blockIdx.y = batch item.
+template <class S, int CP>
+__global__ void store_interleaved_vox(const float* __restrict__ acc, S* __restrict__ dst, int64_t V, int C) {
+  using VT = typename std::conditional<CP == 4, float4, float2>::type;
+  const int64_t nb = blockIdx.y;
+  const float* a = acc + nb * V * CP;
+  S* o = dst + nb * C * V;
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < V; i += step) {
+    const VT v = *reinterpret_cast<const VT*>(a + i * CP);
+    const float* f = reinterpret_cast<const float*>(&v);
+#pragma unroll
+    for (int c = 0; c < CP; ++c)
+      if (c < C) o[c * V + i] = ppk::from_acc<S>(static_cast<typename ppk::Acc<S>::type>(f[c]));
+  }
+}
+
+template <class S>
+int store_interleaved_fast(const float* acc, S* dst, int64_t N, int64_t V, int C, int CP, cudaStream_t st) {
+  const int64_t want = (V + 255) / 256;
+  const unsigned bx = static_cast<unsigned>(want < 148 * 16 ? want : 148 * 16);
+  const dim3 grid(bx > 0 ? bx : 1, static_cast<unsigned>(N));
+  if (CP == 4) store_interleaved_vox<S, 4><<<grid, 256, 0, st>>>(acc, dst, V, C);
+  else store_interleaved_vox<S, 2><<<grid, 256, 0, st>>>(acc, dst, V, C);
+  count_launch();
+  return cuda_check(cudaGetLastError(), "interleaved store");
+}
+
 int store_interleaved_to(const float* acc, const pp_tensor* out, int CP, cudaStream_t st) {
   const int64_t n = numel(out);
   if (n == 0) return PP_OK;
   Strided s = make_strided(out);
   const int64_t C = out->sizes[1], V = n / (out->sizes[0] * C);
+  bool contiguous = out->sizes[0] <= 65535 && (CP == 2 || CP == 4) && C <= CP;
+  {
+    int64_t e = 1;
+    for (int i = out->ndim - 1; i >= 0 && contiguous; --i) {
+      if (out->sizes[i] > 1 && out->strides[i] != e) contiguous = false;
+      e *= out->sizes[i];
+    }
+  }
+  if (contiguous) {
+    if (out->dtype == PP_FLOAT32)
+      return store_interleaved_fast(acc, static_cast<float*>(out->data), out->sizes[0], V, static_cast<int>(C), CP, st);
+    if (out->dtype == PP_BFLOAT16)
+      return store_interleaved_fast(acc, static_cast<__nv_bfloat16*>(out->data), out->sizes[0], V,
+                                    static_cast<int>(C), CP, st);
+  }
   const int nb = grid_blocks(n);
   switch (out->dtype) {
     case PP_FLOAT32: store_interleaved<float><<<nb, 256, 0, st>>>(acc, static_cast<float*>(out->data), s, V, C, CP); break;

@@ -1078,6 +1078,130 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_lanes_k
   }
 }
 
+// Pull backward (K_PUSHGRAD) with the last axis' taps spread over lanes
+// (3-D, orders 1 and 3, float arithmetic, channel-interleaved float
+// accumulator for the image gradient: flag F_VEC, C <= CP).  NT consecutive
+// lanes serve one sampling point, lane q its last-axis tap q:
+//  * image gradient: the incoming gradient t (C channels at the point)
+//    times the tap weight, one vector reduction per tap -- consecutive lanes
+//    add to consecutive voxels as in pp_lanes_kernel;
+//  * grid gradient: per tap, the dot product of t with the image values
+//    there, weighted by the three derivative stencils; each lane sums its
+//    last-axis tap, the NT partial sums are added with shuffles inside the
+//    lane group and lane 0 stores them.
+// Lanes of one point stay together to the end (no early return between the
+// point's first and last shuffle): a missing tap contributes zero instead.
+template <int ORD, class S, class I, int CP>
+__global__ void __launch_bounds__(PP_THREADS, MinBlocks<K_PUSHGRAD>::value) pp_lanes_pullbwd_kernel(const PPArgs a) {
+  using T = float;
+  constexpr int NT = Taps<ORD>::value;
+  constexpr int PPB = PP_THREADS / NT;
+  const int q = static_cast<int>(threadIdx.x) % NT;
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
+  if (t >= a.nvox) return;  // whole lane groups (t is per group)
+  const unsigned lanes = ((1u << NT) - 1u) << ((threadIdx.x & 31u) & ~static_cast<unsigned>(NT - 1));
+  I v = a.perm != nullptr ? static_cast<I>(__ldg(a.perm + t)) : static_cast<I>(t);
+  I sub[3];
+  sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]);
+  sub[1] = v % static_cast<I>(a.trgt_size[1]); v /= static_cast<I>(a.trgt_size[1]);
+  sub[0] = v % static_cast<I>(a.trgt_size[0]);
+  const I n = v / static_cast<I>(a.trgt_size[0]);
+
+  const T* gp = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
+  int64_t tvox = static_cast<int64_t>(n) * a.trgt_sN, gvox = static_cast<int64_t>(n) * a.gg_sN;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    tvox += static_cast<int64_t>(sub[d]) * a.trgt_s[d];
+    gvox += static_cast<int64_t>(sub[d]) * a.gg_s[d];
+    gp += static_cast<int64_t>(sub[d]) * a.grid_s[d];
+  }
+  T coord[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
+  const bool do_a = (a.flags & F_A) != 0;
+  const bool do_grad = (a.flags & F_GRAD) != 0;
+  {
+    const T tol = (a.extrapolate & 2) ? static_cast<T>(0.5 + 5e-2) : static_cast<T>(5e-2);
+    bool inb = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) inb = inb && in_fov<T>(coord[d], a.src_size[d], tol);
+    if (!((a.extrapolate & 1) || inb)) {  // the whole group: zero grid gradient, no push
+      if (do_grad && q == 0) {
+        T* g = static_cast<T*>(a.gg) + gvox;
+        g[0] = T(0); g[a.gg_sD] = T(0); g[2 * a.gg_sD] = T(0);
+      }
+      return;
+    }
+  }
+  Axis<NT, T, I> ax, ay, az;
+  build_axis<NT, true, false, true, true, T, I>(ax, ORD, a.bound[0], coord[0], static_cast<I>(a.src_size[0]),
+                                                 static_cast<I>(a.src_s[0]), static_cast<I>(a.out_s[0]));
+  build_axis<NT, true, false, true, true, T, I>(ay, ORD, a.bound[1], coord[1], static_cast<I>(a.src_size[1]),
+                                                 static_cast<I>(a.src_s[1]), static_cast<I>(a.out_s[1]));
+  build_axis<NT, true, false, true, true, T, I>(az, ORD, a.bound[2], coord[2], static_cast<I>(a.src_size[2]),
+                                                 static_cast<I>(a.src_s[2]), static_cast<I>(a.out_s[2]));
+  // this lane's last-axis tap (selected without dynamic register indexing)
+  T wz = T(0), gz = T(0);
+  I osz = 0, ooz = 0;
+  bool vz = false;
+#pragma unroll
+  for (int k = 0; k < NT; ++k)
+    if (k == q) { wz = az.w[k]; gz = az.g[k]; osz = az.os[k]; ooz = az.oo[k]; vz = ((az.mask >> k) & 1u) != 0u; }
+
+  const S* trg_v = static_cast<const S*>(a.trgt) + tvox;
+  const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(n) * a.src_sN;
+  float* acc_n = static_cast<float*>(a.out) + static_cast<int64_t>(n) * a.out_sN;
+  float tv[CP];
+#pragma unroll
+  for (int c = 0; c < CP; ++c) tv[c] = c < a.C ? static_cast<float>(ldg_acc(trg_v + c * a.trgt_sC)) : 0.f;
+  T og0 = T(0), og1 = T(0), og2 = T(0);
+  if (vz) {
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      if (((ay.mask >> j) & 1u) == 0u) continue;
+      const I osyz = ay.os[j] + osz, ooyz = ay.oo[j] + ooz;
+      T sx = T(0), dx = T(0);  // sum_i w_i <t, src>, sum_i g_i <t, src>
+#pragma unroll
+      for (int i = 0; i < NT; ++i) {
+        if (((ax.mask >> i) & 1u) == 0u) continue;
+        if (do_grad) {
+          const S* sp = src_n + (ax.os[i] + osyz);
+          T dot = T(0);
+#pragma unroll
+          for (int c = 0; c < CP; ++c)
+            if (c < a.C) dot = fma(tv[c], ldg_acc(sp + c * a.src_sC), dot);
+          sx = fma(ax.w[i], dot, sx);
+          dx = fma(ax.g[i], dot, dx);
+        }
+        if (do_a) {
+          const float wt = ax.w[i] * ay.w[j] * wz;
+          if (wt != 0.f) {
+            float vals[CP];
+#pragma unroll
+            for (int c = 0; c < CP; ++c) vals[c] = wt * tv[c];
+            red_vec<CP>(acc_n + (ax.oo[i] + ooyz), vals);
+          }
+        }
+      }
+      og0 = fma(ay.w[j] * wz, dx, og0);
+      og1 = fma(ay.g[j] * wz, sx, og1);
+      og2 = fma(ay.w[j] * gz, sx, og2);
+    }
+  }
+  if (do_grad) {
+#pragma unroll
+    for (int o = 1; o < NT; o <<= 1) {
+      og0 += __shfl_xor_sync(lanes, og0, o);
+      og1 += __shfl_xor_sync(lanes, og1, o);
+      og2 += __shfl_xor_sync(lanes, og2, o);
+    }
+    if (q == 0) {
+      T* g = static_cast<T*>(a.gg) + gvox;
+      g[0] = og0; g[a.gg_sD] = og1; g[2 * a.gg_sD] = og2;
+    }
+  }
+}
+
 // The lane-split push applies to 3-D push / count at orders 1 and 3.
 template <int D, int ORD, int MODE> struct UseLanes {
   static constexpr bool value = D == 3 && (ORD == 1 || ORD == 3) && (MODE == K_PUSH || MODE == K_COUNT);
@@ -1087,6 +1211,18 @@ bool lanes_enabled();  // host switch (pp_capi.cu), on unless PP_PUSH_LANES=0
 template <int D, int ORD, int CB, class S, int MODE, class I>
 inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
   if (a.nvox == 0) return cudaSuccess;
+  if constexpr (D == 3 && (ORD == 1 || ORD == 3) && MODE == K_PUSHGRAD && CB >= 2 &&
+                std::is_same<typename Acc<S>::type, float>::value) {
+    // pull backward into the interleaved accumulator: lane-split kernel
+    if (lanes_enabled() && (a.flags & F_VEC) && a.det_acc == nullptr &&
+        !(a.flags & (F_IDGRID | F_ADDSELF | F_AFFINE | F_NOTRGT))) {
+      constexpr int PPB = PP_THREADS / Taps<ORD>::value;
+      const int64_t nb = (a.nvox + PPB - 1) / PPB;
+      if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+      pp_lanes_pullbwd_kernel<ORD, S, I, (CB == 2 ? 2 : 4)><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
+      return cudaGetLastError();
+    }
+  }
   if constexpr (UseLanes<D, ORD, MODE>::value) {
     if (lanes_enabled()) {
       constexpr int PPB = PP_THREADS / Taps<ORD>::value;
