@@ -48,23 +48,30 @@ inline int64_t key_geometry(KeyArgs& a, int D, const int64_t* src) {
   return n;
 }
 
+// One thread per sampling point.  Index arithmetic in 32 bits (the host
+// guarantees fewer than 2^31 samples and keys); memory offsets in 64.
 template <class T>
 __global__ void order_keys(KeyArgs a, int32_t* count, int32_t* keys, int32_t* ranks) {
-  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (s >= a.nvox) return;
-  int64_t v = s, sub[3] = {0, 0, 0};
-  for (int d = a.D - 1; d >= 0; --d) { sub[d] = v % a.size[d]; v /= a.size[d]; }
-  const int64_t n = v;
-  const T* g = static_cast<const T*>(a.grid) + n * a.gsN;
-  for (int d = 0; d < a.D; ++d) g += sub[d] * a.gs[d];
-  int64_t lin = 0;
-  for (int d = 0; d < a.D; ++d) {
-    T c = g[d * a.gsD];
-    // floor, clamped into the volume (NaN -> 0)
-    int64_t i = (c >= T(0)) ? static_cast<int64_t>(fmin(c, static_cast<T>(a.src[d] - 1))) : 0;
-    lin = lin * a.src[d] + i;
+  const unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= static_cast<unsigned>(a.nvox)) return;
+  int v = static_cast<int>(s), sub[3] = {0, 0, 0};
+  for (int d = a.D - 1; d >= 0; --d) {
+    const int n = static_cast<int>(a.size[d]);
+    const int q = v / n;
+    sub[d] = v - q * n;
+    v = q;
   }
-  const int32_t key = static_cast<int32_t>(n * a.nsrc + lin);
+  const T* g = static_cast<const T*>(a.grid) + static_cast<int64_t>(v) * a.gsN;
+  for (int d = 0; d < a.D; ++d) g += static_cast<int64_t>(sub[d]) * a.gs[d];
+  int lin = 0;
+  for (int d = 0; d < a.D; ++d) {
+    const T c = g[d * a.gsD];
+    const int n = static_cast<int>(a.src[d]);
+    // floor, clamped into the volume (NaN -> 0)
+    const int i = (c >= T(0)) ? static_cast<int>(fmin(c, static_cast<T>(n - 1))) : 0;
+    lin = lin * n + i;
+  }
+  const int32_t key = v * static_cast<int>(a.nsrc) + lin;
   keys[s] = key;
   ranks[s] = atomicAdd(count + key, 1);
 }
