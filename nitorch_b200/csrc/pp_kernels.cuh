@@ -103,7 +103,6 @@ struct Axis {
   I oo[NT];   // offsets into the scattered tensor (out)
   unsigned mask;  // bit t set: tap t is a real node (sign != 0)
   int nt;
-  bool inside;    // every tap inside [0, n): offsets consecutive, no boundary mapping
 };
 
 template <int NT, bool NEED_G, bool NEED_H, bool NEED_OS, bool NEED_OO, class T, class I>
@@ -117,7 +116,6 @@ __device__ __forceinline__ void build_axis(Axis<NT, T, I>& ax, int ORDc, int bnd
   x = fmin(fmax(x, T(-1073741824.0)), T(1073741824.0));
   const I low = support_low<I, T>(ord, x);
   const bool inside = low >= 0 && low + nt - 1 < n;
-  ax.inside = inside;
   const T f = (x - static_cast<T>(low)) - T(0.5) * static_cast<T>(ord - 1);
   bspline_stencil<NT, NEED_G, NEED_H, T>(ord, ord == 0 ? T(0) : f, ax.w, ax.g, ax.h);
   ax.mask = 0;
@@ -142,7 +140,7 @@ __device__ __forceinline__ void build_axis(Axis<NT, T, I>& ax, int ORDc, int bnd
 
 template <int NT, class T, class I>
 __device__ __forceinline__ void unit_axis(Axis<NT, T, I>& ax) {
-  ax.nt = 1; ax.mask = 1u; ax.inside = true;
+  ax.nt = 1; ax.mask = 1u;
 #pragma unroll
   for (int t = 0; t < NT; ++t) { ax.w[t] = t == 0 ? T(1) : T(0); ax.g[t] = T(0); ax.h[t] = T(0); ax.os[t] = 0; ax.oo[t] = 0; }
 }
@@ -352,50 +350,12 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
   // ======================= gather-only modes ================================
   if constexpr (MODE == K_PULL) {
     S* op = static_cast<S*>(a.out) + ovox;
-    // Interior fast path (compile-time order, 3-D): every x / y tap a real
-    // node, the z taps inside the volume and z contiguous in memory.  Per
-    // (x, y) row one address per channel; the z taps load at constant
-    // offsets from it, with no per-tap address arithmetic or validity select.
-    bool fast = false;
-    if constexpr (ORD > 0 && D == 3) {
-      fast = az.inside && a.src_s[2] == 1 && ax.mask == (1u << NT) - 1u && ay.mask == (1u << NT) - 1u;
-    }
     for (int64_t c0 = 0; c0 < C; c0 += CB) {
       const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
       const S* sp = src_n + c0 * a.src_sC;
       T acc[CB];
 #pragma unroll
       PP_CB acc[cb] = T(0);
-      if constexpr (ORD > 0 && D == 3) {
-        if (fast) {
-          const S* spc[CB];
-#pragma unroll
-          PP_CB spc[cb] = sp + (CB == 1 || cb < nc ? cb : 0) * a.src_sC + az.os[0];
-#pragma unroll
-          for (int i = 0; i < NX; ++i) {
-            T accy[CB];
-#pragma unroll
-            PP_CB accy[cb] = T(0);
-#pragma unroll
-            for (int j = 0; j < NY; ++j) {
-              const I o = ax.os[i] + ay.os[j];
-#pragma unroll
-              PP_CB {
-                if (CB == 1 || cb < nc) {
-                  const S* p = spc[cb] + o;
-                  T accz = T(0);
-#pragma unroll
-                  for (int k = 0; k < NZ; ++k) accz = fma(az.w[k], ldg_acc(p + k), accz);
-                  accy[cb] = fma(ay.w[j], accz, accy[cb]);
-                }
-              }
-            }
-#pragma unroll
-            PP_CB acc[cb] = fma(ax.w[i], accy[cb], acc[cb]);
-          }
-        }
-      }
-      if (!fast) {
 #pragma unroll (OuterUnroll<ORD, NZ>::value)
       for (int k = 0; k < NZ; ++k) {
         if (k < tz) {
@@ -431,7 +391,6 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
 #pragma unroll
           PP_CB acc[cb] = fma(az.w[k], accy[cb], acc[cb]);
         }
-      }
       }
       if (a.flags & F_ADDSELF) {
         // self-composition: add the field's own value at the point
