@@ -55,11 +55,13 @@ struct VecStore {
 constexpr int kMaxStores = 256;
 struct StoreLaunch {
   int32_t n, pad;
-  int64_t first[kMaxStores + 1];  // element prefix sums (V * C per volume)
+  int64_t first[kMaxStores + 1];  // voxel prefix sums (V per volume)
   VecStore s[kMaxStores];
 };
 static_assert(sizeof(StoreLaunch) <= 32764, "store argument above the kernel-parameter limit");
 
+// One thread per voxel: its CP accumulator slots (consecutive, so a warp
+// reads whole sectors) to the C channel planes of the output (coalesced).
 __global__ void __launch_bounds__(256) batch_store_kernel(const __grid_constant__ StoreLaunch L) {
   const int64_t total = L.first[L.n];
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
@@ -70,9 +72,10 @@ __global__ void __launch_bounds__(256) batch_store_kernel(const __grid_constant_
       if (L.first[mid] <= i) lo = mid; else hi = mid - 1;
     }
     const VecStore& v = L.s[lo];
-    const int64_t j = i - L.first[lo];  // = c * V + lin
-    const int64_t c = j / v.V, lin = j - c * v.V;
-    v.out[j] = v.acc[lin * v.CP + c];
+    const int64_t lin = i - L.first[lo];
+    const float* a = v.acc + lin * v.CP;
+    float* o = v.out + lin;
+    for (int c = 0; c < v.C; ++c) o[c * v.V] = a[c];
   }
 }
 
@@ -364,7 +367,7 @@ int pp_batch_run(const void* plan, void* stream) {
     SL.first[0] = 0;
     for (int e = 0; e < n; ++e) {
       SL.s[e] = ps[s0 + e];
-      SL.first[e + 1] = SL.first[e] + SL.s[e].V * SL.s[e].C;
+      SL.first[e + 1] = SL.first[e] + SL.s[e].V;
     }
     const int nb = grid_blocks(SL.first[n]);
     batch_store_kernel<<<nb, 256, 0, st>>>(SL);
