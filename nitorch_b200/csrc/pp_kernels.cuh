@@ -356,54 +356,42 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
       T acc[CB];
 #pragma unroll
       PP_CB acc[cb] = T(0);
-      // The tap nest, instantiated twice: with every tap a real node (all
-      // points under the replicate / dct / dft bounds) no per-tap validity
-      // mask and select.  Same summation order either way.
-      auto nest = [&](auto all_valid) {
-        constexpr bool ALL = decltype(all_valid)::value;
 #pragma unroll (OuterUnroll<ORD, NZ>::value)
-        for (int k = 0; k < NZ; ++k) {
-          if (k < tz) {
-            T accy[CB];
+      for (int k = 0; k < NZ; ++k) {
+        if (k < tz) {
+          T accy[CB];
 #pragma unroll
-            PP_CB accy[cb] = T(0);
+          PP_CB accy[cb] = T(0);
 #pragma unroll
-            for (int j = 0; j < NY; ++j) {
-              if (j < ty) {
-                const I oyz = ay.os[j] + az.os[k];
-                T accx[CB];
+          for (int j = 0; j < NY; ++j) {
+            if (j < ty) {
+              const I oyz = ay.os[j] + az.os[k];
+              T accx[CB];
 #pragma unroll
-                PP_CB accx[cb] = T(0);
+              PP_CB accx[cb] = T(0);
 #pragma unroll
-                for (int i = 0; i < NX; ++i) {
-                  if (i < tx) {
-                    const I off = ax.os[i] + oyz;
-                    bool valid = true;
-                    if constexpr (!ALL) valid = PP_TAP_VALID(i, j, k);
+              for (int i = 0; i < NX; ++i) {
+                if (i < tx) {
+                  const I off = ax.os[i] + oyz;
+                  const bool valid = PP_TAP_VALID(i, j, k);
 #pragma unroll
-                    PP_CB {
-                      if (CB == 1 || cb < nc) {
-                        // (channel base) + 32-bit tap offset: one wide multiply-add
-                        T v = ldg_acc(sp + cb * a.src_sC + off);
-                        if constexpr (!ALL) {
-                          if (!valid) v = T(0);
-                        }
-                        accx[cb] = fma(ax.w[i], v, accx[cb]);
-                      }
+                  PP_CB {
+                    if (CB == 1 || cb < nc) {
+                      T v = ldg_acc(sp + (cb * a.src_sC + off));
+                      if (!valid) v = T(0);
+                      accx[cb] = fma(ax.w[i], v, accx[cb]);
                     }
                   }
                 }
-#pragma unroll
-                PP_CB accy[cb] = fma(ay.w[j], accx[cb], accy[cb]);
               }
-            }
 #pragma unroll
-            PP_CB acc[cb] = fma(az.w[k], accy[cb], acc[cb]);
+              PP_CB accy[cb] = fma(ay.w[j], accx[cb], accy[cb]);
+            }
           }
+#pragma unroll
+          PP_CB acc[cb] = fma(az.w[k], accy[cb], acc[cb]);
         }
-      };
-      if (full) nest(std::true_type{});
-      else nest(std::false_type{});
+      }
       if (a.flags & F_ADDSELF) {
         // self-composition: add the field's own value at the point
         int64_t so = 0;
