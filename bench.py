@@ -262,6 +262,7 @@ def timed_steps(fn, args, world, device, l2buf, timer=None, clocks=None, steps=N
 # GPU's atomic path sustains when fully coalesced, measured on B200 with
 # tests/perf_atomic_throughput.py (1.46 T scalar adds/s; vector forms 1.6 T).
 ATOMIC_ADDS_PER_S = 1.46e12
+HBM_SPEC_GBS = 8000.0  # B200 HBM3e specification (the measured copy bandwidth is the roofline)
 SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
 
 
@@ -271,10 +272,14 @@ def roofline(ops, labels, nvox, C, ms_per_step, traffic):
     per = algo_bytes(dom, 4, C) * nvox
     achieved = per / (ops[dom]["avg_ms"] * 1e-3) / 1e9
     step_bytes = sum(algo_bytes(k, 4, C) for k in labels) * nvox
+    step_gbs = step_bytes / (ms_per_step * 1e-3) / 1e9
     out = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
            "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": src,
            "algorithmic_bytes_per_launch": per, "traffic": traffic,
-           "step_frac": round(step_bytes / (ms_per_step * 1e-3) / 1e9 / hbm, 4)}
+           "step_frac": round(step_gbs / hbm, 4),
+           # the same against the 8 TB/s HBM3e specification
+           "spec_gbs": HBM_SPEC_GBS, "frac_of_spec": round(achieved / HBM_SPEC_GBS, 4),
+           "step_frac_of_spec": round(step_gbs / HBM_SPEC_GBS, 4)}
     if dom in SCATTER_OPS:
         # the binding resource of a scatter: 64 taps x C channels float adds per point (cubic 3-D)
         adds = 64 * C * nvox
