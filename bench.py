@@ -266,16 +266,28 @@ HBM_SPEC_GBS = 8000.0  # B200 HBM3e specification (the measured copy bandwidth i
 SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dominant kernel on this workload (config 2: 1x3x192^3, cubic, dct2,
+# source-sorted order), from one ncu capture of the same kernel.
+MEASURED_TRAFFIC = {
+    "pull_bwd": (396.5e6 + 168.6e6, "ncu capture of pp_lanes_pullbwd_kernel, "
+                 "profiles/pp_lanes_pullbwd_cubic_c3_192_sorted_order.md"),
+}
+
+
 def roofline(ops, labels, nvox, C, ms_per_step, traffic):
     hbm, src = peaks()
     dom = max(ops, key=lambda k: ops[k]["total_ms"])
+    traffic_src = "--traffic" if traffic is not None else None
+    if traffic is None and dom in MEASURED_TRAFFIC and nvox == 192 ** 3 and C == 3:
+        traffic, traffic_src = MEASURED_TRAFFIC[dom]
     per = algo_bytes(dom, 4, C) * nvox
     achieved = per / (ops[dom]["avg_ms"] * 1e-3) / 1e9
     step_bytes = sum(algo_bytes(k, 4, C) for k in labels) * nvox
     step_gbs = step_bytes / (ms_per_step * 1e-3) / 1e9
     out = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
            "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": src,
-           "algorithmic_bytes_per_launch": per, "traffic": traffic,
+           "algorithmic_bytes_per_launch": per, "traffic": traffic, "traffic_source": traffic_src,
            "step_frac": round(step_gbs / hbm, 4),
            # the same against the 8 TB/s HBM3e specification
            "spec_gbs": HBM_SPEC_GBS, "frac_of_spec": round(achieved / HBM_SPEC_GBS, 4),
