@@ -1206,171 +1206,6 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
   }
 }
 
-// Fused normal operator push(pull(src)) (K_PP) and its adjoint (K_PP_BWD)
-// with the last axis' taps spread over lanes (3-D, orders 1 and 3, float
-// arithmetic, channel-interleaved float accumulator: flag F_VEC, C <= CP).
-// NT consecutive lanes serve one point, lane q its last-axis tap q.  Each
-// lane gathers its tap's share of the interpolants (K_PP: the pulled value;
-// K_PP_BWD: src's and W's values and spatial derivatives); an xor-shuffle
-// all-reduce inside the lane group gives every lane the full sums; each lane
-// then scatters its own taps with vector reductions, and lane 0 stores the
-// grid gradient.  Lanes of a point stay together up to the last shuffle.
-template <int ORD, class S, class I, int CP, bool BWD>
-__global__ void __launch_bounds__(PP_THREADS, BWD ? 2 : 4) pp_lanes_pp_kernel(const PPArgs a) {
-  using T = float;
-  constexpr int NT = Taps<ORD>::value;
-  constexpr int PPB = PP_THREADS / NT;
-  constexpr int NV = BWD ? 8 : 1;  // reduced quantities per channel
-  const int q = static_cast<int>(threadIdx.x) % NT;
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
-  if (t >= a.nvox) return;  // whole lane groups
-  const unsigned lanes = ((1u << NT) - 1u) << ((threadIdx.x & 31u) & ~static_cast<unsigned>(NT - 1));
-  I v = a.perm != nullptr ? static_cast<I>(__ldg(a.perm + t)) : static_cast<I>(t);
-  I sub[3];
-  sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]);
-  sub[1] = v % static_cast<I>(a.trgt_size[1]); v /= static_cast<I>(a.trgt_size[1]);
-  sub[0] = v % static_cast<I>(a.trgt_size[0]);
-  const I n = v / static_cast<I>(a.trgt_size[0]);
-
-  const T* gp = static_cast<const T*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN;
-  int64_t gvox = static_cast<int64_t>(n) * a.gg_sN;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    gvox += static_cast<int64_t>(sub[d]) * a.gg_s[d];
-    gp += static_cast<int64_t>(sub[d]) * a.grid_s[d];
-  }
-  T coord[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
-  const bool do_a = BWD ? (a.flags & F_A) != 0 : true;
-  const bool do_grad = BWD && (a.flags & F_GRAD) != 0;
-  {
-    const T tol = (a.extrapolate & 2) ? static_cast<T>(0.5 + 5e-2) : static_cast<T>(5e-2);
-    bool inb = true;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) inb = inb && in_fov<T>(coord[d], a.src_size[d], tol);
-    if (!((a.extrapolate & 1) || inb)) {  // the whole group: no push, zero grid gradient
-      if (do_grad && q == 0) {
-        T* g = static_cast<T*>(a.gg) + gvox;
-        g[0] = T(0); g[a.gg_sD] = T(0); g[2 * a.gg_sD] = T(0);
-      }
-      return;
-    }
-  }
-  Axis<NT, T, I> ax, ay, az;
-  build_axis<NT, BWD, false, true, true, T, I>(ax, ORD, a.bound[0], coord[0], static_cast<I>(a.src_size[0]),
-                                                static_cast<I>(a.src_s[0]), static_cast<I>(a.out_s[0]));
-  build_axis<NT, BWD, false, true, true, T, I>(ay, ORD, a.bound[1], coord[1], static_cast<I>(a.src_size[1]),
-                                                static_cast<I>(a.src_s[1]), static_cast<I>(a.out_s[1]));
-  build_axis<NT, BWD, false, true, true, T, I>(az, ORD, a.bound[2], coord[2], static_cast<I>(a.src_size[2]),
-                                                static_cast<I>(a.src_s[2]), static_cast<I>(a.out_s[2]));
-  T wz = T(0), gz = T(0);
-  I osz = 0, ooz = 0;
-  bool vz = false;
-#pragma unroll
-  for (int k = 0; k < NT; ++k)
-    if (k == q) { wz = az.w[k]; gz = az.g[k]; osz = az.os[k]; ooz = az.oo[k]; vz = ((az.mask >> k) & 1u) != 0u; }
-
-  const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(n) * a.src_sN;
-  const S* w_n = BWD ? static_cast<const S*>(a.trgt) + static_cast<int64_t>(n) * a.src_sN : nullptr;
-  // r[c][0..NV): K_PP: y; K_PP_BWD: yv, yx, yy, yz (src), dv, dx, dy, dz (W)
-  T r[CP][NV];
-#pragma unroll
-  for (int c = 0; c < CP; ++c)
-#pragma unroll
-    for (int e = 0; e < NV; ++e) r[c][e] = T(0);
-  if (vz) {
-#pragma unroll
-    for (int j = 0; j < NT; ++j) {
-      if (((ay.mask >> j) & 1u) == 0u) continue;
-      const I osyz = ay.os[j] + osz;
-      T sx[CP], sdx[CP], ux[CP], udx[CP];
-#pragma unroll
-      for (int c = 0; c < CP; ++c) sx[c] = sdx[c] = ux[c] = udx[c] = T(0);
-#pragma unroll
-      for (int i = 0; i < NT; ++i) {
-        if (((ax.mask >> i) & 1u) == 0u) continue;
-        const I off = ax.os[i] + osyz;
-#pragma unroll
-        for (int c = 0; c < CP; ++c) {
-          if (c < a.C) {
-            const T vv = ldg_acc(src_n + c * a.src_sC + off);
-            sx[c] = fma(ax.w[i], vv, sx[c]);
-            if constexpr (BWD) {
-              const T uu = ldg_acc(w_n + c * a.src_sC + off);
-              sdx[c] = fma(ax.g[i], vv, sdx[c]);
-              ux[c] = fma(ax.w[i], uu, ux[c]);
-              udx[c] = fma(ax.g[i], uu, udx[c]);
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < CP; ++c) {
-        if constexpr (BWD) {
-          r[c][0] = fma(ay.w[j] * wz, sx[c], r[c][0]);
-          r[c][1] = fma(ay.w[j] * wz, sdx[c], r[c][1]);
-          r[c][2] = fma(ay.g[j] * wz, sx[c], r[c][2]);
-          r[c][3] = fma(ay.w[j] * gz, sx[c], r[c][3]);
-          r[c][4] = fma(ay.w[j] * wz, ux[c], r[c][4]);
-          r[c][5] = fma(ay.w[j] * wz, udx[c], r[c][5]);
-          r[c][6] = fma(ay.g[j] * wz, ux[c], r[c][6]);
-          r[c][7] = fma(ay.w[j] * gz, ux[c], r[c][7]);
-        } else {
-          r[c][0] = fma(ay.w[j] * wz, sx[c], r[c][0]);
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 1; o < NT; o <<= 1)
-#pragma unroll
-    for (int c = 0; c < CP; ++c)
-#pragma unroll
-      for (int e = 0; e < NV; ++e) r[c][e] += __shfl_xor_sync(lanes, r[c][e], o);
-  // the values a separate pull / push-backward would have stored
-#pragma unroll
-  for (int c = 0; c < CP; ++c) {
-    r[c][0] = to_acc(from_acc<S>(r[c][0]));
-    if constexpr (BWD) r[c][4] = to_acc(from_acc<S>(r[c][4]));
-  }
-  if constexpr (BWD) {
-    if (do_grad && q == 0) {
-      T og0 = T(0), og1 = T(0), og2 = T(0);
-#pragma unroll
-      for (int c = 0; c < CP; ++c) {
-        if (c < a.C) {
-          og0 += r[c][0] * r[c][5] + r[c][4] * r[c][1];
-          og1 += r[c][0] * r[c][6] + r[c][4] * r[c][2];
-          og2 += r[c][0] * r[c][7] + r[c][4] * r[c][3];
-        }
-      }
-      T* g = static_cast<T*>(a.gg) + gvox;
-      g[0] = og0; g[a.gg_sD] = og1; g[2 * a.gg_sD] = og2;
-    }
-  }
-  if (do_a && vz) {
-    float* acc_n = static_cast<float*>(a.out) + static_cast<int64_t>(n) * a.out_sN;
-    constexpr int SRC = BWD ? 4 : 0;  // scatter dv (adjoint) or y (forward)
-#pragma unroll
-    for (int j = 0; j < NT; ++j) {
-      if (((ay.mask >> j) & 1u) == 0u) continue;
-      const T wyz = ay.w[j] * wz;
-      const I ooyz = ay.oo[j] + ooz;
-#pragma unroll
-      for (int i = 0; i < NT; ++i) {
-        if (((ax.mask >> i) & 1u) == 0u) continue;
-        const float wt = ax.w[i] * wyz;
-        if (wt == 0.f) continue;
-        float vals[CP];
-#pragma unroll
-        for (int c = 0; c < CP; ++c) vals[c] = wt * r[c][SRC];
-        red_vec<CP>(acc_n + (ax.oo[i] + ooyz), vals);
-      }
-    }
-  }
-}
-
 // The lane-split push applies to 3-D push / count at orders 1 and 3.
 template <int D, int ORD, int MODE> struct UseLanes {
   static constexpr bool value = D == 3 && (ORD == 1 || ORD == 3) && (MODE == K_PUSH || MODE == K_COUNT);
@@ -1380,19 +1215,6 @@ bool lanes_enabled();  // host switch (pp_capi.cu), on unless PP_PUSH_LANES=0
 template <int D, int ORD, int CB, class S, int MODE, class I>
 inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
   if (a.nvox == 0) return cudaSuccess;
-  if constexpr (D == 3 && (ORD == 1 || ORD == 3) && (MODE == K_PP || MODE == K_PP_BWD) && CB >= 2 &&
-                std::is_same<typename Acc<S>::type, float>::value) {
-    // fused normal operator into the interleaved accumulator: lane-split kernel
-    if (lanes_enabled() && (a.flags & F_VEC) && a.det_acc == nullptr &&
-        !(a.flags & (F_IDGRID | F_ADDSELF | F_AFFINE | F_NOTRGT))) {
-      constexpr int PPB = PP_THREADS / Taps<ORD>::value;
-      const int64_t nb = (a.nvox + PPB - 1) / PPB;
-      if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-      pp_lanes_pp_kernel<ORD, S, I, (CB == 2 ? 2 : 4), MODE == K_PP_BWD>
-          <<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
-      return cudaGetLastError();
-    }
-  }
   if constexpr (D == 3 && (ORD == 1 || ORD == 3) && MODE == K_PUSHGRAD && CB >= 2 &&
                 std::is_same<typename Acc<S>::type, float>::value) {
     // pull backward into the interleaved accumulator: lane-split kernel
