@@ -41,7 +41,7 @@ static const pb_launcher_t kBatchLaunchers[2][ppk::K_NMODES] = {PB_ROW(f32), PB_
 
 namespace ppb {
 
-constexpr int kMaxGroups = 32;     // (order 0-3) x (channel block 1-4) x (lane-split or not)
+constexpr int kMaxGroups = 16;     // (order 0-3) x (channel block 1-4)
 constexpr uint32_t kMagic = 0x50504231u;
 
 // Interleaved float accumulator (X*Y*Z*CP floats, channel fastest) of one
@@ -149,7 +149,7 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
   if (!plan || plan_bytes_ < plan_bytes(nvol))
     return fail(PP_ERR_WORKSPACE, "(): batch plan needs %zu bytes", plan_bytes(nvol));
   std::vector<ppk::PPArgs> args(nvol);
-  std::vector<int> order(nvol), cbs(nvol), lanes(nvol);
+  std::vector<int> order(nvol), cbs(nvol);
   std::vector<int64_t> nitems(nvol);
   std::vector<Fill> fills;
   std::vector<VecStore> stores;
@@ -261,6 +261,7 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
     if (!fits32(a.nvox)) return fail(PP_ERR_UNSUPPORTED, "(): batch entry %d: too many sampling points", v);
     order[v] = iso;
     cbs[v] = static_cast<int>(a.C >= 4 ? 4 : a.C);
+    nitems[v] = (a.nvox + kBatchPoints - 1) / kBatchPoints;
     const int CP = scatter && out && use_scratch ? entry_slots(mode, a.C, iso) : 0;
     if (CP) {
       // vector reductions into this entry's interleaved accumulator, stored
@@ -281,17 +282,12 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
     } else if (scatter && out) {
       fills.push_back({out->data, static_cast<size_t>(numel(out)) * 4});
     }
-    lanes[v] = lanes_entry(mode, iso, a.flags) ? 1 : 0;
-    const int ppi = lanes[v] ? kLanePoints : kBatchPoints;  // points per work item
-    nitems[v] = (a.nvox + ppi - 1) / ppi;
   }
   // group by (order, channel block)
   std::vector<int> idx(nvol);
   for (int v = 0; v < nvol; ++v) idx[v] = v;
   std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
-    if (order[x] != order[y]) return order[x] < order[y];
-    if (cbs[x] != cbs[y]) return cbs[x] < cbs[y];
-    return lanes[x] < lanes[y];
+    return order[x] != order[y] ? order[x] < order[y] : cbs[x] < cbs[y];
   });
   unsigned char* p = static_cast<unsigned char*>(plan);
   PlanHeader* h = reinterpret_cast<PlanHeader*>(p);
@@ -307,7 +303,7 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
   int g = -1;
   for (int k = 0; k < nvol; ++k) {
     const int v = idx[k];
-    if (g < 0 || h->gorder[g] != order[v] || h->gcb[g] != cbs[v] || lanes[idx[k - 1]] != lanes[v]) {
+    if (g < 0 || h->gorder[g] != order[v] || h->gcb[g] != cbs[v]) {
       ++g;
       h->gorder[g] = order[v];
       h->gcb[g] = cbs[v];

@@ -45,50 +45,12 @@ __global__ void __launch_bounds__(kBatchPoints, ppk::MinBlocks<MODE>::value)
   }
 }
 
-// Entries whose push / pull-backward runs lane-split (cubic, interleaved
-// accumulator): a work item is kBatchPoints / 4 sampling points, four
-// consecutive threads per point (see lanes_push_point, lanes_pullbwd_point).
-// The host plan sizes these entries' items with the same predicate.
-__host__ __device__ constexpr bool lanes_entry(int mode, int iso, int flags) {
-  return (mode == ppk::K_PUSH || mode == ppk::K_PUSHGRAD) && iso == 3 && (flags & ppk::F_VEC) != 0;
-}
-constexpr int kLanePoints = kBatchPoints / 4;
-
-template <class S, int MODE, int CB>
-__global__ void __launch_bounds__(kBatchPoints, MODE == ppk::K_PUSH ? 5 : 4)
-    pp_batch_lanes_kernel(const __grid_constant__ BatchLaunch L) {
-  constexpr int CP = CB == 2 ? 2 : 4;
-  const int64_t total = L.first[L.n];
-  for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    int lo = 0, hi = L.n - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (L.first[mid] <= item) lo = mid; else hi = mid - 1;
-    }
-    const ppk::PPArgs& a = L.e[lo];
-    const int64_t t = (item - L.first[lo]) * kLanePoints + threadIdx.x / 4;
-    if (t < a.nvox) {  // whole lane groups
-      if constexpr (MODE == ppk::K_PUSH) ppk::lanes_push_point<3, CB, S, MODE, int32_t, CP>(a, t, threadIdx.x % 4);
-      else ppk::lanes_pullbwd_point<3, S, int32_t, CP>(a, t, threadIdx.x % 4);
-    }
-  }
-}
-
 template <class S, int MODE, int ORD, int CB>
 cudaError_t launch_chunk(const BatchLaunch& L, int ctas, cudaStream_t st) {
   const int64_t total = L.first[L.n];
   if (total == 0) return cudaSuccess;
   const int64_t blocks = ctas > 0 ? (ctas < total ? ctas : total) : total;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-  if constexpr (ORD == 3 && CB >= 2 && (MODE == ppk::K_PUSH || MODE == ppk::K_PUSHGRAD) &&
-                std::is_same<typename ppk::Acc<S>::type, float>::value) {
-    // groups are homogeneous in lanes_entry (part of the plan's group key)
-    if (lanes_entry(MODE, ORD, L.e[0].flags)) {
-      pp_batch_lanes_kernel<S, MODE, CB><<<static_cast<unsigned>(blocks), kBatchPoints, 0, st>>>(L);
-      ppc::count_launch();
-      return cudaGetLastError();
-    }
-  }
   pp_batch_kernel<S, MODE, ORD, CB><<<static_cast<unsigned>(blocks), kBatchPoints, 0, st>>>(L);
   ppc::count_launch();
   return cudaGetLastError();

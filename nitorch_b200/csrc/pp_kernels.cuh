@@ -963,9 +963,13 @@ __global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(
 // CTAs per SM (48 registers, no spills; 1.45 -> 1.40 ms on config 2); the
 // scalar forms keep MinBlocks.
 template <int ORD, int CB, class S, int MODE, class I, int CP>
-__device__ __forceinline__ void lanes_push_point(const PPArgs& a, const int64_t t, const int q) {
+__global__ void __launch_bounds__(PP_THREADS, (CP > 0 ? 5 : MinBlocks<MODE>::value)) pp_lanes_kernel(const PPArgs a) {
   using T = typename Acc<S>::type;
   constexpr int NT = Taps<ORD>::value;
+  constexpr int PPB = PP_THREADS / NT;  // sampling points per CTA
+  const int q = static_cast<int>(threadIdx.x) % NT;
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
+  if (t >= a.nvox) return;
   I v = a.perm != nullptr ? static_cast<I>(__ldg(a.perm + t)) : static_cast<I>(t);
   I sub[3];
   sub[2] = v % static_cast<I>(a.trgt_size[2]); v /= static_cast<I>(a.trgt_size[2]);
@@ -1076,15 +1080,6 @@ __device__ __forceinline__ void lanes_push_point(const PPArgs& a, const int64_t 
   }
 }
 
-template <int ORD, int CB, class S, int MODE, class I, int CP>
-__global__ void __launch_bounds__(PP_THREADS, (CP > 0 ? 5 : MinBlocks<MODE>::value)) pp_lanes_kernel(const PPArgs a) {
-  constexpr int NT = Taps<ORD>::value;
-  constexpr int PPB = PP_THREADS / NT;  // sampling points per CTA
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
-  if (t >= a.nvox) return;
-  lanes_push_point<ORD, CB, S, MODE, I, CP>(a, t, static_cast<int>(threadIdx.x) % NT);
-}
-
 // Pull backward (K_PUSHGRAD) with the last axis' taps spread over lanes
 // (3-D, orders 1 and 3, float arithmetic, channel-interleaved float
 // accumulator for the image gradient: flag F_VEC, C <= CP).  NT consecutive
@@ -1101,10 +1096,13 @@ __global__ void __launch_bounds__(PP_THREADS, (CP > 0 ? 5 : MinBlocks<MODE>::val
 // Four CTAs per SM (64 registers): the gathers' latency is the main stall,
 // and 32 warps per SM hide it better than 24 (2.50 -> 2.37 ms on config 2).
 template <int ORD, class S, class I, int CP>
-__device__ __forceinline__ void lanes_pullbwd_point(const PPArgs& a, const int64_t t, const int q) {
+__global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const PPArgs a) {
   using T = float;
   constexpr int NT = Taps<ORD>::value;
-  // the point's lane group: NT consecutive threads, aligned to NT in the warp
+  constexpr int PPB = PP_THREADS / NT;
+  const int q = static_cast<int>(threadIdx.x) % NT;
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
+  if (t >= a.nvox) return;  // whole lane groups (t is per group)
   const unsigned lanes = ((1u << NT) - 1u) << ((threadIdx.x & 31u) & ~static_cast<unsigned>(NT - 1));
   I v = a.perm != nullptr ? static_cast<I>(__ldg(a.perm + t)) : static_cast<I>(t);
   I sub[3];
@@ -1206,15 +1204,6 @@ __device__ __forceinline__ void lanes_pullbwd_point(const PPArgs& a, const int64
       g[0] = og0; g[a.gg_sD] = og1; g[2 * a.gg_sD] = og2;
     }
   }
-}
-
-template <int ORD, class S, class I, int CP>
-__global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const PPArgs a) {
-  constexpr int NT = Taps<ORD>::value;
-  constexpr int PPB = PP_THREADS / NT;
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
-  if (t >= a.nvox) return;  // whole lane groups (t is per group)
-  lanes_pullbwd_point<ORD, S, I, CP>(a, t, static_cast<int>(threadIdx.x) % NT);
 }
 
 // The lane-split push applies to 3-D push / count at orders 1 and 3.
