@@ -1095,11 +1095,13 @@ __global__ void __launch_bounds__(PP_THREADS, (CP > 0 ? 5 : MinBlocks<MODE>::val
 // point's first and last shuffle): a missing tap contributes zero instead.
 // Four CTAs per SM (64 registers): the gathers' latency is the main stall,
 // and 32 warps per SM hide it better than 24 (2.50 -> 2.37 ms on config 2).
-template <int ORD, class S, class I, int CP>
+template <int ORD, class S, class I, int CP, int CB>
 __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const PPArgs a) {
   using T = float;
   constexpr int NT = Taps<ORD>::value;
   constexpr int PPB = PP_THREADS / NT;
+  constexpr int NC = CP > 0 ? CP : CB;  // channel slots: vector width, or the channel block
+  const bool self = (a.flags & F_ADDSELF) != 0;  // self-composition (C = 3, grid = displacement)
   const int q = static_cast<int>(threadIdx.x) % NT;
   const int64_t t = static_cast<int64_t>(blockIdx.x) * PPB + static_cast<int64_t>(threadIdx.x) / NT;
   if (t >= a.nvox) return;  // whole lane groups (t is per group)
@@ -1122,6 +1124,18 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
   T coord[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) coord[d] = __ldg(gp + d * a.grid_sD);
+  if (a.flags & F_IDGRID) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) coord[d] += static_cast<T>(sub[d]);
+  }
+  // the point's own voxel in `out` (self-composition terms)
+  T* self_out = nullptr;
+  if (self) {
+    int64_t oo = static_cast<int64_t>(n) * a.out_sN;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) oo += static_cast<int64_t>(sub[d]) * a.out_s[d];
+    self_out = static_cast<T*>(a.out) + oo;
+  }
   const bool do_a = (a.flags & F_A) != 0;
   const bool do_grad = (a.flags & F_GRAD) != 0;
   {
@@ -1130,7 +1144,13 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
 #pragma unroll
     for (int d = 0; d < 3; ++d) inb = inb && in_fov<T>(coord[d], a.src_size[d], tol);
     if (!((a.extrapolate & 1) || inb)) {  // the whole group: zero grid gradient, no push
-      if (do_grad && q == 0) {
+      if (self) {  // only the identity terms: g at the point
+        if (q == 0) {
+          const S* tp = static_cast<const S*>(a.trgt) + tvox;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) atomic_acc(self_out + d * a.out_sC, ldg_acc(tp + d * a.trgt_sC));
+        }
+      } else if (do_grad && q == 0) {
         T* g = static_cast<T*>(a.gg) + gvox;
         g[0] = T(0); g[a.gg_sD] = T(0); g[2 * a.gg_sD] = T(0);
       }
@@ -1155,9 +1175,9 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
   const S* trg_v = static_cast<const S*>(a.trgt) + tvox;
   const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(n) * a.src_sN;
   float* acc_n = static_cast<float*>(a.out) + static_cast<int64_t>(n) * a.out_sN;
-  float tv[CP];
+  float tv[NC];
 #pragma unroll
-  for (int c = 0; c < CP; ++c) tv[c] = c < a.C ? static_cast<float>(ldg_acc(trg_v + c * a.trgt_sC)) : 0.f;
+  for (int c = 0; c < NC; ++c) tv[c] = c < a.C ? static_cast<float>(ldg_acc(trg_v + c * a.trgt_sC)) : 0.f;
   T og0 = T(0), og1 = T(0), og2 = T(0);
   if (vz) {
 #pragma unroll
@@ -1172,7 +1192,7 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
           const S* sp = src_n + (ax.os[i] + osyz);
           T dot = T(0);
 #pragma unroll
-          for (int c = 0; c < CP; ++c)
+          for (int c = 0; c < NC; ++c)
             if (c < a.C) dot = fma(tv[c], ldg_acc(sp + c * a.src_sC), dot);
           sx = fma(ax.w[i], dot, sx);
           dx = fma(ax.g[i], dot, dx);
@@ -1180,10 +1200,16 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
         if (do_a) {
           const float wt = ax.w[i] * ay.w[j] * wz;
           if (wt != 0.f) {
-            float vals[CP];
+            if constexpr (CP > 0) {
+              float vals[CP];
 #pragma unroll
-            for (int c = 0; c < CP; ++c) vals[c] = wt * tv[c];
-            red_vec<CP>(acc_n + (ax.oo[i] + ooyz), vals);
+              for (int c = 0; c < CP; ++c) vals[c] = wt * tv[c];
+              red_vec<CP>(acc_n + (ax.oo[i] + ooyz), vals);
+            } else {
+#pragma unroll
+              for (int c = 0; c < NC; ++c)
+                if (c < a.C) atomic_acc(acc_n + (c * a.out_sC + (ax.oo[i] + ooyz)), wt * tv[c]);
+            }
           }
         }
       }
@@ -1200,8 +1226,16 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
       og2 += __shfl_xor_sync(lanes, og2, o);
     }
     if (q == 0) {
-      T* g = static_cast<T*>(a.gg) + gvox;
-      g[0] = og0; g[a.gg_sD] = og1; g[2 * a.gg_sD] = og2;
+      if (self) {
+        // self-composition backward: g and the grid gradient at the point go
+        // to the same output as the push, atomically
+        const T og[3] = {og0, og1, og2};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) atomic_acc(self_out + d * a.out_sC, og[d] + ldg_acc(trg_v + d * a.trgt_sC));
+      } else {
+        T* g = static_cast<T*>(a.gg) + gvox;
+        g[0] = og0; g[a.gg_sD] = og1; g[2 * a.gg_sD] = og2;
+      }
     }
   }
 }
@@ -1215,16 +1249,27 @@ bool lanes_enabled();  // host switch (pp_capi.cu), on unless PP_PUSH_LANES=0
 template <int D, int ORD, int CB, class S, int MODE, class I>
 inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
   if (a.nvox == 0) return cudaSuccess;
-  if constexpr (D == 3 && (ORD == 1 || ORD == 3) && MODE == K_PUSHGRAD && CB >= 2 &&
+  if constexpr (D == 3 && (ORD == 1 || ORD == 3) && MODE == K_PUSHGRAD &&
                 std::is_same<typename Acc<S>::type, float>::value) {
-    // pull backward into the interleaved accumulator: lane-split kernel
-    if (lanes_enabled() && (a.flags & F_VEC) && a.det_acc == nullptr &&
-        !(a.flags & (F_IDGRID | F_ADDSELF | F_AFFINE | F_NOTRGT))) {
-      constexpr int PPB = PP_THREADS / Taps<ORD>::value;
-      const int64_t nb = (a.nvox + PPB - 1) / PPB;
-      if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-      pp_lanes_pullbwd_kernel<ORD, S, I, (CB == 2 ? 2 : 4)><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
-      return cudaGetLastError();
+    constexpr int PPB = PP_THREADS / Taps<ORD>::value;
+    const int64_t nb = (a.nvox + PPB - 1) / PPB;
+    if (lanes_enabled() && a.det_acc == nullptr && !(a.flags & (F_AFFINE | F_NOTRGT)) && nb <= 0x7fffffffLL) {
+      // pull backward into the interleaved accumulator: lane-split kernel
+      if constexpr (CB >= 2) {
+        if ((a.flags & F_VEC) && !(a.flags & (F_IDGRID | F_ADDSELF))) {
+          pp_lanes_pullbwd_kernel<ORD, S, I, (CB == 2 ? 2 : 4), CB>
+              <<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
+          return cudaGetLastError();
+        }
+      }
+      // linear self-composition backward (velocity exponentiation):
+      // lane-split with scalar reductions into the field
+      if constexpr (ORD == 1 && CB == 3) {
+        if (!(a.flags & F_VEC) && (a.flags & F_IDGRID) && (a.flags & F_ADDSELF)) {
+          pp_lanes_pullbwd_kernel<ORD, S, I, 0, CB><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
+          return cudaGetLastError();
+        }
+      }
     }
   }
   if constexpr (UseLanes<D, ORD, MODE>::value) {
