@@ -910,7 +910,7 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
 }
 
 template <int D, int ORD, int CB, class S, int MODE, class I>
-__global__ void __launch_bounds__(PP_THREADS, MinBlocks<MODE>::value) pp_kernel(const PPArgs a) {
+__global__ void __launch_bounds__(PP_THREADS, (MODE == K_PUSHGRAD && CB == 1 && D == 3 && ORD >= 2 && ORD <= 3) ? 3 : MinBlocks<MODE>::value) pp_kernel(const PPArgs a) {
   // ---- sampling point (n, x, y, z) -------------------------------------
   I sub[3] = {0, 0, 0};
   I n = 0;
