@@ -97,11 +97,18 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         self.fh.close()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
             lines = f.readlines()
-        during = lines[getattr(self, "skip", 0):] or lines[-1:]
+        return self.parse(lines, getattr(self, "skip", 0))
+
+    @staticmethod
+    def parse(lines, skip=0):
+        """Median SM clock, max clock and active throttle reasons of the
+        samples after the first `skip` lines (taken before the timed region;
+        the last line stands in if none came after)."""
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        during = lines[skip:] or lines[-1:]
         for line in during:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
