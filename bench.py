@@ -13,13 +13,14 @@ Metric: output-grid voxels per second (Gvox/s) of that step.
 --impl b200 (default) prints one JSON line with the device-timed value, the
 end-to-end value through the public API with host buffers (`e2e`), the
 roofline of the dominant kernel, the CPU baseline (the reference's own C++
-backend on a bounded sample), clocks and kernel-launch counts; `fused`
-reports the same step through the fused pull_push operator, and `batched`
-the config-4 workload (64 uneven volumes, float32 and bfloat16) as one
-captured batched step against the per-call loop; `svf` times config-5
+backend on the full workload), `reference_cuda` (the reference's own CUDA
+kernels on the same chain and inputs), clocks and kernel-launch counts;
+`fused` reports the same step through the fused pull_push operator, and
+`batched` the config-4 workload (64 uneven volumes, float32 and bfloat16) as
+one captured batched step against the per-call loop; `svf` times config-5
 registration iterations (velocity exponentiation, warp, MSE, backward).
 --impl reference times the reference's CPU implementation of the same step
-on the host cores (bounded sample) and prints the same metric.
+(full size) on the host cores and prints the same metric.
 With N > 1 (torchrun), every rank runs an independent replica of the
 single-volume step (it does not shard; "replicas only"); value = all ranks'
 voxels / max-over-ranks time.  The batched volumes are sharded over the
@@ -30,6 +31,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -62,12 +64,12 @@ class ClockSampler:
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix="clocks_bench_", suffix=".csv")
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "50"],
@@ -99,6 +101,7 @@ class ClockSampler:
         self.fh.close()
         with open(self.path) as f:
             lines = f.readlines()
+        os.unlink(self.path)
         return self.parse(lines, getattr(self, "skip", 0))
 
     @staticmethod
@@ -141,6 +144,7 @@ class OpTimer:
     def __init__(self, labels=None):
         self.labels = labels or self.CHAIN
         self.events = {}
+        self.kernels = {}
         self.enabled = False
         self._orig = []
 
@@ -166,6 +170,8 @@ class OpTimer:
             out = fn(*a, **k)
             e.record()
             self.events.setdefault(label, []).append((s, e))
+            from nitorch_b200 import _lib
+            self.kernels[label] = _lib.last_kernel()
             return out
         return inner
 
@@ -173,7 +179,8 @@ class OpTimer:
         out = {}
         for label, evs in self.events.items():
             ms = [s.elapsed_time(e) for s, e in evs]
-            out[label] = {"launches": len(ms), "avg_ms": float(np.mean(ms)), "total_ms": float(np.sum(ms))}
+            out[label] = {"launches": len(ms), "avg_ms": float(np.mean(ms)), "total_ms": float(np.sum(ms)),
+                          "kernel": self.kernels.get(label, "")}
         return out
 
 
@@ -265,34 +272,34 @@ def timed_steps(fn, args, world, device, l2buf, timer=None, clocks=None, steps=N
     return total_ms, launches, clk
 
 
-# Ceiling of the scatter kernels: float reductions (RED) per second that this
-# GPU's atomic path sustains when fully coalesced, measured on B200 with
-# tests/perf_atomic_throughput.py (1.46 T scalar adds/s; vector forms 1.6 T).
+# Ceiling of the per-tap scatter kernels: float reductions (RED) per second
+# that this GPU's atomic path sustains when fully coalesced (1.46 T scalar
+# adds/s, vector forms 1.6 T; measured on B200 with a reduction probe).
 ATOMIC_ADDS_PER_S = 1.46e12
 HBM_SPEC_GBS = 8000.0  # B200 HBM3e specification (the measured copy bandwidth is the roofline)
 SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# dominant kernel on this workload (config 2: 1x3x192^3, cubic, dct2,
-# source-sorted order), from one ncu capture of the same kernel.
-MEASURED_TRAFFIC = {
-    "pull_bwd": (396.5e6 + 168.6e6, "ncu capture of pp_lanes_pullbwd_kernel, "
-                 "profiles/pp_lanes_pullbwd_cubic_c3_192_sorted_order.md"),
-}
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a
+# kernel on the default workload (1x3x192^3, cubic, dct2, brick-major
+# order), from one ncu capture of that kernel, keyed by the kernel family /
+# mode / order / channel block that pp_last_kernel reports.  A kernel not
+# listed here reports traffic null.
+MEASURED_TRAFFIC = {}
 
 
 def roofline(ops, labels, nvox, C, ms_per_step, traffic):
     hbm, src = peaks()
     dom = max(ops, key=lambda k: ops[k]["total_ms"])
+    kernel = ops[dom].get("kernel", "")
     traffic_src = "--traffic" if traffic is not None else None
-    if traffic is None and dom in MEASURED_TRAFFIC and nvox == 192 ** 3 and C == 3:
-        traffic, traffic_src = MEASURED_TRAFFIC[dom]
+    if traffic is None and kernel in MEASURED_TRAFFIC and nvox == 192 ** 3 and C == 3:
+        traffic, traffic_src = MEASURED_TRAFFIC[kernel], f"ncu capture of {kernel} on this workload"
     per = algo_bytes(dom, 4, C) * nvox
     achieved = per / (ops[dom]["avg_ms"] * 1e-3) / 1e9
     step_bytes = sum(algo_bytes(k, 4, C) for k in labels) * nvox
     step_gbs = step_bytes / (ms_per_step * 1e-3) / 1e9
-    out = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm,
+    out = {"bound": "hbm", "op": dom, "kernel": kernel, "achieved": round(achieved, 1), "peak": hbm,
            "unit": "GB/s", "frac": round(achieved / hbm, 4), "peak_source": src,
            "algorithmic_bytes_per_launch": per, "traffic": traffic, "traffic_source": traffic_src,
            "step_frac": round(step_gbs / hbm, 4),
@@ -300,13 +307,14 @@ def roofline(ops, labels, nvox, C, ms_per_step, traffic):
            "spec_gbs": HBM_SPEC_GBS, "frac_of_spec": round(achieved / HBM_SPEC_GBS, 4),
            "step_frac_of_spec": round(step_gbs / HBM_SPEC_GBS, 4)}
     if dom in SCATTER_OPS:
-        # the binding resource of a scatter: 64 taps x C channels float adds per point (cubic 3-D)
+        # the scatter's tap additions (64 taps x C channels per point, cubic
+        # 3-D) against the ceiling of one global reduction per tap
         adds = 64 * C * nvox
         rate = adds / (ops[dom]["avg_ms"] * 1e-3)
         out["atomic"] = {"adds_per_launch": adds, "achieved_adds_per_s": round(rate / 1e9, 1),
                          "ceiling_adds_per_s": ATOMIC_ADDS_PER_S / 1e9, "unit": "G adds/s",
                          "frac": round(rate / ATOMIC_ADDS_PER_S, 3),
-                         "ceiling_source": "measured on B200 by tests/perf_atomic_throughput.py"}
+                         "ceiling_source": "coalesced global float reductions measured on B200"}
     return out
 
 
@@ -426,8 +434,10 @@ def run_b200(args, rank, world, device):
                   **{k: fused[k] for k in ("value", "ms_per_step", "e2e", "roofline", "ops", "gpu_launches",
                                            "gpu_launches_per_step")}},
     }
+    if not args.no_reference_cuda and world == 1:
+        line["reference_cuda"] = reference_cuda_leg(args, device, x, grid, w, chain["ms_per_step"])
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_size, steps=2, warmup=1)
+        line["cpu_baseline"] = cpu_baseline(args.cpu_size or size, steps=1, warmup=1)
     return line
 
 
@@ -604,10 +614,12 @@ def run_all(args, rank, world, device):
 # ---------------------------------------------------------------------- #
 def reference_step_fn():
     """The step through the reference's own compiled CPU backend (its native
-    API: the functions GridPull / GridPush call) with the prefilter from the
-    CPU oracle port (the reference's prefilter lives in a third-party Python
-    package that is not present on the benchmark host)."""
-    from oracle import oracle as O
+    API: the functions GridPull / GridPush call).  The prefilter -- in the
+    reference a third-party Python package that is not present on the
+    benchmark host -- is the oracle's restatement of it, vectorised over
+    lines with torch CPU operations in float32 as the reference's own runs
+    (0.33 s for 3x192^3 on 8 cores against the reference's 0.325 s)."""
+    from oracle import prefilter_torch as P
     from oracle import reference as R
     ref = R.load_compiled()
     if ref is None:
@@ -615,7 +627,7 @@ def reference_step_fn():
     b, o = [ref.BoundType.dct2], [ref.InterpolationType.cubic]
 
     def prefilter(a):
-        return torch.from_numpy(O.spline_coeff_nd(a.numpy(), [3], [3], dim=3).astype(np.float32))
+        return P.spline_coeff_nd(a, [3], [3], 3)
 
     def run(x, grid, w):
         c = prefilter(x)
@@ -632,7 +644,14 @@ def reference_step_fn():
     return run, "reference"
 
 
-def cpu_baseline(size, steps=2, warmup=1):
+CPU_SAMPLE = ("1x3x{size}^3 float32, the same chain (prefilter -> pull -> push -> <z,w> -> backward to the "
+              "image and the grid); pull / push and their backward passes through the reference's compiled "
+              "C++ CPU backend, prefilter through the oracle's line-vectorised torch restatement")
+
+
+def cpu_baseline(size, steps=1, warmup=1):
+    """The reference's CPU implementation of the step on the host cores (all
+    threads), full size: one warm-up and `steps` timed steps."""
     torch.set_num_threads(os.cpu_count() or 1)
     x, grid, w, _ = make_inputs(size, 3, torch.device("cpu"))
     run, kind = reference_step_fn()
@@ -646,16 +665,75 @@ def cpu_baseline(size, steps=2, warmup=1):
         run(x, grid, w)
     dt = (time.perf_counter() - t0) / steps
     return {"value": round(size ** 3 / dt / 1e9, 6), "unit": "Gvox/s", "cores": torch.get_num_threads(),
-            "kind": kind,
-            "sample": f"1x3x{size}^3 (1/{(192 // size) ** 3} of the 192^3 voxels), same chain, "
-                      f"{steps} steps after {warmup} warm-up; pull/push via the reference's compiled "
-                      "C++ CPU backend, prefilter via the CPU oracle port", "sec_per_step": round(dt, 4)}
+            "kind": kind, "sample": CPU_SAMPLE.format(size=size) + f"; {steps} step(s) after {warmup} warm-up",
+            "sec_per_step": round(dt, 4)}
+
+
+def reference_cuda_leg(args, device, x, grid, w, ours_ms):
+    """The reference's own CUDA push/pull kernels (nitorch's CUDA backend,
+    compiled for sm_100a from its sources into oracle/_ref/cuda) timed on the
+    same inputs and chain as the headline step, with the same CUDA events and
+    L2 flush: the GPU implementation this library replaces.  Its prefilter
+    is this library's (the reference's prefilter is a third-party package
+    that is not present); the rest runs through the reference's native
+    functions with the requires_grad wiring of nitorch/_C/grid.py.  Also
+    reports the largest relative difference of the outputs."""
+    from oracle import reference as R
+    ref = R.load_compiled_cuda()
+    if ref is None:
+        return {"unavailable": "reference CUDA backend not built (oracle/build_ref_cuda.py)"}
+    import nitorch_b200 as nb
+    b, o = [ref.BoundType.dct2], [ref.InterpolationType.cubic]
+    l2buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def chain():
+        c = nb.spline_coeff_nd(x.detach(), ORDER, BOUND, dim=3)
+        y = ref.grid_pull(c, grid.detach(), b, o, 0)
+        z = ref.grid_push(y, grid.detach(), list(x.shape[2:]), b, o, 0)
+        loss = (z * w).sum()
+        yr = y.detach().requires_grad_(True)
+        gr = grid.detach().requires_grad_(True)
+        dy, dg1 = ref.grid_push_backward(w, yr, gr, b, o, 0)
+        cr = c.detach().requires_grad_(True)
+        dc, dg2 = ref.grid_pull_backward(dy, cr, gr, b, o, 0)
+        dx = nb.spline_coeff_nd(dc, ORDER, BOUND, dim=3)
+        return z, dx, dg1 + dg2, loss
+
+    for _ in range(max(1, min(args.warmup, 3))):
+        chain()
+    torch.cuda.synchronize()
+    steps = max(1, min(args.steps, 5))
+    ts = []
+    for _ in range(steps):
+        l2buf.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        out = chain()
+        e.record()
+        torch.cuda.synchronize()
+        ts.append(s.elapsed_time(e))
+    ms = float(np.mean(ts))
+    # this library's outputs on the same inputs
+    xr = x.detach().requires_grad_(True)
+    gr = grid.detach().requires_grad_(True)
+    z = nb.grid_push(nb.grid_pull(xr, gr, ORDER, BOUND, EXTRAP, prefilter=True), gr, None, ORDER, BOUND, EXTRAP)
+    (z * w).sum().backward()
+    diff = {}
+    for k, a_, r_ in (("push", z, out[0]), ("dx", xr.grad, out[1]), ("dgrid", gr.grad, out[2])):
+        a_, r_ = a_.detach().double(), r_.detach().double()
+        diff[k] = float((a_ - r_).abs().max() / r_.abs().max().clamp_min(1e-30))
+    nvox = int(np.prod(x.shape[2:]))
+    return {"ms_per_step": round(ms, 4), "value": round(nvox / (ms * 1e-3) / 1e9, 4), "unit": "Gvox/s",
+            "steps": steps, "speedup_of_this_library": round(ms / ours_ms, 2),
+            "max_rel_diff_vs_this_library": diff,
+            "note": "nitorch's CUDA pushpull_kernel built for sm_100a from the reference sources; "
+                    "prefilter from this library"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    size = args.cpu_size
+    size = args.cpu_size or args.size
     torch.set_num_threads(os.cpu_count() or 1)
     x, grid, w, _ = make_inputs(size, 3, torch.device("cpu"))
     run, kind = reference_step_fn()
@@ -668,14 +746,12 @@ def run_reference(args, rank, world):
         run(x, grid, w)
     total = time.perf_counter() - t0
     value = size ** 3 * args.steps / total / 1e9
-    sample = (f"1x3x{size}^3 bounded sample of the 1x3x192^3 workload per step, "
-              f"{torch.get_num_threads()} threads; reference compiled C++ CPU backend "
-              "(prefilter via the CPU oracle port)")
+    sample = CPU_SAMPLE.format(size=size) + f"; {torch.get_num_threads()} threads"
     return {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Gvox/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "1x3x192^3 order-3 dct2 prefilter pull+push fwd+bwd (cfg2)",
+            "config": {"workload": f"1x3x{args.size}^3 order-3 dct2 prefilter pull+push fwd+bwd (cfg2)",
                        "sample_size": size},
             "cpu_baseline": {"value": round(value, 6), "unit": "Gvox/s", "cores": torch.get_num_threads(),
                              "kind": kind, "sample": sample},
@@ -690,7 +766,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=192)
-    ap.add_argument("--cpu-size", type=int, default=96)
+    ap.add_argument("--cpu-size", type=int, default=None,
+                    help="spatial size of the CPU baseline (default: the workload's own)")
+    ap.add_argument("--no-reference-cuda", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-volumes", type=int, default=64)

@@ -93,6 +93,13 @@ typedef struct pp_options {
                                     from pp_sample_order); NULL = natural.
                                     Results do not depend on it beyond
                                     floating-point summation order.        */
+  const int32_t* brick_start;    /* optional device array, 3-D grids only:
+                                    with sample_order from pp_brick_order,
+                                    its brick offsets (N * nbricks + 1
+                                    entries).  Lets the cubic scatters
+                                    accumulate each brick of the scatter
+                                    target in on-chip memory.  NULL = no
+                                    brick pass.                           */
 } pp_options;
 
 /* Version of this ABI (major * 100 + minor). */
@@ -104,6 +111,11 @@ PP_API const char* pp_last_error(void);
 /* Number of kernels this library has launched since it was loaded (all
  * threads and devices); for auditing what ran on the GPU. */
 PP_API unsigned long long pp_kernel_launches(void);
+
+/* Kernel family, mode, order and channel block of the last push/pull
+ * launch made on this host thread, e.g. "pp_brick_kernel mode=5 order=3
+ * cb=3" ("" if none); for auditing which code path a call took. */
+PP_API const char* pp_last_kernel(void);
 
 /* Workspace (device bytes, 256-byte aligned) that a push-type call with
  * output `out` needs: 0 for float32 / float64 outputs without
@@ -250,6 +262,25 @@ PP_API int pp_jacobian_det(const pp_tensor* jac, const pp_tensor* det, const pp_
 PP_API size_t pp_sample_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size);
 PP_API int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* Brick-major processing order (no counterpart in the reference; a
+ * scheduling aid for the cubic 3-D scatters).  The source volume (spatial
+ * size `src_size`, 3 entries) is cut into bricks of PP_BRICK_X x PP_BRICK_Y
+ * x PP_BRICK_Z voxels, nb = prod(ceil(src_size / brick)) per batch item.
+ * Writes to `perm` (int32, N*prod(grid spatial) entries) the sample
+ * indices sorted by (batch item, brick, voxel in brick) of the source voxel
+ * floor(coordinate) they fall in (clamped into the volume), and to
+ * `brick_start` (int32, N*nb + 1 entries) where each brick's samples start
+ * in `perm` (the last entry is the number of samples).  Pass both in
+ * pp_options.  3-D grids only; needs pp_brick_order_workspace_bytes()
+ * bytes of device workspace.  pp_brick_count() gives N*nb. */
+#define PP_BRICK_X 4
+#define PP_BRICK_Y 4
+#define PP_BRICK_Z 6
+PP_API int64_t pp_brick_count(const pp_tensor* grid, const int64_t* src_size);
+PP_API size_t pp_brick_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size);
+PP_API int pp_brick_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
+                          int32_t* brick_start, void* workspace, size_t workspace_bytes, void* stream);
 
 /* pp_sample_order without any device allocation or caller workspace (no
  * counterpart in the reference).  For callers that cannot allocate device

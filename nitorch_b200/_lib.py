@@ -52,6 +52,7 @@ class PPOptions(ctypes.Structure):
         ("extrapolate", ctypes.c_int32),
         ("flags", ctypes.c_int32),
         ("sample_order", ctypes.c_void_p),
+        ("brick_start", ctypes.c_void_p),
     ]
 
 
@@ -63,12 +64,13 @@ class PPBatchEntry(ctypes.Structure):
 
 
 EXPORTS = (
-    "pp_abi_version", "pp_last_error", "pp_kernel_launches", "pp_push_workspace_bytes",
+    "pp_abi_version", "pp_last_error", "pp_kernel_launches", "pp_last_kernel", "pp_push_workspace_bytes",
     "pp_grid_pull", "pp_grid_pull_backward", "pp_grid_push",
     "pp_grid_push_backward", "pp_grid_count", "pp_grid_count_backward",
     "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
     "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
-    "pp_sample_order_noalloc", "pp_grid_pull_push", "pp_grid_pull_push_backward",
+    "pp_sample_order_noalloc", "pp_brick_count", "pp_brick_order_workspace_bytes", "pp_brick_order",
+    "pp_grid_pull_push", "pp_grid_pull_push_backward",
     "pp_batch_plan_bytes", "pp_batch_scratch_bytes", "pp_batch_plan", "pp_batch_run",
     "pp_svf_compose", "pp_svf_compose_backward", "pp_affine_pull", "pp_affine_push",
     "pp_affine_grad_workspace_bytes", "pp_affine_grad_matrix",
@@ -87,6 +89,7 @@ def _declare(L):
     vp, sz = ctypes.c_void_p, ctypes.c_size_t
     L.pp_abi_version.restype = ctypes.c_int
     L.pp_last_error.restype = ctypes.c_char_p
+    L.pp_last_kernel.restype = ctypes.c_char_p
     L.pp_kernel_launches.restype = ctypes.c_ulonglong
     L.pp_push_workspace_bytes.argtypes = [T, ctypes.c_int32]
     L.pp_push_workspace_bytes.restype = sz
@@ -128,10 +131,15 @@ def _declare(L):
     L.pp_sample_order_workspace_bytes.restype = sz
     L.pp_sample_order.argtypes = [T, I64P, vp, vp, sz, vp]
     L.pp_sample_order_noalloc.argtypes = [T, I64P, vp, vp]
+    L.pp_brick_count.argtypes = [T, I64P]
+    L.pp_brick_count.restype = ctypes.c_int64
+    L.pp_brick_order_workspace_bytes.argtypes = [T, I64P]
+    L.pp_brick_order_workspace_bytes.restype = sz
+    L.pp_brick_order.argtypes = [T, I64P, vp, vp, vp, sz, vp]
     for name in EXPORTS:
-        if name not in ("pp_last_error", "pp_push_workspace_bytes", "pp_kernel_launches",
+        if name not in ("pp_last_error", "pp_last_kernel", "pp_push_workspace_bytes", "pp_kernel_launches",
                         "pp_sample_order_workspace_bytes", "pp_batch_plan_bytes", "pp_batch_scratch_bytes",
-                        "pp_affine_grad_workspace_bytes"):
+                        "pp_affine_grad_workspace_bytes", "pp_brick_count", "pp_brick_order_workspace_bytes"):
             getattr(L, name).restype = ctypes.c_int
     return L
 
@@ -151,6 +159,12 @@ def load():
 def kernel_launches():
     """Kernels launched by the library so far (process-wide counter)."""
     return int(load().pp_kernel_launches())
+
+
+def last_kernel():
+    """Kernel family / mode / order / channel block of the last push/pull
+    launch on this thread (see pp_last_kernel)."""
+    return load().pp_last_kernel().decode()
 
 
 def check(rc):
@@ -184,9 +198,10 @@ def ref(d):
     return None if d is None else ctypes.byref(d)
 
 
-def options(bound, order, extrapolate, flags=0, sample_order=None):
+def options(bound, order, extrapolate, flags=0, sample_order=None, brick_start=None):
     o = PPOptions()
     o.sample_order = sample_order
+    o.brick_start = brick_start
     b = [int(x) for x in bound][:3]
     i = [int(x) for x in order][:3]
     o.nbound = len(b)

@@ -4,8 +4,8 @@ Same signatures, defaults, broadcasting and output shapes as
 ``nitorch/spatial/_grid.py``:
   grid_pull (146-205), grid_push (208-251), grid_count (254-287),
   grid_grad (290-328), spline_coeff (331-375), spline_coeff_nd (378-421),
-  identity_grid (443-478), with the pre/post-processing of _preproc /
-  _postproc (90-143) and the soft label-map pull (187-198).
+  identity_grid (443-478); the broadcasting of leading dimensions and the
+  label-map pull follow the behaviour of _grid.py:90-143 and 187-198.
 """
 import torch
 
@@ -13,52 +13,72 @@ from .affine import affine_pull, affine_push
 from .grid import GridCount, GridGrad, GridPull, GridPullPush, GridPush, SplineCoeff, SplineCoeffND
 
 
-def _expanded_shape(*shapes):
-    return list(torch.broadcast_shapes(*[tuple(s) for s in shapes]))
+class _Layout:
+    """How a caller's tensors fold into the kernels' layout and back.
+
+    The kernels take images as (B, C, *spatial) and grids as (B, *spatial, D).
+    Callers may add any number of leading batch dimensions to either tensor
+    (broadcast against each other) and may leave the channel dimension out.
+    ``lead`` holds the broadcast leading dimensions (flattened into B) and
+    ``chan`` the channel dimensions the result gets back: the image's
+    channel size when it has one, a singleton when it has none but there
+    are leading dimensions, nothing otherwise."""
+
+    __slots__ = ("lead", "chan", "dim")
+
+    def __init__(self, lead, chan, dim):
+        self.lead = tuple(lead)
+        self.chan = tuple(chan)
+        self.dim = dim
+
+    def restore(self, out):
+        """(B, C, *rest) kernel output -> (*lead, *chan, *rest)."""
+        return out.reshape(*self.lead, *self.chan, *out.shape[2:])
 
 
-def _preproc(grid, input=None, mode=None):
-    """Broadcast and reshape to (B, C, *spatial) / (B, *spatial, D)
-    (_grid.py:90-127).  This *can* allocate (expand + reshape)."""
+def _fold(grid, image=None, shared_space=False):
+    """Fold ``grid`` (*g_lead, *g_space, D) and ``image``
+    (*i_lead, [C], *i_space) into kernel layout.  An image with exactly D
+    dimensions has no channel; with more, dimension -D-1 is the channel.
+    ``shared_space`` (push) broadcasts the two spatial shapes together as
+    well.  Expanding can allocate when the reshape cannot view."""
     dim = grid.shape[-1]
-    if input is None:
-        spatial = grid.shape[-dim - 1:-1]
-        batch = grid.shape[:-dim - 1]
-        grid = grid.reshape([-1, *spatial, dim])
-        info = dict(batch=batch, channel=[1] if batch else [], dim=dim)
-        return grid, info
-
-    grid_spatial = grid.shape[-dim - 1:-1]
-    grid_batch = grid.shape[:-dim - 1]
-    input_spatial = input.shape[-dim:]
-    channel = 0 if input.dim() == dim else input.shape[-dim - 1]
-    input_batch = input.shape[:-dim - 1]
-
-    if mode == "push":
-        grid_spatial = input_spatial = _expanded_shape(grid_spatial, input_spatial)
-
-    batch = _expanded_shape(grid_batch, input_batch)
-    grid = grid.expand([*batch, *grid_spatial, dim])
-    grid = grid.reshape([-1, *grid_spatial, dim])
-    input = input.expand([*batch, channel or 1, *input_spatial])
-    input = input.reshape([-1, channel or 1, *input_spatial])
-
-    out_channel = [channel] if channel else ([1] if batch else [])
-    info = dict(batch=batch, channel=out_channel, dim=dim)
-    return grid, input, info
+    g_lead, g_space = grid.shape[:-dim - 1], grid.shape[-dim - 1:-1]
+    if image is None:
+        layout = _Layout(g_lead, (1,) if len(g_lead) else (), dim)
+        return grid.reshape(-1, *g_space, dim), None, layout
+    has_chan = image.dim() > dim
+    nchan = image.shape[-dim - 1] if has_chan else 0
+    i_lead = image.shape[:-dim - 1] if has_chan else ()
+    i_space = image.shape[-dim:]
+    if shared_space:
+        g_space = i_space = torch.broadcast_shapes(g_space, i_space)
+    lead = torch.broadcast_shapes(g_lead, i_lead)
+    folded_grid = grid.expand(*lead, *g_space, dim).reshape(-1, *g_space, dim)
+    folded_image = image.expand(*lead, nchan or 1, *i_space).reshape(-1, nchan or 1, *i_space)
+    chan = (nchan,) if nchan else ((1,) if len(lead) else ())
+    return folded_grid, folded_image, _Layout(lead, chan, dim)
 
 
-def _postproc(out, shape_info, mode):
-    dim = shape_info["dim"]
-    if mode != "grad":
-        spatial = out.shape[-dim:]
-        feat = []
-    else:
-        spatial = out.shape[-dim - 1:-1]
-        feat = [out.shape[-1]]
-    batch = shape_info["batch"]
-    channel = shape_info["channel"]
-    return out.reshape([*batch, *channel, *spatial, *feat])
+def _pull_labels(labels, grid, interpolation, bound, extrapolate, prefilter):
+    """Pull of an integer label map: every label is pulled as a 0/1 mask and
+    each output voxel takes the label whose pulled mask is largest.  Masks
+    are visited in increasing label order and a label must beat the best
+    value so far strictly, so ties keep the smaller label and voxels where
+    every mask pulls to zero (or less) get 0."""
+    dim = grid.shape[-1]
+    shape = (labels.shape[0], labels.shape[1], *grid.shape[1:-1])
+    winner = labels.new_zeros(shape)
+    score = grid.new_zeros(shape)
+    for value in torch.unique(labels):
+        mask = (labels == value).to(grid.dtype)
+        if prefilter:
+            mask = spline_coeff_nd(mask, interpolation=interpolation, bound=bound, dim=dim, inplace=True)
+        prob = GridPull.apply(mask, grid, interpolation, bound, extrapolate)
+        better = prob > score
+        winner = torch.where(better, value.to(winner.dtype), winner)
+        score = torch.maximum(score, prob)
+    return winner
 
 
 def grid_pull(input, grid, interpolation="linear", bound="zero", extrapolate=False,
@@ -66,43 +86,28 @@ def grid_pull(input, grid, interpolation="linear", bound="zero", extrapolate=Fal
     """Sample an image at the voxel coordinates of `grid`.
 
     input: (..., [channel], *inshape); grid: (..., *outshape, dim)
-    -> (..., [channel], *outshape).  Integer inputs are label maps: each
-    label is pulled as a soft mask and the arg-max label is returned.
+    -> (..., [channel], *outshape).  Integer inputs are label maps (see
+    _pull_labels).
     """
-    grid, input, shape_info = _preproc(grid, input)
-    batch, channel = input.shape[:2]
-    dim = grid.shape[-1]
-
+    grid, input, layout = _fold(grid, input)
     if not input.dtype.is_floating_point:
-        out = input.new_zeros([batch, channel, *grid.shape[1:-1]])
-        pmax = grid.new_zeros([batch, channel, *grid.shape[1:-1]])
-        for label in input.unique():
-            soft = (input == label).to(grid.dtype)
-            if prefilter:
-                soft = spline_coeff_nd(soft, interpolation=interpolation, bound=bound,
-                                       dim=dim, inplace=True)
-            soft = GridPull.apply(soft, grid, interpolation, bound, extrapolate)
-            out[soft > pmax] = label
-            pmax = torch.max(pmax, soft)
-    else:
-        if prefilter:
-            input = spline_coeff_nd(input, interpolation=interpolation, bound=bound, dim=dim)
-        out = GridPull.apply(input, grid, interpolation, bound, extrapolate)
-    return _postproc(out, shape_info, mode="pull")
+        return layout.restore(_pull_labels(input, grid, interpolation, bound, extrapolate, prefilter))
+    if prefilter:
+        input = spline_coeff_nd(input, interpolation=interpolation, bound=bound, dim=layout.dim)
+    return layout.restore(GridPull.apply(input, grid, interpolation, bound, extrapolate))
 
 
 def grid_push(input, grid, shape=None, interpolation="linear", bound="zero",
               extrapolate=False, prefilter=False):
-    """Splat an image with respect to a deformation field (adjoint of pull)."""
-    grid, input, shape_info = _preproc(grid, input, mode="push")
-    dim = grid.shape[-1]
-    if shape is None:
-        shape = tuple(input.shape[2:])
-    out = GridPush.apply(input, grid, shape, interpolation, bound, extrapolate)
+    """Splat an image with respect to a deformation field (adjoint of pull).
+    `shape` defaults to the image's own spatial shape; `prefilter` applies
+    the spline prefilter to the splatted result."""
+    grid, input, layout = _fold(grid, input, shared_space=True)
+    target = tuple(input.shape[2:]) if shape is None else shape
+    out = GridPush.apply(input, grid, target, interpolation, bound, extrapolate)
     if prefilter:
-        out = spline_coeff_nd(out, interpolation=interpolation, bound=bound, dim=dim,
-                              inplace=True)
-    return _postproc(out, shape_info, mode="push")
+        out = spline_coeff_nd(out, interpolation=interpolation, bound=bound, dim=layout.dim, inplace=True)
+    return layout.restore(out)
 
 
 def pull_push(input, grid, interpolation="linear", bound="zero", extrapolate=False, prefilter=False):
@@ -112,33 +117,27 @@ def pull_push(input, grid, interpolation="linear", bound="zero", extrapolate=Fal
     input.shape[-dim:], ...) up to floating-point summation order; the grid
     may have any spatial shape.  `prefilter` applies to the pulled input, as
     in grid_pull.  Not in the reference, which runs the two calls."""
-    grid, input, shape_info = _preproc(grid, input)
-    dim = grid.shape[-1]
+    grid, input, layout = _fold(grid, input)
     if prefilter:
-        input = spline_coeff_nd(input, interpolation=interpolation, bound=bound, dim=dim)
-    out = GridPullPush.apply(input, grid, interpolation, bound, extrapolate)
-    return _postproc(out, shape_info, mode="push")
+        input = spline_coeff_nd(input, interpolation=interpolation, bound=bound, dim=layout.dim)
+    return layout.restore(GridPullPush.apply(input, grid, interpolation, bound, extrapolate))
 
 
 def grid_count(grid, shape=None, interpolation="linear", bound="zero", extrapolate=False):
     """Splatting weights of a deformation field (push of ones)."""
-    grid, shape_info = _preproc(grid)
-    if shape is None:
-        shape = tuple(grid.shape[1:-1])
-    out = GridCount.apply(grid, shape, interpolation, bound, extrapolate)
-    return _postproc(out, shape_info, mode="count")
+    grid, _, layout = _fold(grid)
+    target = tuple(grid.shape[1:-1]) if shape is None else shape
+    return layout.restore(GridCount.apply(grid, target, interpolation, bound, extrapolate))
 
 
 def grid_grad(input, grid, interpolation="linear", bound="zero", extrapolate=False,
               prefilter=False):
     """Spatial gradients of the interpolant at the grid points:
     (..., [channel], *outshape, dim)."""
-    grid, input, shape_info = _preproc(grid, input)
-    dim = grid.shape[-1]
+    grid, input, layout = _fold(grid, input)
     if prefilter:
-        input = spline_coeff_nd(input, interpolation, bound, dim)
-    out = GridGrad.apply(input, grid, interpolation, bound, extrapolate)
-    return _postproc(out, shape_info, mode="grad")
+        input = spline_coeff_nd(input, interpolation, bound, layout.dim)
+    return layout.restore(GridGrad.apply(input, grid, interpolation, bound, extrapolate))
 
 
 def spline_coeff(input, interpolation="linear", bound="dct2", dim=-1, inplace=False):

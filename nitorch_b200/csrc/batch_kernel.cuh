@@ -7,7 +7,7 @@
 namespace ppb {
 
 constexpr int kBatchPoints = 256;  // sampling points per work item (= threads per CTA)
-constexpr int kMaxEntries = 80;    // volumes per launch: keeps BatchLaunch under 32 KB
+constexpr int kMaxEntries = 72;    // volumes per launch: keeps BatchLaunch under 32 KB
 
 struct BatchLaunch {
   int32_t n;                       // volumes in this launch

@@ -196,9 +196,147 @@ int sizes_of(const pp_tensor* grid, const int64_t* src_size, int& D, int64_t& nv
   return PP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Brick-major order (3-D): the same counting sort with the key
+//   ((n * NBX + bx) * NBY + by) * NBZ + bz) * BRICK + local
+// of the clamped floor voxel (x, y, z), (bx, by, bz) its brick and `local`
+// its index inside the brick (z fastest), so that the samples of one brick
+// are consecutive.  The brick kernels read brick b's samples from
+// perm[brick_start[b] .. brick_start[b + 1]).
+// ---------------------------------------------------------------------------
+constexpr int BRK[3] = {PP_BRICK_X, PP_BRICK_Y, PP_BRICK_Z};
+constexpr int BRK_VOL = PP_BRICK_X * PP_BRICK_Y * PP_BRICK_Z;
+
+struct BrickGeom {
+  int64_t nb[3];     // bricks per axis
+  int64_t per_item;  // bricks per batch item
+  int64_t nkeys;     // N * per_item * BRK_VOL
+};
+
+BrickGeom brick_geometry(int64_t N, const int64_t* src) {
+  BrickGeom g;
+  g.per_item = 1;
+  for (int d = 0; d < 3; ++d) {
+    g.nb[d] = (src[d] + BRK[d] - 1) / BRK[d];
+    g.per_item *= g.nb[d];
+  }
+  g.nkeys = N * g.per_item * BRK_VOL;
+  return g;
+}
+
+template <class T>
+__global__ void brick_keys(KeyArgs a, int nbx, int nby, int nbz, int32_t* count, int32_t* keys, int32_t* ranks) {
+  const unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= static_cast<unsigned>(a.nvox)) return;
+  int v = static_cast<int>(s), sub[3];
+  for (int d = 2; d >= 0; --d) {
+    const int n = static_cast<int>(a.size[d]);
+    const int q = v / n;
+    sub[d] = v - q * n;
+    v = q;
+  }
+  const T* g = static_cast<const T*>(a.grid) + static_cast<int64_t>(v) * a.gsN;
+  for (int d = 0; d < 3; ++d) g += static_cast<int64_t>(sub[d]) * a.gs[d];
+  int f[3];
+  for (int d = 0; d < 3; ++d) {
+    const T c = g[d * a.gsD];
+    const int n = static_cast<int>(a.src[d]);
+    f[d] = (c >= T(0)) ? static_cast<int>(fmin(c, static_cast<T>(n - 1))) : 0;  // NaN -> 0
+  }
+  const int bx = f[0] / PP_BRICK_X, by = f[1] / PP_BRICK_Y, bz = f[2] / PP_BRICK_Z;
+  const int local = ((f[0] - bx * PP_BRICK_X) * PP_BRICK_Y + (f[1] - by * PP_BRICK_Y)) * PP_BRICK_Z +
+                    (f[2] - bz * PP_BRICK_Z);
+  const int32_t key = (((v * nbx + bx) * nby + by) * nbz + bz) * BRK_VOL + local;
+  keys[s] = key;
+  ranks[s] = atomicAdd(count + key, 1);
+}
+
+// brick_start[b] = offset of brick b's first key; brick_start[nb] = nvox
+__global__ void brick_starts(const int32_t* offset, int64_t nbricks, int32_t nvox, int32_t* start) {
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b < nbricks) start[b] = offset[b * BRK_VOL];
+  else if (b == nbricks) start[b] = nvox;
+}
+
+int brick_sizes_of(const pp_tensor* grid, const int64_t* src_size, int64_t& nvox, BrickGeom& g) {
+  int D;
+  int64_t nsrc;
+  int rc = sizes_of(grid, src_size, D, nvox, nsrc);
+  if (rc) return rc;
+  if (D != 3) return ppc::fail(PP_ERR_UNSUPPORTED, "(): brick ordering needs a 3-D grid");
+  g = brick_geometry(grid->sizes[0], src_size);
+  if (g.nkeys >= (int64_t(1) << 31))
+    return ppc::fail(PP_ERR_UNSUPPORTED, "(): brick ordering needs fewer than 2^31 brick voxels");
+  return PP_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int64_t pp_brick_count(const pp_tensor* grid, const int64_t* src_size) {
+  int64_t nvox;
+  BrickGeom g;
+  if (brick_sizes_of(grid, src_size, nvox, g)) return -1;
+  return grid->sizes[0] * g.per_item;
+}
+
+size_t pp_brick_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size) {
+  int64_t nvox;
+  BrickGeom g;
+  if (brick_sizes_of(grid, src_size, nvox, g)) return 0;
+  return layout(nvox, g.nkeys).total;
+}
+
+int pp_brick_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm, int32_t* brick_start,
+                   void* workspace, size_t workspace_bytes, void* stream) {
+  int64_t nvox;
+  BrickGeom g;
+  int rc = brick_sizes_of(grid, src_size, nvox, g);
+  if (rc) return rc;
+  if (!perm || !brick_start) return ppc::fail(PP_ERR_ARG, "(): expected an output permutation and brick offsets");
+  const Layout L = layout(nvox, g.nkeys);
+  if (!workspace || workspace_bytes < L.total)
+    return ppc::fail(PP_ERR_WORKSPACE, "(): brick ordering needs %zu bytes of workspace", L.total);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t nbricks = grid->sizes[0] * g.per_item;
+  unsigned char* ws = static_cast<unsigned char*>(workspace);
+  int32_t* count = reinterpret_cast<int32_t*>(ws + L.count);
+  int32_t* keys = reinterpret_cast<int32_t*>(ws + L.keys);
+  int32_t* ranks = reinterpret_cast<int32_t*>(ws + L.ranks);
+  int32_t* partial = reinterpret_cast<int32_t*>(ws + L.partial);
+  if ((rc = ppc::cuda_check(cudaMemsetAsync(count, 0, static_cast<size_t>(g.nkeys) * 4, st), "brick order clear")))
+    return rc;
+  KeyArgs a;
+  a.grid = grid->data;
+  a.N = grid->sizes[0];
+  a.D = 3;
+  a.gsN = grid->strides[0];
+  a.gsD = grid->strides[4];
+  for (int d = 0; d < 3; ++d) {
+    a.size[d] = grid->sizes[1 + d];
+    a.src[d] = src_size[d];
+    a.gs[d] = grid->strides[1 + d];
+  }
+  a.nvox = nvox;
+  a.nsrc = g.per_item * BRK_VOL;
+  if (nvox > 0) {
+    const unsigned nb = static_cast<unsigned>((nvox + 255) / 256);
+    const int nbx = static_cast<int>(g.nb[0]), nby = static_cast<int>(g.nb[1]), nbz = static_cast<int>(g.nb[2]);
+    if (grid->dtype == PP_FLOAT32) brick_keys<float><<<nb, 256, 0, st>>>(a, nbx, nby, nbz, count, keys, ranks);
+    else brick_keys<double><<<nb, 256, 0, st>>>(a, nbx, nby, nbz, count, keys, ranks);
+    const int64_t ntile = (g.nkeys + SCAN_TILE - 1) / SCAN_TILE;
+    scan_reduce<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, g.nkeys, partial);
+    scan_partials<<<1, SCAN_THREADS, 0, st>>>(partial, ntile);
+    scan_apply<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, g.nkeys, partial);
+    order_scatter<<<nb, 256, 0, st>>>(keys, ranks, count, nvox, perm);
+    ppc::count_launch(5);
+  }
+  brick_starts<<<static_cast<unsigned>((nbricks + 1 + 255) / 256), 256, 0, st>>>(count, nbricks,
+                                                                                 static_cast<int32_t>(nvox), brick_start);
+  ppc::count_launch();
+  return ppc::cuda_check(cudaGetLastError(), "brick order launch");
+}
 
 size_t pp_sample_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size) {
   int D;

@@ -1,0 +1,457 @@
+// Brick kernels for 3-D cubic sampling in brick-major order.
+//
+// pp_brick_order sorts the sampling points by the brick (PP_BRICK_X x
+// PP_BRICK_Y x PP_BRICK_Z source voxels) of their floor voxel.  A brick's
+// points then touch only the brick's source window: the brick plus the cubic
+// support halo, 7 x 7 x 9 voxels.  Two kernels use that window in shared
+// memory.
+//
+// pp_brick_scatter_kernel (push, count, and the image gradient of the pull's
+// backward pass).  The reference scatters every tap with a global atomic add
+// (nitorch/_C/src/impl/bounds_common.h:185-191, from the tap loop of
+// pushpull_common.cpp:1232-1240): 64 * C float reductions per point.  Here a
+// warp owns one brick and a shared accumulator window:
+//   1. the window starts at zero;
+//   2. points are read 32 at a time, one per lane (coordinates, the
+//      out-of-bound test, B-spline weights), into shared records;
+//   3. the warp walks the recorded points one at a time, lane (i, j, kk)
+//      taking taps (i, j, kk) and (i, j, kk + 2) of the 4x4x4 support:
+//      plain shared read-modify-writes (the 32 lanes touch 32 distinct
+//      voxels and the window belongs to this warp alone, so no atomics);
+//   4. the window is added to the output with one vector reduction per
+//      touched window voxel (boundary index and sign applied there), ~14x
+//      fewer global reductions than one per tap.
+// Float shared-memory atomics are no alternative: on B200 they sustain
+// ~0.7 T adds/s on scatter-like patterns, below the ~1-1.5 T of global
+// reductions.
+//
+// pp_brick_gather_kernel (pull, and the grid gradient of the pull's backward
+// pass).  A CTA owns one brick: its
+// threads stage the source window in shared memory (boundary condition
+// applied per window voxel: value times sign), then each thread takes one
+// point and gathers its 64 taps from the window at compile-time offsets.
+//
+// Points whose support leaves the window (sampling outside the volume with
+// extrapolation, or just below a volume edge) and points outside the field
+// of view run the per-point body pp_point with global memory instead.
+//
+// Window layout: voxel (x, y, z) of the window at (x * PX + y * PY + z) * CP
+// floats, CP channel slots per voxel (1, 2 or 4).  In the scatter, with
+// lane = kk + 2j + 8i and PY = 10, PX = 72 (voxels), the 32 lanes of a step
+// fall in distinct banks for 4-, 8- and 16-byte voxels alike; the gather's
+// pitches are chosen for its own access pattern (GatherWin).
+#pragma once
+#include "../../include/nitorch_b200.h"
+
+namespace ppk {
+
+constexpr int BRK_X = PP_BRICK_X, BRK_Y = PP_BRICK_Y, BRK_Z = PP_BRICK_Z;
+
+// Source window of one brick for cubic taps: floor(x) in [o, o + B) has taps
+// [floor(x) - 1, floor(x) + 2], inside [o - 1, o + B + 2).
+struct BrickWin {
+  static constexpr int LO = 1;
+  static constexpr int EX = BRK_X + 3, EY = BRK_Y + 3, EZ = BRK_Z + 3;
+  static constexpr int PY = 10, PX = 72;
+  static constexpr int NV = EX * PX;       // storage voxels
+  static constexpr int NE = EX * EY * EZ;  // window voxels
+  static_assert(PY >= EZ && PX >= EY * PY, "window pitches too small");
+};
+
+// Per-point scatter record in shared memory (floats, 16-byte aligned rows):
+//   [0, 4) x tap weights   [4, 8) y tap weights
+//   [8, 12) z tap weights in the order 0, 2, 1, 3   [12, 16) target values
+//   [16] window offset of the lowest node
+constexpr int BRK_REC = 20;
+
+constexpr int BRK_SCATTER_WARPS = 4;  // warps (bricks) per scatter CTA
+constexpr int BRK_GATHER_THREADS = 128;
+
+template <int CP> struct BrickScatterSmem {
+  static constexpr int PER_WARP = BrickWin::NV * CP + 32 * BRK_REC;  // floats
+  static constexpr size_t bytes = size_t(PER_WARP) * 4 * BRK_SCATTER_WARPS;
+};
+// The gather kernel's window: the same extents, pitches for thread-per-point
+// reads.  Eight consecutive points of a brick (one phase of a 16-byte shared
+// load) are mostly runs along z of one or two (x, y) columns: with
+// PY = 6 (mod 8) and PX = 0 (mod 8) voxels such runs fall in distinct
+// 16-byte bank groups.
+struct GatherWin {
+  static constexpr int PY = 14, PX = 104;
+  static constexpr int NV = BrickWin::EX * PX;
+  static_assert(PY >= BrickWin::EZ && PX >= BrickWin::EY * PY, "window pitches too small");
+};
+template <int CP> struct BrickGatherSmem {
+  static constexpr size_t bytes = size_t(GatherWin::NV) * CP * 4;
+};
+// Resident CTAs per SM the gather kernels are built for (register caps).
+template <int MODE> struct GatherBlocks { static constexpr int value = MODE == K_PULL ? 6 : 4; };
+
+template <int CP> __device__ __forceinline__ void vload(const float* p, float (&v)[CP]) {
+  if constexpr (CP == 4) { const float4 q = *reinterpret_cast<const float4*>(p); v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w; }
+  else if constexpr (CP == 2) { const float2 q = *reinterpret_cast<const float2*>(p); v[0] = q.x; v[1] = q.y; }
+  else v[0] = *p;
+}
+template <int CP> __device__ __forceinline__ void vstore(float* p, const float (&v)[CP]) {
+  if constexpr (CP == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  else if constexpr (CP == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  else *p = v[0];
+}
+
+// acc[p .. p + CP) += w * t
+template <int CP> __device__ __forceinline__ void vaxpy(float* p, float w, const float (&t)[CP]) {
+  float v[CP];
+  vload<CP>(p, v);
+#pragma unroll
+  for (int c = 0; c < CP; ++c) v[c] = fmaf(w, t[c], v[c]);
+  vstore<CP>(p, v);
+}
+
+// Brick b of the scatter target / gathered source: batch item, window origin
+// (absolute voxel of window voxel 0) and whether the window lies inside the
+// volume on every axis.
+struct BrickPos {
+  int n, ox, oy, oz;
+  bool interior;
+};
+__device__ __forceinline__ BrickPos brick_pos(const PPArgs& a, int64_t b) {
+  using W = BrickWin;
+  BrickPos q;
+  int64_t r = b;
+  const int bz = static_cast<int>(r % a.nbrick[2]); r /= a.nbrick[2];
+  const int by = static_cast<int>(r % a.nbrick[1]); r /= a.nbrick[1];
+  const int bx = static_cast<int>(r % a.nbrick[0]);
+  q.n = static_cast<int>(r / a.nbrick[0]);
+  q.ox = bx * BRK_X - W::LO;
+  q.oy = by * BRK_Y - W::LO;
+  q.oz = bz * BRK_Z - W::LO;
+  q.interior = q.ox >= 0 && q.oy >= 0 && q.oz >= 0 && q.ox + W::EX <= a.src_size[0] &&
+               q.oy + W::EY <= a.src_size[1] && q.oz + W::EZ <= a.src_size[2];
+  return q;
+}
+
+// Window voxel e (x slowest, z fastest) -> window coordinates.
+__device__ __forceinline__ void win_coords(int e, int& wx, int& wy, int& wz) {
+  using W = BrickWin;
+  wx = e / (W::EY * W::EZ);
+  const int rem = e - wx * (W::EY * W::EZ);
+  wy = rem / W::EZ;
+  wz = rem - wy * W::EZ;
+}
+
+// Offset (elements) and sign of absolute voxel (X, Y, Z) under the bound
+// condition, for strides s[]; sign 0 = outside (zero bound, dst nodes).
+__device__ __forceinline__ int64_t bound_offset(const PPArgs& a, int X, int Y, int Z, const int64_t (&s)[3],
+                                                bool interior, int& sgn) {
+  if (interior) {
+    sgn = 1;
+    return X * s[0] + Y * s[1] + Z * s[2];
+  }
+  const int nX = static_cast<int>(a.src_size[0]), nY = static_cast<int>(a.src_size[1]),
+            nZ = static_cast<int>(a.src_size[2]);
+  sgn = bound_sign<int>(a.bound[0], X, nX) * bound_sign<int>(a.bound[1], Y, nY) * bound_sign<int>(a.bound[2], Z, nZ);
+  return bound_index<int>(a.bound[0], X, nX) * s[0] + bound_index<int>(a.bound[1], Y, nY) * s[1] +
+         bound_index<int>(a.bound[2], Z, nZ) * s[2];
+}
+
+// One sampling point of a brick: its grid position, coordinates and whether
+// its 4x4x4 support lies in the brick's window (lo: lowest support node).
+struct BrickPoint {
+  int sub[3], n;
+  float x[3];
+  int lo[3];
+  bool fits;
+};
+__device__ __forceinline__ BrickPoint brick_point(const PPArgs& a, int p, const BrickPos& bp) {
+  using W = BrickWin;
+  BrickPoint q;
+  int v = __ldg(a.perm + p);
+  q.sub[2] = v % static_cast<int>(a.trgt_size[2]); v /= static_cast<int>(a.trgt_size[2]);
+  q.sub[1] = v % static_cast<int>(a.trgt_size[1]); v /= static_cast<int>(a.trgt_size[1]);
+  q.sub[0] = v % static_cast<int>(a.trgt_size[0]);
+  q.n = v / static_cast<int>(a.trgt_size[0]);
+  const float* gp = static_cast<const float*>(a.grid) + static_cast<int64_t>(q.n) * a.grid_sN +
+                    q.sub[0] * a.grid_s[0] + q.sub[1] * a.grid_s[1] + q.sub[2] * a.grid_s[2];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) q.x[d] = __ldg(gp + d * a.grid_sD);
+  const float tol = (a.extrapolate & 2) ? 0.55f : 0.05f;
+  bool inb = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) inb = inb && in_fov<float>(q.x[d], a.src_size[d], tol);
+  // window fit: lowest node floor(x) - 1 within [o, o + E - 4] on every axis
+  q.fits = q.n == bp.n && ((a.extrapolate & 1) || inb);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float xc = fminf(fmaxf(q.x[d], -1073741824.f), 1073741824.f);
+    q.lo[d] = static_cast<int>(floorf(xc)) - 1;
+    const int o = d == 0 ? bp.ox : (d == 1 ? bp.oy : bp.oz);
+    const int e = d == 0 ? W::EX : (d == 1 ? W::EY : W::EZ);
+    q.fits = q.fits && q.lo[d] >= o && q.lo[d] <= o + e - 4;
+  }
+  return q;
+}
+
+// ===========================================================================
+// Scatter: one warp per brick (see the file comment).  CB: channel block of
+// the per-point fallback body (= C for C <= 4); CP: channel slots per window
+// voxel (1 for C = 1, 2 for C = 2, 4 for C = 3-4).
+// ===========================================================================
+template <int MODE, int CB, int CP, class S>
+__global__ void __launch_bounds__(32 * BRK_SCATTER_WARPS) pp_brick_scatter_kernel(const PPArgs a) {
+  using W = BrickWin;
+  using SM = BrickScatterSmem<CP>;
+  static_assert(MODE == K_PUSH || MODE == K_COUNT, "scatter modes");
+  extern __shared__ float4 brick_smem4[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  float* acc = reinterpret_cast<float*>(brick_smem4) + wid * SM::PER_WARP;
+  float* rec = acc + W::NV * CP;
+
+  const int64_t nbricks = a.N * a.nbrick[0] * a.nbrick[1] * a.nbrick[2];
+  const int64_t b = static_cast<int64_t>(blockIdx.x) * BRK_SCATTER_WARPS + wid;
+  if (b >= nbricks) return;  // whole warp
+  const int p0 = __ldg(a.brick_start + b), p1 = __ldg(a.brick_start + b + 1);
+  if (p0 >= p1) return;
+  const BrickPos bp = brick_pos(a, b);
+
+  {
+    float4* a4 = reinterpret_cast<float4*>(acc);
+    for (int e = lane; e < W::NV * CP / 4; e += 32) a4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncwarp();
+
+  // this lane's taps inside a point's 4x4x4 support
+  const int ti = lane >> 3, tj = (lane >> 1) & 3, tk = lane & 1;
+  const int loff = ti * W::PX + tj * W::PY + tk;
+
+  for (int c0 = p0; c0 < p1; c0 += 32) {
+    const int p = c0 + lane;
+    bool mine = false;
+    if (p < p1) {
+      const BrickPoint q = brick_point(a, p, bp);
+      if (!q.fits) {
+        pp_point<3, 3, CB, S, MODE, int>(a, q.sub, q.n);  // global reductions
+      } else {
+        mine = true;
+        float w[3][4], g[3][4], h[3][4];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          bspline_stencil<4, false, false, float>(3, q.x[d] - static_cast<float>(q.lo[d] + 1), w[d], g[d], h[d]);
+        float t[4] = {1.f, 0.f, 0.f, 0.f};
+        if (MODE != K_COUNT) {
+          const S* tp = static_cast<const S*>(a.trgt) + static_cast<int64_t>(q.n) * a.trgt_sN +
+                        q.sub[0] * a.trgt_s[0] + q.sub[1] * a.trgt_s[1] + q.sub[2] * a.trgt_s[2];
+#pragma unroll
+          for (int c = 0; c < 4; ++c) t[c] = (c < CB && c < a.C) ? static_cast<float>(ldg_acc(tp + c * a.trgt_sC)) : 0.f;
+        }
+        float* rr = rec + lane * BRK_REC;
+        *reinterpret_cast<float4*>(rr + 0) = make_float4(w[0][0], w[0][1], w[0][2], w[0][3]);
+        *reinterpret_cast<float4*>(rr + 4) = make_float4(w[1][0], w[1][1], w[1][2], w[1][3]);
+        *reinterpret_cast<float4*>(rr + 8) = make_float4(w[2][0], w[2][2], w[2][1], w[2][3]);
+        *reinterpret_cast<float4*>(rr + 12) = make_float4(t[0], t[1], t[2], t[3]);
+        rr[16] = __int_as_float((q.lo[0] - bp.ox) * W::PX + (q.lo[1] - bp.oy) * W::PY + (q.lo[2] - bp.oz));
+      }
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, mine);
+    __syncwarp();
+    while (todo) {
+      const int q = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const float* rr = rec + q * BRK_REC;
+      const float wxy = rr[ti] * rr[4 + tj];
+      const float2 zp = *reinterpret_cast<const float2*>(rr + 8 + 2 * tk);  // (wz_k, wz_k+2)
+      float t[CP];
+      {
+        const float4 tq = *reinterpret_cast<const float4*>(rr + 12);
+        const float tt[4] = {tq.x, tq.y, tq.z, tq.w};
+#pragma unroll
+        for (int c = 0; c < CP; ++c) t[c] = tt[c];
+      }
+      const int off0 = (__float_as_int(rr[16]) + loff) * CP;
+      vaxpy<CP>(acc + off0, wxy * zp.x, t);
+      vaxpy<CP>(acc + off0 + 2 * CP, wxy * zp.y, t);
+      __syncwarp();
+    }
+  }
+
+  // flush the accumulator window
+  float* out_n = static_cast<float*>(a.out) + static_cast<int64_t>(bp.n) * a.out_sN;
+  const bool vec = (a.flags & F_VEC) != 0;
+  const int64_t os[3] = {a.out_s[0], a.out_s[1], a.out_s[2]};
+  for (int e = lane; e < W::NE; e += 32) {
+    int wx, wy, wz;
+    win_coords(e, wx, wy, wz);
+    float v[CP];
+    vload<CP>(acc + (wx * W::PX + wy * W::PY + wz) * CP, v);
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < CP; ++c) any = any || v[c] != 0.f;
+    if (!any) continue;
+    int sgn;
+    const int64_t off = bound_offset(a, bp.ox + wx, bp.oy + wy, bp.oz + wz, os, bp.interior, sgn);
+    if (sgn == 0) continue;
+    if (sgn < 0) {
+#pragma unroll
+      for (int c = 0; c < CP; ++c) v[c] = -v[c];
+    }
+    if constexpr (CP >= 2) {
+      if (vec) {
+        red_vec<CP>(out_n + off, v);
+        continue;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CP; ++c)
+      if (c < a.C && v[c] != 0.f) atomicAdd(out_n + c * a.out_sC + off, v[c]);
+  }
+}
+
+// ===========================================================================
+// Gather: one CTA per brick, one thread per point.  Modes:
+//   K_PULL      out[c] = sum w src[c]
+//   K_PUSHGRAD  pull backward's grid gradient only (flag F_GRAD, no F_A):
+//               gg_d = sum_c t[c] sum dw_d src[c], src the pulled image and
+//               t the incoming gradient at the point
+// ===========================================================================
+template <int MODE, int CB, int CP, class S>
+__global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
+    pp_brick_gather_kernel(const PPArgs a) {
+  using W = BrickWin;
+  using G = GatherWin;
+  static_assert(MODE == K_PULL || MODE == K_PUSHGRAD, "gather modes");
+  constexpr bool GG = MODE != K_PULL;
+  extern __shared__ float4 brick_smem4[];
+  float* img = reinterpret_cast<float*>(brick_smem4);
+
+  const int64_t b = blockIdx.x;
+  const int p0 = __ldg(a.brick_start + b), p1 = __ldg(a.brick_start + b + 1);
+  if (p0 >= p1) return;  // whole CTA
+  const BrickPos bp = brick_pos(a, b);
+  constexpr bool want_val = MODE == K_PULL;
+  const bool want_gg = GG && (a.flags & F_GRAD) != 0;
+
+  // stage the source window (value times boundary sign; 0 outside): every
+  // thread issues all of its loads before its first shared store
+  {
+    constexpr int NIT = (W::NE + BRK_GATHER_THREADS - 1) / BRK_GATHER_THREADS;
+    const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(bp.n) * a.src_sN;
+    const int64_t ss[3] = {a.src_s[0], a.src_s[1], a.src_s[2]};
+    float v[NIT][CP];
+    int dst[NIT];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int e = static_cast<int>(threadIdx.x) + it * BRK_GATHER_THREADS;
+#pragma unroll
+      for (int c = 0; c < CP; ++c) v[it][c] = 0.f;
+      dst[it] = -1;
+      if (e < W::NE) {
+        int wx, wy, wz;
+        win_coords(e, wx, wy, wz);
+        dst[it] = (wx * G::PX + wy * G::PY + wz) * CP;
+        int sgn;
+        const int64_t so = bound_offset(a, bp.ox + wx, bp.oy + wy, bp.oz + wz, ss, bp.interior, sgn);
+        if (sgn != 0) {
+#pragma unroll
+          for (int c = 0; c < CP; ++c)
+            if (c < CB && c < a.C)
+              v[it][c] = static_cast<float>(sgn) * static_cast<float>(ldg_acc(src_n + c * a.src_sC + so));
+        }
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it)
+      if (dst[it] >= 0) vstore<CP>(img + dst[it], v[it]);
+  }
+  __syncthreads();
+
+  for (int p = p0 + static_cast<int>(threadIdx.x); p < p1; p += BRK_GATHER_THREADS) {
+    const BrickPoint q = brick_point(a, p, bp);
+    if (!q.fits) {
+      pp_point<3, 3, CB, S, MODE, int>(a, q.sub, q.n);  // global memory
+      continue;
+    }
+    float w[3][4], g[3][4], h[3][4];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      bspline_stencil<4, GG, false, float>(3, q.x[d] - static_cast<float>(q.lo[d] + 1), w[d], g[d], h[d]);
+    float t[CP];
+#pragma unroll
+    for (int c = 0; c < CP; ++c) t[c] = 0.f;
+    if (GG && want_gg) {
+      const S* tp = static_cast<const S*>(a.trgt) + static_cast<int64_t>(q.n) * a.trgt_sN +
+                    q.sub[0] * a.trgt_s[0] + q.sub[1] * a.trgt_s[1] + q.sub[2] * a.trgt_s[2];
+#pragma unroll
+      for (int c = 0; c < CP; ++c)
+        if (c < CB && c < a.C) t[c] = static_cast<float>(ldg_acc(tp + c * a.trgt_sC));
+    }
+    const float* ib = img + ((q.lo[0] - bp.ox) * G::PX + (q.lo[1] - bp.oy) * G::PY + (q.lo[2] - bp.oz)) * CP;
+    // separable partial sums, x innermost: per channel the interpolant, and
+    // for the grid gradient the dot product with t under w and dw
+    float val[CP], gx = 0.f, gy = 0.f, gz = 0.f;
+#pragma unroll
+    for (int c = 0; c < CP; ++c) val[c] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float yv[CP], yw = 0.f, ygx = 0.f, ygy = 0.f;
+#pragma unroll
+      for (int c = 0; c < CP; ++c) yv[c] = 0.f;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        float xv[CP], sx = 0.f, sdx = 0.f;
+#pragma unroll
+        for (int c = 0; c < CP; ++c) xv[c] = 0.f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          float iv[CP];
+          vload<CP>(ib + (i * G::PX + j * G::PY + k) * CP, iv);
+          if (want_val) {
+#pragma unroll
+            for (int c = 0; c < CP; ++c)
+              if (c < CB) xv[c] = fmaf(w[0][i], iv[c], xv[c]);
+          }
+          if (GG && want_gg) {
+            float dot = 0.f;
+#pragma unroll
+            for (int c = 0; c < CP; ++c)
+              if (c < CB) dot = fmaf(t[c], iv[c], dot);
+            sx = fmaf(w[0][i], dot, sx);
+            sdx = fmaf(g[0][i], dot, sdx);
+          }
+        }
+        if (want_val) {
+#pragma unroll
+          for (int c = 0; c < CP; ++c)
+            if (c < CB) yv[c] = fmaf(w[1][j], xv[c], yv[c]);
+        }
+        if (GG && want_gg) {
+          yw = fmaf(w[1][j], sx, yw);
+          ygx = fmaf(w[1][j], sdx, ygx);
+          ygy = fmaf(g[1][j], sx, ygy);
+        }
+      }
+      if (want_val) {
+#pragma unroll
+        for (int c = 0; c < CP; ++c)
+          if (c < CB) val[c] = fmaf(w[2][k], yv[c], val[c]);
+      }
+      if (GG && want_gg) {
+        gx = fmaf(w[2][k], ygx, gx);
+        gy = fmaf(w[2][k], ygy, gy);
+        gz = fmaf(g[2][k], yw, gz);
+      }
+    }
+    if (want_val) {
+      S* op = static_cast<S*>(a.out) + static_cast<int64_t>(q.n) * a.out_sN + q.sub[0] * a.out_s[0] +
+              q.sub[1] * a.out_s[1] + q.sub[2] * a.out_s[2];
+#pragma unroll
+      for (int c = 0; c < CP; ++c)
+        if (c < CB && c < a.C) op[c * a.out_sC] = from_acc<S>(val[c]);
+    }
+    if (GG && want_gg) {
+      float* gg = static_cast<float*>(a.gg) + static_cast<int64_t>(q.n) * a.gg_sN + q.sub[0] * a.gg_s[0] +
+                  q.sub[1] * a.gg_s[1] + q.sub[2] * a.gg_s[2];
+      gg[0] = gx; gg[a.gg_sD] = gy; gg[2 * a.gg_sD] = gz;
+    }
+  }
+}
+
+}  // namespace ppk

@@ -45,6 +45,11 @@ static const pp_launcher_t kLaunchers[4][3][ppk::K_NMODES] = {PP_TYPE(f32), PP_T
 #undef PP_ROW
 
 namespace ppk {
+thread_local char g_last_kernel[64] = "";
+void note_kernel(const char* family, int mode, int ord, int cb) {
+  std::snprintf(g_last_kernel, sizeof(g_last_kernel), "%s mode=%d order=%d cb=%d", family, mode, ord, cb);
+}
+
 // Lane-split push (pp_lanes_kernel) and vectorised scatters (F_VEC): on
 // unless the environment sets PP_PUSH_LANES=0 (read once), which falls back
 // to one scalar reduction per channel and tap everywhere.
@@ -175,6 +180,7 @@ int prepare(Call& k, const pp_tensor* grid, const pp_options* opt) {
   for (int a = 0; a < 3; ++a) { k.a.bound[a] = k.bound[a]; k.a.order[a] = k.order[a]; }
   k.a.extrapolate = opt->extrapolate;
   k.a.perm = opt->sample_order;
+  k.a.brick_start = (k.D == 3 && opt->sample_order) ? opt->brick_start : nullptr;
   k.a.grid = grid->data;
   set_grid(grid, k.D, k.a.grid_sN, k.a.grid_s, k.a.grid_sD);
   k.a.N = grid->sizes[0];
@@ -197,6 +203,11 @@ bool need_wide(const Call& k, std::initializer_list<const pp_tensor*> spatial) {
 int run(Call& k, int mode, bool wide, cudaStream_t st) {
   const int ord = iso_order(k.D, k.order);
   if (k.a.nvox == 0) return PP_OK;
+  if (k.a.brick_start) {
+    // bricks of the scatter target / gathered source, as pp_brick_order cut it
+    const int bs[3] = {PP_BRICK_X, PP_BRICK_Y, PP_BRICK_Z};
+    for (int a = 0; a < 3; ++a) k.a.nbrick[a] = (k.a.src_size[a] + bs[a] - 1) / bs[a];
+  }
   return cuda_check(launch(k.dtype, k.D, mode, ord, wide, k.a, st), "push/pull kernel launch");
 }
 
@@ -373,11 +384,13 @@ int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const u
 
 extern "C" {
 
-int pp_abi_version(void) { return 100; }
+int pp_abi_version(void) { return 101; }
 
 const char* pp_last_error(void) { return g_err.c_str(); }
 
 unsigned long long pp_kernel_launches(void) { return g_launches.load(); }
+
+const char* pp_last_kernel(void) { return ppk::g_last_kernel; }
 
 size_t pp_push_workspace_bytes(const pp_tensor* out, int32_t flags) {
   return scatter_ws_bytes(out, flags);
@@ -484,7 +497,7 @@ static int scatter_into(Call& k, int mode, const pp_tensor* out, const pp_tensor
       fits32(numel(out) / k.a.C * CP)) {
     // the lane-split cubic push runs fastest in the grid's own order (1.69
     // vs 1.89 ms on config 2); the other scatters keep the sample order
-    if (mode == ppk::K_PUSH && iso == 3) k.a.perm = nullptr;
+    if (mode == ppk::K_PUSH && iso == 3 && !k.a.brick_start) k.a.perm = nullptr;
     float* acc = static_cast<float*>(ws);
     const int64_t vox = numel(out) / k.a.C;
     if ((rc = cuda_check(cudaMemsetAsync(acc, 0, static_cast<size_t>(vox) * CP * 4, st), "workspace clear"))) return rc;

@@ -30,6 +30,7 @@
 //              gg_d = sum_c [ (P src)_c d(P W)_c/dx_d + (P W)_c d(P src)_c/dx_d ]
 // Runtime flags select the optional halves of the fused modes.
 #pragma once
+#include <atomic>
 #include <type_traits>
 
 #include "pp_common.cuh"
@@ -78,6 +79,11 @@ struct PPArgs {
   unsigned long long* det_acc;
   const unsigned int* det_max;
   double det_bound;
+  // Brick-major order (pp_brick_order): with `perm` brick-major, brick b of
+  // batch item n holds samples perm[brick_start[b] .. brick_start[b + 1]),
+  // nbrick[] bricks per axis of the scatter target / gathered source.
+  const int32_t* brick_start;
+  int64_t nbrick[3];
 };
 
 // Power-of-two scale of the deterministic accumulators: bound * scale < 2^61.
@@ -1243,15 +1249,115 @@ __global__ void __launch_bounds__(PP_THREADS, 4) pp_lanes_pullbwd_kernel(const P
   }
 }
 
+}  // namespace ppk
+
+#include "pp_brick.cuh"
+
+namespace ppk {
+
+void note_kernel(const char* family, int mode, int ord, int cb);
+
+// Dynamic shared memory above 48 KB must be opted into, once per kernel and
+// device: `done` is the caller's per-instantiation record of the devices
+// already set up (bit d = device d).
+template <class K>
+inline cudaError_t brick_smem_optin(K kernel, size_t bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_relaxed) & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  // the whole unified L1 / shared array as shared memory: several CTAs of
+  // these window-sized allocations per SM
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess) done.fetch_or(bit);
+  return e;
+}
+
+template <int MODE, int CB, class S>
+inline cudaError_t launch_brick_scatter(const PPArgs& a, cudaStream_t st) {
+  constexpr int CP = CB == 1 ? 1 : (CB == 2 ? 2 : 4);
+  constexpr size_t bytes = BrickScatterSmem<CP>::bytes;
+  const int64_t nb = a.N * a.nbrick[0] * a.nbrick[1] * a.nbrick[2];
+  const int64_t grid = (nb + BRK_SCATTER_WARPS - 1) / BRK_SCATTER_WARPS;
+  if (grid <= 0) return cudaSuccess;
+  if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  static std::atomic<unsigned long long> optin_done{0};  // one per kernel instantiation
+  cudaError_t e = brick_smem_optin(pp_brick_scatter_kernel<MODE, CB, CP, S>, bytes, optin_done);
+  if (e != cudaSuccess) return e;
+  note_kernel("pp_brick_scatter_kernel", MODE, 3, CB);
+  pp_brick_scatter_kernel<MODE, CB, CP, S><<<static_cast<unsigned>(grid), 32 * BRK_SCATTER_WARPS, bytes, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <int MODE, int CB, class S>
+inline cudaError_t launch_brick_gather(const PPArgs& a, cudaStream_t st) {
+  constexpr int CP = CB == 1 ? 1 : (CB == 2 ? 2 : 4);
+  constexpr size_t bytes = BrickGatherSmem<CP>::bytes;
+  const int64_t nb = a.N * a.nbrick[0] * a.nbrick[1] * a.nbrick[2];
+  if (nb <= 0) return cudaSuccess;
+  if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  static std::atomic<unsigned long long> optin_done{0};
+  cudaError_t e = brick_smem_optin(pp_brick_gather_kernel<MODE, CB, CP, S>, bytes, optin_done);
+  if (e != cudaSuccess) return e;
+  note_kernel("pp_brick_gather_kernel", MODE, 3, CB);
+  pp_brick_gather_kernel<MODE, CB, CP, S><<<static_cast<unsigned>(nb), BRK_GATHER_THREADS, bytes, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Brick kernels of one mode: push / count scatter; pull gather; pull
+// backward = the scatter of the incoming gradient (image gradient) plus the
+// gather of the grid gradient.
+template <int MODE, int CB, class S>
+inline cudaError_t launch_brick(const PPArgs& a, cudaStream_t st) {
+  if constexpr (MODE == K_PUSH || MODE == K_COUNT) {
+    return launch_brick_scatter<MODE, CB, S>(a, st);
+  } else if constexpr (MODE == K_PULL) {
+    return launch_brick_gather<MODE, CB, S>(a, st);
+  } else {
+    static_assert(MODE == K_PUSHGRAD, "brick modes");
+    if (a.flags & F_A) {
+      PPArgs s = a;
+      s.flags &= ~F_GRAD;
+      const cudaError_t e = launch_brick_scatter<K_PUSH, CB, S>(s, st);
+      if (e != cudaSuccess || !(a.flags & F_GRAD)) return e;
+    }
+    PPArgs g = a;
+    g.flags &= ~F_A;
+    return launch_brick_gather<K_PUSHGRAD, CB, S>(g, st);
+  }
+}
+
+// The brick kernels apply to 3-D cubic pull, push, count and the pull's
+// backward pass of float arithmetic and at most four channels, given a
+// brick-major order.  (The push's backward pass -- a pull with derivatives --
+// measured faster as one thread per point through L1: 1.1 vs 1.3 ms on a
+// 3 x 192^3 image.)
+template <int D, int ORD, int MODE> struct UseBrick {
+  static constexpr bool value = D == 3 && ORD == 3 &&
+                                (MODE == K_PUSH || MODE == K_COUNT || MODE == K_PUSHGRAD || MODE == K_PULL);
+};
+
 // The lane-split push applies to 3-D push / count at orders 1 and 3.
 template <int D, int ORD, int MODE> struct UseLanes {
   static constexpr bool value = D == 3 && (ORD == 1 || ORD == 3) && (MODE == K_PUSH || MODE == K_COUNT);
 };
 bool lanes_enabled();  // host switch (pp_capi.cu), on unless PP_PUSH_LANES=0
+// Records, per host thread, which kernel family (and mode, order, channel
+// block) the last launch used (pp_capi.cu; read back by pp_last_kernel).
+void note_kernel(const char* family, int mode, int ord, int cb);
 
 template <int D, int ORD, int CB, class S, int MODE, class I>
 inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
   if (a.nvox == 0) return cudaSuccess;
+  if constexpr (UseBrick<D, ORD, MODE>::value && std::is_same<typename Acc<S>::type, float>::value &&
+                std::is_same<I, int32_t>::value) {
+    if (a.brick_start != nullptr && a.perm != nullptr && a.det_acc == nullptr && a.C <= CB && lanes_enabled() &&
+        !(a.flags & (F_AFFINE | F_IDGRID | F_ADDSELF | F_NOTRGT)))
+      return launch_brick<MODE, CB, S>(a, st);
+  }
   if constexpr (D == 3 && (ORD == 1 || ORD == 3) && MODE == K_PUSHGRAD &&
                 std::is_same<typename Acc<S>::type, float>::value) {
     constexpr int PPB = PP_THREADS / Taps<ORD>::value;
@@ -1260,6 +1366,7 @@ inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
       // pull backward into the interleaved accumulator: lane-split kernel
       if constexpr (CB >= 2) {
         if ((a.flags & F_VEC) && !(a.flags & (F_IDGRID | F_ADDSELF))) {
+          note_kernel("pp_lanes_pullbwd_kernel", MODE, ORD, CB);
           pp_lanes_pullbwd_kernel<ORD, S, I, (CB == 2 ? 2 : 4), CB>
               <<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
           return cudaGetLastError();
@@ -1271,6 +1378,7 @@ inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
       // measured slower this way: 1.43 -> 1.59 ms on a 192^3 grid.)
       if constexpr (ORD == 1) {
         if (!(a.flags & F_VEC) && a.C <= CB) {
+          note_kernel("pp_lanes_pullbwd_kernel", MODE, ORD, CB);
           pp_lanes_pullbwd_kernel<ORD, S, I, 0, CB><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
           return cudaGetLastError();
         }
@@ -1284,11 +1392,13 @@ inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
       if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
       if (a.flags & F_VEC) {
         if constexpr (MODE == K_PUSH && CB >= 2 && std::is_same<typename Acc<S>::type, float>::value) {
+          note_kernel("pp_lanes_kernel", MODE, ORD, CB);
           pp_lanes_kernel<ORD, CB, S, MODE, I, (CB == 2 ? 2 : 4)><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
           return cudaGetLastError();
         }
         return cudaErrorInvalidValue;  // the host only sets F_VEC where a vector kernel exists
       }
+      note_kernel("pp_lanes_kernel", MODE, ORD, CB);
       pp_lanes_kernel<ORD, CB, S, MODE, I, 0><<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);
       return cudaGetLastError();
     }
@@ -1301,6 +1411,7 @@ inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
   if (gx > 0x7fffffffLL || gy > 65535) return cudaErrorInvalidConfiguration;
   dim3 grid(static_cast<unsigned>(gx), static_cast<unsigned>(gy), 1);
   dim3 block(TILE_IN, TILE_MID, 1);
+  note_kernel("pp_kernel", MODE, ORD, CB);
   pp_kernel<D, ORD, CB, S, MODE, I><<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
 }

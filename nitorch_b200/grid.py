@@ -24,39 +24,46 @@ def make_list(x):
     return list(x)
 
 
+# Accepted spellings of each boundary condition (case-insensitive), keyed by
+# the canonical name that is also the BoundType member name.
+_BOUND_SPELLINGS = {
+    "replicate": ("replicate", "repeat", "border", "nearest"),
+    "zero": ("zero", "zeros", "constant"),
+    "dct2": ("dct2", "reflect", "reflection", "neumann"),
+    "dct1": ("dct1", "mirror"),
+    "dft": ("dft", "wrap", "circular"),
+    "dst2": ("dst2", "antireflect", "dirichlet"),
+    "dst1": ("dst1", "antimirror"),
+}
+_BOUND_BY_SPELLING = {s: canon for canon, spellings in _BOUND_SPELLINGS.items() for s in spellings}
+
+
+def _bound_name(b):
+    """Canonical name of one boundary condition given as a BoundType member or
+    any accepted spelling; anything else (integers included) is rejected."""
+    if isinstance(b, BoundType):
+        return b.name        # enum aliases resolve to the canonical member
+    name = _BOUND_BY_SPELLING.get(b.lower()) if isinstance(b, str) else None
+    if name is None:
+        raise ValueError(f"Unknown boundary condition {b}")
+    return name
+
+
 def bound_to_nitorch(bound, as_type="str"):
-    """Convert boundary type to niTorch's convention (grid.py:92-136)."""
-    intype = type(bound)
-    if not isinstance(bound, (list, tuple)):
-        bound = [bound]
-    obound = []
-    for b in bound:
-        b = b.lower() if isinstance(b, str) else b
-        if b in ("replicate", "repeat", "border", "nearest", BoundType.replicate):
-            obound.append("replicate")
-        elif b in ("zero", "zeros", "constant", BoundType.zero):
-            obound.append("zero")
-        elif b in ("dct2", "reflect", "reflection", "neumann", BoundType.dct2):
-            obound.append("dct2")
-        elif b in ("dct1", "mirror", BoundType.dct1):
-            obound.append("dct1")
-        elif b in ("dft", "wrap", "circular", BoundType.dft):
-            obound.append("dft")
-        elif b in ("dst2", "antireflect", "dirichlet", BoundType.dst2):
-            obound.append("dst2")
-        elif b in ("dst1", "antimirror", BoundType.dst1):
-            obound.append("dst1")
-        else:
-            raise ValueError(f"Unknown boundary condition {b}")
-    if as_type in ("enum", "int", int):
-        obound = [getattr(BoundType, b) for b in obound]
-        if as_type in ("int", int):
-            obound = [TS_BOUND[b] for b in obound]
-    if issubclass(intype, (list, tuple)):
-        obound = intype(obound)
+    """Normalise boundary conditions (behaviour of nitorch/_C/grid.py:92-136).
+
+    `bound` is one value or a list / tuple of values; the result has the same
+    form.  as_type: "str" -> canonical names, "enum" -> BoundType members,
+    "int" / int -> the prefilter's integer codes."""
+    is_seq = isinstance(bound, (list, tuple))
+    names = [_bound_name(b) for b in (bound if is_seq else (bound,))]
+    if as_type in ("int", int):
+        out = [TS_BOUND[BoundType[n]] for n in names]
+    elif as_type == "enum":
+        out = [BoundType[n] for n in names]
     else:
-        obound = obound[0]
-    return obound
+        out = names
+    return type(bound)(out) if is_seq else out[0]
 
 
 def inter_to_nitorch(inter, as_type="str"):

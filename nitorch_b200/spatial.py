@@ -49,8 +49,9 @@ _SORT_MIN_SAMPLES = 1 << 18
 
 def set_sample_order(mode="auto"):
     """Processing order of the sampling points: "natural" (grid order),
-    "sorted" (source-sorted, see pp_sample_order) or "auto" (sorted for
-    grids of at least 2^18 points).  Only the speed depends on it."""
+    "sorted" (brick-major for 3-D grids, see pp_brick_order; source-sorted
+    for 1-D / 2-D, see pp_sample_order) or "auto" (sorted for grids of at
+    least 2^18 points).  Only the speed depends on it."""
     global _sample_order_mode
     if mode not in ("auto", "natural", "sorted"):
         raise ValueError(f"unknown sample order mode {mode}")
@@ -114,20 +115,57 @@ def sample_order(grid, src_size):
     return perm
 
 
+def brick_order(grid, src_size):
+    """Brick-major processing order of a 3-D grid's sampling points for a
+    source of spatial size `src_size`: (perm, brick_start), int32 device
+    tensors (see pp_brick_order)."""
+    L = _lib.load()
+    src = (ctypes.c_int64 * 3)(*[int(v) for v in src_size])
+    d = _lib.desc(grid)
+    nbytes = L.pp_brick_order_workspace_bytes(ctypes.byref(d), src)
+    nb = L.pp_brick_count(ctypes.byref(d), src)
+    if nbytes == 0 or nb < 0:
+        raise RuntimeError(L.pp_last_error().decode(errors="replace"))
+    nvox = grid.numel() // grid.shape[-1]
+    perm = torch.empty(nvox, dtype=torch.int32, device=grid.device)
+    starts = torch.empty(nb + 1, dtype=torch.int32, device=grid.device)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=grid.device)
+    with _On(grid):
+        _lib.check(L.pp_brick_order(ctypes.byref(d), src, ctypes.c_void_p(perm.data_ptr()),
+                                    ctypes.c_void_p(starts.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
+                                    nbytes, _lib.stream_of(grid)))
+    return perm, starts
+
+
+def _brick_keys_fit(grid, src_size):
+    """The brick sort keys (N * bricks * brick volume) fit in 32 bits."""
+    nkeys = grid.shape[0] * _BRICK[0] * _BRICK[1] * _BRICK[2]
+    for s, b in zip(src_size, _BRICK):
+        nkeys *= -(-int(s) // b)
+    return nkeys < (1 << 31)
+
+
+_BRICK = (4, 4, 6)  # PP_BRICK_X, PP_BRICK_Y, PP_BRICK_Z
+
+
 def _order_for(grid, src_size):
+    """(perm, brick_start) for the call, or (None, None) for the natural
+    order.  3-D grids get the brick-major order (it also drives the brick
+    scatters); 1-D / 2-D grids the source-sorted one."""
     mode = _sample_order_mode
     if mode == "natural":
-        return None
+        return None, None
     nvox = grid.numel() // grid.shape[-1]
     if mode == "auto" and nvox < _SORT_MIN_SAMPLES:
-        return None
+        return None, None
     if nvox >= (1 << 31):
-        return None
-    perm = _orders.get(grid, src_size)
-    if perm is None:
-        perm = sample_order(grid, src_size)
-        _orders.put(grid, src_size, perm)
-    return perm
+        return None, None
+    bricks = grid.dim() == 5 and _brick_keys_fit(grid, src_size)
+    entry = _orders.get(grid, src_size)
+    if entry is None:
+        entry = brick_order(grid, src_size) if bricks else (sample_order(grid, src_size), None)
+        _orders.put(grid, src_size, entry)
+    return entry
 
 
 def set_deterministic(flag=True):
@@ -220,11 +258,12 @@ def _grid32(grid):
 
 def _opts(bound, interpolation, extrapolate, grid=None, src_size=None):
     _check_opts(bound, interpolation)
-    perm = _order_for(grid, src_size) if grid is not None and grid.is_cuda else None
+    perm, starts = _order_for(grid, src_size) if grid is not None and grid.is_cuda else (None, None)
     o = _lib.options([int(b) for b in bound], [int(i) for i in interpolation],
                      int(extrapolate), _lib.PP_DETERMINISTIC if _deterministic else 0,
-                     None if perm is None else perm.data_ptr())
-    o._keep = perm       # keep the permutation alive for the call
+                     None if perm is None else perm.data_ptr(),
+                     None if starts is None else starts.data_ptr())
+    o._keep = (perm, starts)  # keep the order alive for the call
     return o
 
 

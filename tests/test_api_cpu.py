@@ -68,18 +68,32 @@ def test_checks_and_messages():
         spatial.grid_pull(x.bfloat16(), g, [BoundType.dct2], [InterpolationType.linear], 0)
 
 
-def test_preproc_broadcasting():
+def test_fold_broadcasting():
     grid = torch.zeros(2, 1, 5, 6, 3)
-    inp = torch.zeros(3, 7, 8, 9)          # channel 3, no batch
-    g, i, info = api._preproc(grid, inp)
-    assert g.shape == (2, 5, 6, 3) or g.shape == (2, 1, 5, 6, 3)
-    assert list(info["channel"]) == [3]
+    inp = torch.zeros(3, 7, 8, 9)          # channel 3, no leading dimension
+    g, i, lay = api._fold(grid, inp)
+    assert g.shape == (2, 5, 6, 1, 3) or g.shape == (2, 1, 5, 6, 3)
+    assert i.shape == (2, 3, 7, 8, 9)
+    assert lay.chan == (3,) and lay.lead == (2,)
+    assert api._Layout((2,), (3,), 3).restore(torch.zeros(2, 3, 1, 5, 6)).shape == (2, 3, 1, 5, 6)
     grid = torch.zeros(5, 6, 7, 3)
-    inp = torch.zeros(5, 6, 7)
-    g, i, info = api._preproc(grid, inp)
+    inp = torch.zeros(5, 6, 7)             # no channel, no leading dimension
+    g, i, lay = api._fold(grid, inp)
     assert g.shape == (1, 5, 6, 7, 3) and i.shape == (1, 1, 5, 6, 7)
-    out = api._postproc(torch.zeros(1, 1, 5, 6, 7), info, "pull")
-    assert out.shape == (5, 6, 7)
+    assert lay.restore(torch.zeros(1, 1, 5, 6, 7)).shape == (5, 6, 7)
+    # leading dimensions broadcast; an image without channel gets a singleton one back
+    g, i, lay = api._fold(torch.zeros(4, 1, 2, 3, 2), torch.zeros(5, 2, 3))
+    assert g.shape == (4, 2, 3, 2) and i.shape == (4, 5, 2, 3) and lay.chan == (5,)
+    g, i, lay = api._fold(torch.zeros(4, 2, 3, 2), torch.zeros(2, 3))
+    assert i.shape == (4, 1, 2, 3) and lay.chan == (1,) and lay.lead == (4,)
+    assert lay.restore(torch.zeros(4, 1, 2, 3)).shape == (4, 1, 2, 3)
+    # push broadcasts the spatial shapes too
+    g, i, lay = api._fold(torch.zeros(1, 4, 2), torch.zeros(2, 3, 1), shared_space=True)
+    assert g.shape == (1, 3, 4, 2) and i.shape == (1, 2, 3, 4)
+    # count: grid only
+    g, _, lay = api._fold(torch.zeros(2, 3, 4, 5, 3))
+    assert g.shape == (2, 3, 4, 5, 3) and lay.chan == (1,)
+    assert lay.restore(torch.zeros(2, 1, 3, 4, 5)).shape == (2, 1, 3, 4, 5)
 
 
 def test_identity_grid():

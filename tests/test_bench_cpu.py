@@ -37,26 +37,42 @@ def test_clock_parse_falls_back_to_the_last_sample():
     assert bench.ClockSampler.parse(["garbage\n"], skip=0) is None
 
 
+KERNEL = "pp_brick_gather_kernel mode=5 order=3 cb=3"
+
+
 def _ops(pull_bwd_ms):
     return {"pull_fwd": {"avg_ms": 1.0, "total_ms": 20.0},
             "push_fwd": {"avg_ms": 1.4, "total_ms": 28.0},
             "push_bwd": {"avg_ms": 1.0, "total_ms": 20.0},
-            "pull_bwd": {"avg_ms": pull_bwd_ms, "total_ms": 20 * pull_bwd_ms}}
+            "pull_bwd": {"avg_ms": pull_bwd_ms, "total_ms": 20 * pull_bwd_ms, "kernel": KERNEL}}
 
 
 def test_roofline_of_config2():
     nvox, C = 192 ** 3, 3
     labels = ["pull_fwd", "push_fwd", "push_bwd", "pull_bwd"]
     r = bench.roofline(_ops(2.4), labels, nvox, C, 6.4, None)
-    assert r["kernel"] == "pull_bwd" and r["bound"] == "hbm" and r["unit"] == "GB/s"
+    assert r["op"] == "pull_bwd" and r["kernel"] == KERNEL
+    assert r["bound"] == "hbm" and r["unit"] == "GB/s"
     per = (24 + 3 * 4 * C) * nvox
     assert r["algorithmic_bytes_per_launch"] == per
     assert r["achieved"] == pytest.approx(per / 2.4e-3 / 1e9, rel=1e-3)
     assert r["frac"] == pytest.approx(r["achieved"] / r["peak"], abs=1e-4)
     assert r["spec_gbs"] == 8000.0
     assert r["frac_of_spec"] == pytest.approx(r["achieved"] / 8000.0, abs=1e-4)
-    # the dominant kernel's DRAM traffic comes from its ncu capture on this workload
-    assert r["traffic"] == pytest.approx(565.1e6) and "ncu" in r["traffic_source"]
+    # the dominant kernel's DRAM traffic comes from the ncu capture of the
+    # kernel that ran (looked up by its name), null for a kernel not captured
+    saved = dict(bench.MEASURED_TRAFFIC)
+    try:
+        bench.MEASURED_TRAFFIC.clear()
+        bench.MEASURED_TRAFFIC[KERNEL] = 5.0e8
+        r = bench.roofline(_ops(2.4), labels, nvox, C, 6.4, None)
+        assert r["traffic"] == pytest.approx(5.0e8) and KERNEL in r["traffic_source"]
+        bench.MEASURED_TRAFFIC.clear()
+        r = bench.roofline(_ops(2.4), labels, nvox, C, 6.4, None)
+        assert r["traffic"] is None
+    finally:
+        bench.MEASURED_TRAFFIC.clear()
+        bench.MEASURED_TRAFFIC.update(saved)
     # a scatter: the atomic ceiling beside the HBM roofline
     assert r["atomic"]["adds_per_launch"] == 64 * C * nvox
     assert 0 < r["atomic"]["frac"] < 1

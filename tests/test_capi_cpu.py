@@ -36,7 +36,7 @@ def test_library_exports_every_symbol():
 
 def test_abi_version_and_error_state():
     L = _lib.load()
-    assert L.pp_abi_version() == 100
+    assert L.pp_abi_version() == 101
     assert isinstance(L.pp_last_error(), bytes)
 
 
@@ -135,3 +135,19 @@ def test_batch_plan_validation_on_host():
     arr = (_lib.PPBatchEntry * 1)(lin)
     assert L.pp_batch_scratch_bytes(arr, 1, _lib.PP_BATCH_PULL_PUSH) == 0
     assert L.pp_batch_scratch_bytes(arr, 1, _lib.PP_BATCH_PULL) == 0
+
+
+def test_brick_order_geometry():
+    """Brick counts and workspace of the brick-major order (host side only):
+    ceil(size / brick) bricks per axis and batch item; 3-D grids only."""
+    L = _lib.load()
+    grid = _t((2, 5, 6, 7, 3))
+    src = (ctypes.c_int64 * 3)(21, 22, 27)
+    assert L.pp_brick_count(ctypes.byref(grid), src) == 2 * 6 * 6 * 5
+    nkeys = 2 * 6 * 6 * 5 * 96
+    assert L.pp_brick_order_workspace_bytes(ctypes.byref(grid), src) >= nkeys * 4 + 2 * 2 * 5 * 6 * 7 * 4
+    g2 = _t((1, 5, 6, 2))
+    assert L.pp_brick_count(ctypes.byref(g2), src) == -1
+    assert b"3-D" in L.pp_last_error()
+    rc = L.pp_brick_order(ctypes.byref(grid), src, None, None, None, 0, None)
+    assert rc == _lib.PP_ERR_ARG

@@ -147,3 +147,19 @@ def test_oracle_svf_vs_reference_golden():
     assert np.abs(O.svf_exp(v, inverse=True, displacement=True) - ref).max() <= 1e-11 * np.abs(ref).max()
     ref = SPATIAL["exp_grad"]
     assert np.abs(O.svf_exp_backward(v, w) - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("bound_ts", [0, 1, 2, 3, 6])
+@pytest.mark.parametrize("order", list(range(8)))
+def test_vectorised_prefilter_vs_line_restatement(bound_ts, order):
+    """The line-vectorised torch prefilter of the timed CPU baseline equals
+    the C restatement (itself pinned to the reference's prefilter golden
+    vectors) in float64, including lines shorter than the truncated series."""
+    import torch
+    from oracle import prefilter_torch as P
+    r = np.random.default_rng(10 * bound_ts + order)
+    for shape in [(2, 3, 7, 9, 11), (1, 1, 30, 2, 5)]:
+        a = r.standard_normal(shape)
+        ref = O.spline_coeff_nd(a, [bound_ts], [order], dim=3)
+        mine = P.spline_coeff_nd(torch.from_numpy(a), [bound_ts], [order], 3).numpy()
+        assert np.abs(ref - mine).max() <= 1e-11 * np.abs(ref).max()

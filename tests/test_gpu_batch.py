@@ -86,12 +86,12 @@ def test_batch_graph_replay_equals_eager():
 
 
 def test_batch_more_volumes_than_one_launch_holds():
-    n = 90  # above the 80 volumes one launch carries: two launches per group
+    n = 80  # above the 72 volumes one launch carries: two launches per group
     shapes = [(5 + i % 4, 6, 4 + i % 3) for i in range(n)]
     b = PullPushBatch(shapes, [1] * n, [1] * n, dtype=torch.float32, sorted_order=False)
     _fill(b, seed=5)
     b.step_eager()
-    for i in (0, 45, 89):
+    for i in (0, 45, 79):
         _, z, _, dx, dg = _reference(b, i)
         assert relerr(_np(b.z[i]), _np(z)) < 1e-5
         assert relerr(_np(b.dx[i]), _np(dx)) < 1e-5
