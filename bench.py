@@ -18,7 +18,9 @@ kernels on the same chain and inputs), clocks and kernel-launch counts;
 `fused` reports the same step through the fused pull_push operator, and
 `batched` the config-4 workload (64 uneven volumes, float32 and bfloat16) as
 one captured batched step against the per-call loop; `svf` times config-5
-registration iterations (velocity exponentiation, warp, MSE, backward).
+registration iterations (velocity exponentiation, warp, MSE, backward);
+`resize` times nitorch's resize (256^3 -> 320^3, cubic) through the
+separable TMA-staged kernel beside the per-point affine pull.
 --impl reference times the reference's CPU implementation of the same step
 (full size) on the host cores and prints the same metric.
 With N > 1 (torchrun), every rank runs an independent replica of the
@@ -503,9 +505,10 @@ def run_batched(args, rank, world, device):
     for dtype in (torch.float32, torch.bfloat16):
         tag = "f32" if dtype == torch.float32 else "bf16"
         tuner = Autotuner()
-        ctas, srt, tried = tuner.choose(shapes_r, chans_r, orders_r, dtype=dtype, device=device,
-                                        init=fill_cfg4)
-        b = PullPushBatch(shapes_r, chans_r, orders_r, dtype=dtype, device=device, sorted_order=srt, ctas=ctas)
+        form, ctas, srt, tried = tuner.choose(shapes_r, chans_r, orders_r, dtype=dtype, device=device,
+                                              init=fill_cfg4)
+        b = PullPushBatch(shapes_r, chans_r, orders_r, dtype=dtype, device=device, sorted_order=srt, ctas=ctas,
+                          form=form)
         fill_cfg4(b)
         b.capture()
         for _ in range(args.warmup):
@@ -522,7 +525,9 @@ def run_batched(args, rank, world, device):
                "plain_per_call": {"value": round(total_points * args.batch_steps / (ms_plain * 1e-3) / 1e9, 4),
                                   "unit": "Gvox/s", "ms_per_step": round(ms_plain / args.batch_steps, 3)},
                "speedup": round(ms_plain / ms_graph, 3),
-               "autotune": {"ctas": ctas, "sorted_order": srt, "candidates_ms": tried}}
+               "autotune": {"form": form, "ctas": ctas, "sorted_order": srt, "candidates_ms": tried}}
+        if rank == 0 and dtype == torch.float32:
+            res["max_rel_err_vs_plain"] = batched_vs_plain(b)
         if rank == 0 and dtype == torch.bfloat16 and not args.no_cpu_baseline:
             res["error_vs_fp64_oracle"] = bf16_error(b)
         out[tag] = res
@@ -534,22 +539,46 @@ def run_batched(args, rank, world, device):
     return out
 
 
+def batched_vs_plain(b):
+    """Largest relative difference (max |err| / max |ref|, per volume and
+    output) between the batched float32 step and the per-volume public API
+    on the same stored inputs: z = push(pull(x)), d loss / d x and
+    d loss / d grid, over every volume."""
+    import nitorch_b200 as nb
+    b.step_eager()
+    worst = {"z": 0.0, "dx": 0.0, "dgrid": 0.0}
+    for i in range(b.n):
+        x = b.x[i].detach().clone().requires_grad_(True)
+        g = b.grid[i].detach().clone().requires_grad_(True)
+        z = nb.grid_push(nb.grid_pull(x, g, b.orders[i], "dct2", False), g, None, b.orders[i], "dct2", False)
+        (z * b.w[i]).sum().backward()
+        for k, mine, ref in (("z", b.z[i], z), ("dx", b.dx[i], x.grad), ("dgrid", b.dgrid[i], g.grad)):
+            mine, ref = mine.detach().double(), ref.detach().double()
+            e = float((mine - ref).abs().max() / ref.abs().max().clamp_min(1e-30))
+            worst[k] = max(worst[k], e)
+    return worst
+
+
 def bf16_error(b):
     """Max relative error of the batched bfloat16 step's forward output z =
-    push(pull(x)) of the smallest volume against the FP64 CPU oracle chain
-    on the same stored (bf16) input."""
+    push(pull(x)) against the FP64 CPU oracle chain on the same stored (bf16)
+    input, on the smallest volume of each (order, channel count) present."""
     from oracle import oracle as O
-    i = min(range(b.n), key=lambda k: int(np.prod(b.shapes[k])) * b.channels[k])
     b.step_eager()
     torch.cuda.synchronize(b.device)
-    x = b.x[i].double().cpu().numpy()
-    g = b.grid[i].double().cpu().numpy()
-    ref = O.grid_push(O.grid_pull(x, g, [2], [b.orders[i]], 0), g, x.shape[2:], [2], [b.orders[i]], 0)
-    z = b.z[i].double().cpu().numpy()
-    err = float(np.abs(z - ref).max() / np.abs(ref).max())
-    return {"volume": list(b.shapes[i]), "channels": b.channels[i], "order": b.orders[i],
-            "push_of_pull_max_rel_err": err,
-            "bound": "2^-8 (one bf16 rounding of the pulled values; non-negative image) + 1e-5"}
+    picks = {}
+    for i in sorted(range(b.n), key=lambda k: int(np.prod(b.shapes[k]))):
+        picks.setdefault((b.orders[i], b.channels[i]), i)
+    rows = []
+    for (order, c), i in sorted(picks.items()):
+        x = b.x[i].double().cpu().numpy()
+        g = b.grid[i].double().cpu().numpy()
+        ref = O.grid_push(O.grid_pull(x, g, [2], [order], 0), g, x.shape[2:], [2], [order], 0)
+        z = b.z[i].double().cpu().numpy()
+        rows.append({"volume": list(b.shapes[i]), "channels": c, "order": order,
+                     "push_of_pull_max_rel_err": float(np.abs(z - ref).max() / np.abs(ref).max())})
+    return {"volumes": rows, "max": max(r["push_of_pull_max_rel_err"] for r in rows),
+            "bound": "2^-8 (one bf16 rounding of the pulled values) + 2^-8 (the bf16 push output) + 1e-5"}
 
 
 # ---------------------------------------------------------------------- #
@@ -588,6 +617,62 @@ def run_svf(args, rank, world, device):
             "gpu_launches_per_iteration": round(launches / args.svf_steps, 1)}
 
 
+# ---------------------------------------------------------------------- #
+# resize: separable sampling at a diagonal affine map                     #
+# ---------------------------------------------------------------------- #
+def run_resize(args, rank, world, device):
+    """nitorch's resize of a 1x3x256^3 float32 image to 320^3 (factor 1.25,
+    anchor "c", cubic, dct2, no prefilter): the separable TMA-staged kernel
+    (pp_resize) against the per-point affine pull of the same map.  Roofline:
+    the image read once and the output written once (algorithmic bytes)."""
+    from nitorch_b200 import affine
+    import nitorch_b200 as nb
+    size, out = 256, 320
+    g = torch.Generator(device=device).manual_seed(51)
+    x = torch.randn((1, 3, size, size, size), generator=g, device=device)
+    _, _, scales, shifts = nb.api._resize_transform([size] * 3, None, [out] * 3, "c")
+    mat = torch.zeros((1, 3, 4), dtype=torch.float32, device=device)
+    for d in range(3):
+        mat[0, d, d] = scales[d]
+        mat[0, d, 3] = shifts[d]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    shape = (out,) * 3
+
+    def timeit(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    from nitorch_b200 import _lib
+    sep = timeit(lambda: affine.resize_pull(x, scales, shifts, shape, 3, "dct2", False), args.steps)
+    kernel = _lib.last_kernel()
+    per_point = timeit(lambda: affine.affine_pull(x, mat, shape, 3, "dct2", False), max(3, args.steps // 4))
+    a = affine.resize_pull(x, scales, shifts, shape, 3, "dct2", False)
+    r = affine.affine_pull(x, mat, shape, 3, "dct2", False)
+    diff = float((a - r).abs().max() / r.abs().max())
+    hbm, src = peaks()
+    algo = (x.numel() + 3 * out ** 3) * 4
+    achieved = algo / (sep * 1e-3) / 1e9
+    nvox = out ** 3
+    return {"workload": f"resize 1x3x{size}^3 -> 1x3x{out}^3 float32, factor 1.25, anchor c, cubic, dct2",
+            "kernel": kernel, "ms": round(sep, 4), "value": round(nvox / (sep * 1e-3) / 1e9, 3), "unit": "Gvox/s",
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "peak_source": src, "algorithmic_bytes_per_launch": algo,
+                         "traffic": None},
+            "per_point_affine_pull_ms": round(per_point, 4), "speedup_over_per_point": round(per_point / sep, 2),
+            "max_rel_diff_vs_per_point": diff, "resize_status": affine.resize_status()}
+
+
 def run_all(args, rank, world, device):
     import gc
     line = run_b200(args, rank, world, device)
@@ -606,6 +691,12 @@ def run_all(args, rank, world, device):
         r = run_svf(args, rank, world, device)
         if line is not None:
             line["svf"] = r
+    if not args.no_resize:
+        gc.collect()
+        torch.cuda.empty_cache()
+        r = run_resize(args, rank, world, device)
+        if line is not None:
+            line["resize"] = r
     return line
 
 
@@ -774,6 +865,7 @@ def main():
     ap.add_argument("--batch-volumes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--no-svf", action="store_true")
+    ap.add_argument("--no-resize", action="store_true")
     ap.add_argument("--svf-steps", type=int, default=5)
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if measured")

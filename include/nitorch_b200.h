@@ -226,6 +226,22 @@ PP_API int pp_affine_grad_matrix(const pp_tensor* grad, const pp_tensor* input, 
                                  const pp_tensor* grad_mat, const pp_options* opt, void* stream,
                                  void* workspace, size_t workspace_bytes);
 
+/* Resize: out (N, C, *shape) = input (N, C, *inshape) sampled at
+ * x_d = scale[d] * o_d + shift[d] for every output voxel o (3-D, float32 or
+ * bfloat16, one B-spline order <= 3 for all axes, positive scales): the
+ * diagonal affine sampling of nitorch's resize (nitorch/spatial/_grid.py:
+ * 618-754, affine_grid then ni::grid_pull) and of its native ni::resize
+ * (nitorch/_C/src/resize.h, resize_common.cpp:600-700, which extrapolates:
+ * set bit 0 of opt->extrapolate).  Computed separably (three 4-tap passes
+ * over TMA-staged tiles); equal to pp_affine_pull with the diagonal matrix.
+ * Other cases return PP_ERR_UNSUPPORTED (use pp_affine_pull). */
+PP_API int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale, const double* shift,
+                     const pp_options* opt, void* stream);
+
+/* Device status of the resize kernels (bit 0: a bounded wait for a TMA copy
+ * gave up; 0 in normal operation).  Synchronous. */
+PP_API int pp_resize_status(uint32_t* status);
+
 /* ---- Jacobians of transformation / displacement fields ----------------
  * nitorch.spatial.grid_jacobian / grid_jacdet (nitorch/spatial/_grid.py:
  * 917-1013) without `sample`: central finite differences of the

@@ -19,7 +19,7 @@ from . import _lib
 from .grid import bound_to_nitorch, inter_to_nitorch
 from .spatial import _On, _require_cuda, _workspace, _wsptr, get_deterministic
 
-__all__ = ["affine_pull", "affine_push"]
+__all__ = ["affine_pull", "affine_push", "resize_pull"]
 
 
 def _options(interpolation, bound, extrapolate):
@@ -156,3 +156,67 @@ def affine_push(input, mat, shape, interpolation="linear", bound="zero", extrapo
     """Adjoint of affine_pull: splat input (N, C, *gridshape) into a `shape`
     lattice from the coordinates A [sub; 1]."""
     return AffinePush.apply(input, mat, tuple(int(s) for s in shape), interpolation, bound, extrapolate)
+
+
+# --------------------------------------------------------------------- #
+# diagonal maps (resize): separable kernel                              #
+# --------------------------------------------------------------------- #
+
+def resize_supported(input, interpolation):
+    """pp_resize covers 3-D float32 / bfloat16 images with one B-spline order
+    of at most 3 on every axis."""
+    orders = inter_to_nitorch(interpolation if isinstance(interpolation, (list, tuple)) else [interpolation],
+                              as_type="int")
+    return (input.dim() == 5 and input.dtype in (torch.float32, torch.bfloat16) and input.is_cuda
+            and len(set(orders)) == 1 and orders[0] <= 3)
+
+
+def _resize(input, scales, shifts, shape, interpolation, bound, extrapolate):
+    L = _lib.load()
+    out = torch.empty((input.shape[0], input.shape[1], *shape), dtype=input.dtype, device=input.device)
+    opt = _options(interpolation, bound, extrapolate)
+    D3 = ctypes.c_double * 3
+    with _On(input):
+        _lib.check(L.pp_resize(ctypes.byref(_lib.desc(input)), ctypes.byref(_lib.desc(out)),
+                               D3(*[float(v) for v in scales]), D3(*[float(v) for v in shifts]),
+                               ctypes.byref(opt), _lib.stream_of(input)))
+    return out
+
+
+def resize_status():
+    """Device status word of the resize kernels (0: no bounded wait gave up)."""
+    L = _lib.load()
+    v = ctypes.c_uint32(0)
+    _lib.check(L.pp_resize_status(ctypes.byref(v)))
+    return int(v.value)
+
+
+class ResizePull(torch.autograd.Function):
+    """Sampling at x_d = scale_d o_d + shift_d (a diagonal affine map) by the
+    separable kernel; the image gradient is the affine push of the same map."""
+
+    @staticmethod
+    def forward(ctx, input, scales, shifts, shape, interpolation, bound, extrapolate):
+        ctx.args = (tuple(input.shape[2:]), tuple(scales), tuple(shifts), interpolation, bound, extrapolate)
+        return _resize(input, scales, shifts, shape, interpolation, bound, extrapolate)
+
+    @staticmethod
+    def backward(ctx, grad):
+        inshape, scales, shifts, interpolation, bound, extrapolate = ctx.args
+        gi = None
+        if ctx.needs_input_grad[0]:
+            dim = len(scales)
+            mat = torch.zeros((1, dim, dim + 1), dtype=torch.float32, device=grad.device)
+            for d in range(dim):
+                mat[0, d, d] = scales[d]
+                mat[0, d, dim] = shifts[d]
+            m = _matrix(mat, grad.shape[0], dim, grad.dtype)
+            gi = _push(grad.contiguous(), m, inshape, interpolation, bound, extrapolate)
+        return gi, None, None, None, None, None, None
+
+
+def resize_pull(input, scales, shifts, shape, interpolation="linear", bound="zero", extrapolate=False):
+    """Sample input (N, C, X, Y, Z) at x_d = scales[d] * o_d + shifts[d] for
+    every voxel o of a `shape` lattice (pp_resize; positive scales)."""
+    return ResizePull.apply(input, tuple(float(v) for v in scales), tuple(float(v) for v in shifts),
+                            tuple(int(v) for v in shape), interpolation, bound, extrapolate)

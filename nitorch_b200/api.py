@@ -9,7 +9,7 @@ Same signatures, defaults, broadcasting and output shapes as
 """
 import torch
 
-from .affine import affine_pull, affine_push
+from .affine import affine_pull, affine_push, resize_pull, resize_supported
 from .grid import GridCount, GridGrad, GridPull, GridPullPush, GridPush, SplineCoeff, SplineCoeffND
 
 
@@ -236,7 +236,11 @@ def resize(image, factor=None, shape=None, affine=None, anchor="c", dim=None, *a
         mat[d, nb_dim] = shifts[d]
     if prefilter:
         x = spline_coeff_nd(x, interpolation=interpolation, bound=bound, dim=nb_dim)
-    out = affine_pull(x, mat, outshape, interpolation, bound, extrapolate)
+    if nb_dim == 3 and all(s > 0 for s in scales) and resize_supported(x, interpolation):
+        # diagonal map: the separable kernel (equal to the affine pull)
+        out = resize_pull(x, scales, shifts, outshape, interpolation, bound, extrapolate)
+    else:
+        out = affine_pull(x, mat, outshape, interpolation, bound, extrapolate)
     out = out.reshape(*batch, *outshape)
     if affine is not None:
         affine = torch.as_tensor(affine)

@@ -12,11 +12,14 @@ whose per-volume arguments travel as kernel parameters.
 `PullPushBatch` is the pull -> push -> <z, w> -> backward step of the
 batched benchmark configuration, on static buffers ("arenas"), so the whole
 step -- per-volume sample ordering, the batched launches and the loss -- can
-be captured once in a CUDA graph and replayed.  By default it runs the fused
-normal operator (two batched passes per step); `fused=False` runs the four
-separate passes of the two-call chain.  `Autotuner` picks the launch shape
-and the sample order per (orders, dtype, channel mix, batch size) key and
-caches the choice on disk.
+be captured once in a CUDA graph and replayed.  Three forms: "fused" (the
+fused normal operator, two batched passes per step), "chain" (the four
+separate passes of the two-call chain, batched) and "percall" (every volume
+through the single-volume entry points and their kernels -- brick order,
+brick kernels -- from one host loop, captured in the same graph).
+`Autotuner` picks the form, the launch shape and the sample order per
+(orders, dtype, channel mix, batch size) key by timing them, and caches the
+choice on disk.
 
 `plan_shards` partitions a batch over ranks (longest processing time first
 on points x channels); the volumes are independent, so multi-GPU runs need
@@ -96,8 +99,10 @@ class PullPushBatch:
     are kept in their own arenas.
     """
 
+    FORMS = ("fused", "chain", "percall")
+
     def __init__(self, shapes, channels, orders, bound="dct2", extrapolate=False,
-                 dtype=torch.float32, device=None, sorted_order=True, ctas=0, fused=True):
+                 dtype=torch.float32, device=None, sorted_order=True, ctas=0, fused=True, form=None):
         self.device = torch.device(device or "cuda")
         self.n = len(shapes)
         self.shapes = [tuple(int(v) for v in s) for s in shapes]
@@ -106,9 +111,15 @@ class PullPushBatch:
         self.dtype = dtype
         self.sorted_order = bool(sorted_order)
         self.ctas = int(ctas)
-        self.fused = bool(fused)
+        self.form = form or ("fused" if fused else "chain")
+        if self.form not in self.FORMS:
+            raise ValueError(f"unknown batch form {self.form}")
+        self.fused = self.form == "fused"
         self.bound = int(BoundType[bound] if isinstance(bound, str) else bound)
         self.extrapolate = int(extrapolate)
+        if self.form == "percall":
+            self._init_percall()
+            return
         img = [(1, c, *s) for c, s in zip(self.channels, self.shapes)]
         grd = [(1, *s, 3) for s in self.shapes]
         dev = self.device
@@ -134,6 +145,76 @@ class PullPushBatch:
         self._build_plans()
         self.graph = None
         self.graph_launches = 0
+
+    # -- the per-call form ------------------------------------------------------
+    def _init_percall(self):
+        """Static buffers of the per-call form: every volume goes through the
+        single-volume entry points (pp_brick_order, pp_grid_pull,
+        pp_grid_push, pp_grid_push_backward, pp_grid_pull_backward) -- the
+        kernels of the per-call API -- enqueued from one host loop, so that a
+        CUDA graph holds the whole step.  Pulled / pushed values and the image
+        gradient keep the image dtype, as the per-call API returns them."""
+        img = [(1, c, *s) for c, s in zip(self.channels, self.shapes)]
+        grd = [(1, *s, 3) for s in self.shapes]
+        dev, dt = self.device, self.dtype
+        self.x_flat, self.x = _arena(img, dt, dev)
+        self.grid_flat, self.grid = _arena(grd, torch.float32, dev)
+        self.w_flat, self.w = _arena(img, dt, dev)
+        self.y_flat, self.y = _arena(img, dt, dev)
+        self.z_flat, self.z = _arena(img, dt, dev)
+        self.dy_flat, self.dy = _arena(img, dt, dev)
+        self.dx_flat, self.dx = _arena(img, dt, dev)
+        self.dg1_flat, self.dg1 = _arena(grd, torch.float32, dev)
+        self.dg2_flat, self.dg2 = _arena(grd, torch.float32, dev)
+        self.dgrid_flat, self.dgrid = _arena(grd, torch.float32, dev)
+        self.loss = torch.zeros((), dtype=torch.float32, device=dev)
+        L = _lib.load()
+        npts = [int(torch.Size(s).numel()) for s in self.shapes]
+        self.perm_flat, self.perm = _arena([(n,) for n in npts], torch.int32, dev)
+        nb, ws, pws = [], 256, 256
+        for g, s, z, dx in zip(self.grid, self.shapes, self.z, self.dx):
+            src = (ctypes.c_int64 * 3)(*s)
+            nb.append(int(L.pp_brick_count(ctypes.byref(_lib.desc(g)), src)) + 1)
+            ws = max(ws, L.pp_brick_order_workspace_bytes(ctypes.byref(_lib.desc(g)), src))
+            pws = max(pws, L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(z)), 0),
+                      L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(dx)), 0))
+        self.starts_flat, self.starts = _arena([(n,) for n in nb], torch.int32, dev)
+        self.sort_ws = torch.empty(ws, dtype=torch.uint8, device=dev)
+        self.push_ws = torch.empty(pws, dtype=torch.uint8, device=dev)
+        self.plans = {}
+        self.graph = None
+        self.graph_launches = 0
+
+    def _step_percall(self):
+        L = _lib.load()
+        B = _lib
+        stream = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        ws, nws = ctypes.c_void_p(self.push_ws.data_ptr()), self.push_ws.numel()
+        ref = lambda t: ctypes.byref(B.desc(t))  # noqa: E731
+        opts = []
+        for i in range(self.n):
+            if self.sorted_order:
+                src = (ctypes.c_int64 * 3)(*self.shapes[i])
+                B.check(L.pp_brick_order(ref(self.grid[i]), src, ctypes.c_void_p(self.perm[i].data_ptr()),
+                                         ctypes.c_void_p(self.starts[i].data_ptr()),
+                                         ctypes.c_void_p(self.sort_ws.data_ptr()), self.sort_ws.numel(), stream))
+                opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, 0,
+                                      self.perm[i].data_ptr(), self.starts[i].data_ptr()))
+            else:
+                opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, 0))
+        for i in range(self.n):
+            o = ctypes.byref(opts[i])
+            B.check(L.pp_grid_pull(ref(self.x[i]), ref(self.grid[i]), ref(self.y[i]), o, stream))
+            B.check(L.pp_grid_push(ref(self.y[i]), ref(self.grid[i]), ref(self.z[i]), o, stream, ws, nws))
+        self._loss()
+        for i in range(self.n):
+            o = ctypes.byref(opts[i])
+            B.check(L.pp_grid_push_backward(ref(self.w[i]), ref(self.y[i]), ref(self.grid[i]), ref(self.dy[i]),
+                                            ref(self.dg1[i]), o, stream))
+            B.check(L.pp_grid_pull_backward(ref(self.dy[i]), ref(self.x[i]), ref(self.grid[i]), ref(self.dx[i]),
+                                            ref(self.dg2[i]), o, stream, ws, nws))
+        torch.add(self.dg1_flat, self.dg2_flat, out=self.dgrid_flat)
+        return self.loss
 
     # -- plans ---------------------------------------------------------------
     def _opt(self, i):
@@ -178,10 +259,12 @@ class PullPushBatch:
         if self.dtype == torch.float32:
             torch.dot(self.z_flat, self.w_flat, out=self.loss)
         else:
-            self.loss.copy_((self.z_flat * self.w_flat.float()).sum())
+            self.loss.copy_((self.z_flat.float() * self.w_flat.float()).sum())
 
     def step_eager(self):
         """One step without the graph; returns the loss tensor (device)."""
+        if self.form == "percall":
+            return self._step_percall()
         if self.sorted_order:
             self._sort()
         if self.fused:
@@ -241,8 +324,11 @@ class Autotuner:
     keyed by GPU, dtype, the set of orders, the channel mix, the batch size
     and the step form (fused or chain)."""
 
-    # (persistent CTAs per SM, 0 = one CTA per work item) x sample order
-    CANDIDATES = [(ctas_per_sm, srt) for srt in (True, False) for ctas_per_sm in (0, 4)]
+    # (form, persistent CTAs per SM (0 = one CTA per work item), sample order):
+    # the per-volume entry points in one graph, and the batched kernels
+    CANDIDATES = ([("percall", 0, True), ("percall", 0, False)] +
+                  [(form, ctas_per_sm, srt) for form in ("chain", "fused") for srt in (True, False)
+                   for ctas_per_sm in (0, 4)])
 
     _lock = threading.Lock()  # one tuning / cache write at a time per process
 
@@ -256,31 +342,32 @@ class Autotuner:
             self.cache = {}
 
     @staticmethod
-    def key(shapes, channels, orders, dtype, device, fused=True):
+    def key(shapes, channels, orders, dtype, device):
         name = torch.cuda.get_device_name(device)
         nb = 1 << max(0, (len(shapes) - 1).bit_length())
         cmix = ",".join(str(c) for c in sorted(set(channels)))
         omix = ",".join(str(o) for o in sorted(set(orders)))
-        return f"{name}|{dtype}|o{omix}|c{cmix}|n{nb}|{'fused' if fused else 'chain'}"
+        return f"{name}|{dtype}|o{omix}|c{cmix}|n{nb}"
 
     def choose(self, shapes, channels, orders, dtype=torch.float32, device=None, bound="dct2",
-               extrapolate=False, reps=3, init=None, fused=True):
-        """Returns (ctas, sorted_order, timings).  `init(batch)` fills the
-        input arenas of a candidate batch before it is timed."""
+               extrapolate=False, reps=3, init=None):
+        """Returns (form, ctas, sorted_order, timings).  `init(batch)` fills
+        the input arenas of a candidate batch before it is timed."""
         with Autotuner._lock:
-            return self._choose(shapes, channels, orders, dtype, device, bound, extrapolate, reps, init, fused)
+            return self._choose(shapes, channels, orders, dtype, device, bound, extrapolate, reps, init)
 
-    def _choose(self, shapes, channels, orders, dtype, device, bound, extrapolate, reps, init, fused):
+    def _choose(self, shapes, channels, orders, dtype, device, bound, extrapolate, reps, init):
         device = torch.device(device or "cuda")
-        k = self.key(shapes, channels, orders, dtype, device, fused)
-        if k in self.cache:
+        k = self.key(shapes, channels, orders, dtype, device)
+        if k in self.cache and "form" in self.cache[k]:
             c = self.cache[k]
-            return c["ctas"], c["sorted"], c.get("ms", {})
+            return c["form"], c["ctas"], c["sorted"], c.get("ms", {})
         sms = torch.cuda.get_device_properties(device).multi_processor_count
         timings = {}
         best = None
-        for per_sm, srt in self.CANDIDATES:
-            b = PullPushBatch(shapes, channels, orders, bound, extrapolate, dtype, device, srt, per_sm * sms, fused)
+        for form, per_sm, srt in self.CANDIDATES:
+            b = PullPushBatch(shapes, channels, orders, bound, extrapolate, dtype, device, srt, per_sm * sms,
+                              form=form)
             if init is not None:
                 init(b)
             b.capture()
@@ -291,14 +378,14 @@ class Autotuner:
                 b.step()
             torch.cuda.synchronize(device)
             ms = (time.perf_counter() - t0) * 1e3 / reps
-            timings[f"{per_sm}x{'sorted' if srt else 'natural'}"] = round(ms, 3)
+            timings[f"{form}:{per_sm}x{'sorted' if srt else 'natural'}"] = round(ms, 3)
             if best is None or ms < best[0]:
-                best = (ms, per_sm * sms, srt)
+                best = (ms, form, per_sm * sms, srt)
             b.release()
             del b
             gc.collect()
             torch.cuda.empty_cache()
-        self.cache[k] = {"ctas": best[1], "sorted": best[2], "ms": timings}
+        self.cache[k] = {"form": best[1], "ctas": best[2], "sorted": best[3], "ms": timings}
         try:
             # write-then-rename: a concurrent reader never sees a partial file
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -308,7 +395,7 @@ class Autotuner:
             os.replace(tmp, self.path)
         except OSError:
             pass
-        return best[1], best[2], timings
+        return best[1], best[2], best[3], timings
 
 
 # ---------------------------------------------------------------------------

@@ -16,6 +16,10 @@ namespace ppc {
 
 extern thread_local std::string g_err;
 
+// pp_options -> per-axis bound codes and orders (padded with the last
+// entry); validates them (pp_capi.cu).
+int read_options(const pp_options* o, int D, int bound[3], int order[3]);
+
 // Number of kernels this library has launched (all threads, all devices);
 // exported as pp_kernel_launches() so callers can audit what ran.
 extern std::atomic<unsigned long long> g_launches;

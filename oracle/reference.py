@@ -32,8 +32,13 @@ _ts = None
 
 
 def load_compiled():
-    """The compiled reference module (``nitorch._C.spatial``) or None."""
+    """The compiled reference module (``nitorch._C.spatial``) or None.  When
+    the CUDA build is already loaded, that module (which carries the CPU
+    backend too) is returned: the two builds register the same pybind11
+    types and cannot both be loaded in one process."""
     global _compiled
+    if _compiled is None and _compiled_cuda is not None:
+        return _compiled_cuda
     if _compiled is None and os.path.exists(REF_SO):
         import torch  # noqa: F401  (the extension links against libtorch)
         spec = importlib.util.spec_from_file_location("spatial", REF_SO)
@@ -44,9 +49,10 @@ def load_compiled():
 
 
 def load_compiled_cuda():
-    """The reference module with its CUDA backend (sm_100a) or None."""
+    """The reference module with its CUDA backend (sm_100a) or None (also
+    None when the CPU-only build is already loaded in this process)."""
     global _compiled_cuda
-    if _compiled_cuda is None and os.path.exists(REF_CUDA_SO):
+    if _compiled_cuda is None and _compiled is None and os.path.exists(REF_CUDA_SO):
         import torch  # noqa: F401
         spec = importlib.util.spec_from_file_location("spatial_cuda", REF_CUDA_SO)
         mod = importlib.util.module_from_spec(spec)

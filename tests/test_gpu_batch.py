@@ -47,23 +47,28 @@ def _np(t):
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
 @pytest.mark.parametrize("sorted_order", [True, False])
-@pytest.mark.parametrize("fused", [True, False], ids=["fused", "chain"])
+@pytest.mark.parametrize("form", ["fused", "chain", "percall"])
 @pytest.mark.parametrize("ctas", [0, 37])
-def test_batch_step_matches_per_volume(dtype, sorted_order, fused, ctas):
-    b = PullPushBatch(SHAPES, CHANNELS, ORDERS, dtype=dtype, sorted_order=sorted_order, fused=fused, ctas=ctas)
+def test_batch_step_matches_per_volume(dtype, sorted_order, form, ctas):
+    if form == "percall" and ctas:
+        pytest.skip("the per-call form has no launch-shape choice")
+    b = PullPushBatch(SHAPES, CHANNELS, ORDERS, dtype=dtype, sorted_order=sorted_order, form=form, ctas=ctas)
     _fill(b)
     loss = b.step_eager().item()
     f32 = dtype == torch.float32
     tot = 0.0
     for i in range(b.n):
         y, z, l, dx, dg = _reference(b, i)
-        if not fused:
+        if form != "fused":
             assert relerr(_np(b.y[i]), _np(y)) < (1e-5 if f32 else 2.0 ** -8)
         assert relerr(_np(b.z[i]), _np(z)) < (1e-5 if f32 else 2.0 ** -7)
         assert relerr(_np(b.dx[i]), _np(dx)) < (1e-5 if f32 else 2.0 ** -7)
-        assert relerr(_np(b.dgrid[i]), _np(dg)) < (1e-4 if f32 else 2.0 ** -6)
+        assert relerr(_np(b.dgrid[i]), _np(dg)) < (1e-5 if f32 else 2.0 ** -6)
         tot += l.item()
-    assert abs(loss - tot) <= 1e-4 * max(1.0, abs(tot))
+    # the per-call form stores z in the image dtype (as the per-call API
+    # returns it): with bfloat16 storage its loss carries that rounding
+    tol = 2.0 ** -7 if (form == "percall" and not f32) else 1e-4
+    assert abs(loss - tot) <= tol * max(1.0, abs(tot))
     b.release()
 
 

@@ -1,10 +1,12 @@
 """The 64-bit offset kernel instances (runtime order, int64 index arithmetic)
 against the FP64 oracle.
 
-A call takes them when the grid has 2^31 points or more, or when a tensor's
-largest element offset does not fit in 32 bits.  Here the image's second
-batch item starts at element 2^31 of one 8 GiB buffer, so every op on it
-runs the 64-bit instances; the grid and the other tensors are small.
+Batch offsets are always 64-bit; a call takes the 64-bit instances when the
+grid has 2^31 points or more, or when an offset inside one batch item does
+not fit in 32 bits.  Here the image is a view of one 8 GiB buffer whose x
+axis has a stride of 2^30 elements: its third x plane starts at element
+2^31, so every op on it runs the 64-bit instances (checked through
+pp_last_kernel); the grid and the other tensors are small.
 
 Tolerances: float32 1e-5 relative (max |err| / max |ref|); order 0
 bit-exact against the oracle's float32 build."""
@@ -14,61 +16,65 @@ import torch
 
 from oracle import oracle as O
 from nitorch_b200 import _lib, spatial
-from tests._cases import make_case
 from tests._gpu_ops import cu, enums, np64, relerr
 
 pytestmark = pytest.mark.gpu
 
-SHAPE = (6, 7, 8)
 C = 2
+XS = 2 ** 30  # x stride of the wide views (elements)
 
 
 @pytest.fixture(scope="module")
 def wide_buffer():
-    buf = torch.zeros(2 ** 31 + 4096, dtype=torch.float32, device="cuda")
+    buf = torch.zeros(2 * XS + 4096, dtype=torch.float32, device="cuda")
     yield buf
     del buf
     torch.cuda.empty_cache()
 
 
-def _wide_image(buf, vol):
-    """(2, C, *SHAPE) view whose item 1 starts at element 2^31 of `buf`."""
-    n = int(np.prod(SHAPE))
-    v = buf.as_strided((2, C) + SHAPE, (2 ** 31, n, SHAPE[1] * SHAPE[2], SHAPE[2], 1))
-    v.copy_(torch.as_tensor(vol, dtype=torch.float32))
+def _wide(buf, arr):
+    """(1, C, 3, Y, Z) view of `buf` with x stride 2^30, holding `arr`."""
+    _, c, x, y, z = arr.shape
+    assert x == 3
+    v = buf.as_strided(arr.shape, (0, y * z, XS, z, 1))
+    v.copy_(torch.as_tensor(arr, dtype=torch.float32))
     return v
+
+
+def _grid(seed, src, out):
+    r = np.random.default_rng(seed)
+    lo, hi = -1.0, np.array(src, np.float64)
+    return (lo + r.random((1,) + out + (3,)) * (hi + 1.0))
 
 
 @pytest.mark.parametrize("order", [0, 1, 3])
 @pytest.mark.parametrize("bound", [2, 7, 5])
 def test_wide_offsets_vs_oracle(wide_buffer, order, bound):
-    _, grid = make_case(3, seed=700 + 10 * bound + order, in_size=7, out_size=5, C=C, N=2)
-    vol = np.random.default_rng(order).standard_normal((2, C) + SHAPE)
-    V = _wide_image(wide_buffer, vol)
+    src = (3, 7, 8)
+    out_shape = (3, 6, 5)
+    grid = _grid(700 + 10 * bound + order, src, out_shape)
+    vol = np.random.default_rng(order).standard_normal((1, C) + src)
     b, o = enums(bound, order)
     G = cu(grid, torch.float32)
+    # pull from a wide image
+    V = _wide(wide_buffer, vol)
     out = spatial.grid_pull(V, G, b, o, 1)
     assert "order=-1" in _lib.last_kernel(), _lib.last_kernel()
-    ref = O.grid_pull(vol, grid, [bound], [order], 1)
-    assert relerr(np64(out), ref) < 1e-5
+    assert relerr(np64(out), O.grid_pull(vol, grid, [bound], [order], 1)) < 1e-5
     if order == 0:
         ref32 = O.grid_pull(vol.astype(np.float32), grid.astype(np.float32), [bound], [order], 1, real="f32")
         assert np.array_equal(out.cpu().numpy(), ref32)
-    # push from a wide input, and the pull's backward pass with a wide image
-    tgt = np.random.default_rng(order + 1).standard_normal((2, C) + grid.shape[1:-1])
-    T = cu(tgt, torch.float32)
-    Vt = V.detach()
-    Vt.requires_grad_(True)
+    # the pull's backward pass with the wide image
+    tgt = np.random.default_rng(order + 1).standard_normal((1, C) + out_shape)
+    Vt = V.detach().requires_grad_(True)
     Gr = cu(grid, torch.float32, True)
-    dx, dg = spatial.grid_pull_backward(T, Vt, Gr, b, o, 1)
+    dx, dg = spatial.grid_pull_backward(cu(tgt, torch.float32), Vt, Gr, b, o, 1)
     assert "order=-1" in _lib.last_kernel(), _lib.last_kernel()
     ref_in, ref_grid = O.grid_pull_backward(tgt, vol, grid, [bound], [order], 1)
     assert relerr(np64(dx), ref_in) < 1e-5
     assert relerr(np64(dg), ref_grid) < 1e-5
-    # the same image as the push input (wide target values)
-    tv = wide_buffer.as_strided((2, C) + grid.shape[1:-1], (2 ** 31, int(np.prod(grid.shape[1:-1])),
-                                                            grid.shape[2] * grid.shape[3], grid.shape[3], 1))
-    tv.copy_(torch.as_tensor(tgt, dtype=torch.float32))
-    pushed = spatial.grid_push(tv, G, list(SHAPE), b, o, 1)
+    # push from a wide input on a 3 x 6 x 5 grid
+    T = _wide(wide_buffer, tgt)
+    pushed = spatial.grid_push(T, G, list(src), b, o, 1)
     assert "order=-1" in _lib.last_kernel(), _lib.last_kernel()
-    assert relerr(np64(pushed), O.grid_push(tgt, grid, SHAPE, [bound], [order], 1)) < 1e-5
+    assert relerr(np64(pushed), O.grid_push(tgt, grid, src, [bound], [order], 1)) < 1e-5
