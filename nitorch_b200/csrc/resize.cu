@@ -12,20 +12,24 @@
 //   1. per axis, each output index's lowest node, weights and field-of-view
 //      test go to shared tables;
 //   2. per channel, the input region the tile reads -- its nodes from the
-//      tile's first to last output, per axis -- is staged in shared memory:
-//      by one TMA tensor copy (cp.async.bulk.tensor, mbarrier completion)
-//      when the region lies inside the volume, else by loads that apply the
-//      boundary condition per voxel (value times sign);
+//      tile's first to last output, per axis -- is staged in shared memory
+//      by one TMA tensor copy (cp.async.bulk.tensor, mbarrier completion);
+//      staged voxels outside the volume are then rewritten under the
+//      boundary condition (sign times the mapped voxel, which the staged
+//      region usually holds already);
 //   3. x pass: T1[ox][y][z] = sum_i wx_i S[lx + i][y][z] over the staged y, z;
 //      y pass: T2[ox][oy][z] = sum_j wy_j T1[ox][ly + j][z];
 //      z pass: out = sum_k wz_k T2[ox][oy][lz + k], stored along z.
 // Each partial sum is the fused multiply-add chain of the per-point kernel
 // (x innermost, then y, then z, starting from zero), so the result equals
-// pp_grid_pull's on the materialised affine grid.  The next channel's TMA
-// copy is issued as soon as the x pass has read the staged region.
+// pp_grid_pull's on the materialised affine grid.  Persistent CTAs walk the
+// (tile, channel) items with two staging buffers: the next item's copy is
+// in flight while the current item is filtered; the x and y passes move
+// four z positions per thread (16-byte shared accesses).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -41,7 +45,8 @@ namespace {
 using namespace ppk;
 
 constexpr int RZ_THREADS = 256;
-constexpr int RZ_MAXT = 64;  // largest tile edge (tables)
+constexpr int RZ_MAXT = 64;   // largest tile edge (tables)
+constexpr int RZ_MAXE = 256;  // largest staged extent (boundary tables)
 
 struct ResizeArgs {
   const void* src;
@@ -56,6 +61,7 @@ struct ResizeArgs {
   int tile[3];  // TX, TY, TZ
   int ext[3];   // staged extents EX, EY, EZ (EZ a multiple of 4: the TMA box)
   int ntile[3];
+  int zls;  // log2 of the lanes per staged z row in the x and y passes (2^zls >= EZ / 4, at most 32)
   int use_tma;
 };
 
@@ -93,130 +99,155 @@ __device__ __forceinline__ void axis_stencil(const ResizeArgs& a, int d, int o, 
   bspline_stencil<NT, false, false, float>(a.order, a.order == 0 ? 0.f : f, w, g, h);
 }
 
+// One work item: channel c of output tile t (items are channel-minor).
+struct RzItem {
+  int n, c, o0[3], tn[3];
+  int base[3];      // first staged node per axis (z on a 16-byte boundary)
+  int fits;         // the tile's nodes lie within the staged extents
+  int interior;     // ... and inside the volume
+};
+
+// Item setup by the 32 lanes of warp 0: lane d < 3 handles axis d.
+template <int NT>
+__device__ void rz_item(const ResizeArgs& a, int item, RzItem& it) {
+  const int lane = threadIdx.x & 31;
+  const int t = item / a.C;
+  int r = t;
+  const int tz = r % a.ntile[2]; r /= a.ntile[2];
+  const int ty = r % a.ntile[1]; r /= a.ntile[1];
+  const int tx = r % a.ntile[0];
+  bool fits = true, interior = true;
+  if (lane < 3) {
+    const int d = lane;
+    const int o0 = (d == 0 ? tx : (d == 1 ? ty : tz)) * a.tile[d];
+    const int tn = min(a.tile[d], a.out_size[d] - o0);
+    float w[NT];
+    int lo0, lo1;
+    bool inb;
+    axis_stencil<NT>(a, d, o0, lo0, w, inb);
+    axis_stencil<NT>(a, d, o0 + tn - 1, lo1, w, inb);
+    const int b = d == 2 ? (lo0 & ~3) : lo0;
+    const int hi = lo1 + NT - 1;
+    it.o0[d] = o0;
+    it.tn[d] = tn;
+    it.base[d] = b;
+    fits = hi - b < a.ext[d];
+    interior = b >= 0 && hi < a.in_size[d];
+  }
+  const bool all_fit = __all_sync(0xffffffffu, fits), all_in = __all_sync(0xffffffffu, interior);
+  if (lane == 0) {
+    it.c = item - t * a.C;
+    it.n = r / a.ntile[0];
+    it.fits = all_fit;
+    it.interior = all_fit && all_in;
+  }
+  __syncwarp();
+}
+
+// Persistent CTAs walk the (tile, channel) items with two staging buffers:
+// the TMA copy of the next item is in flight while the current one is
+// filtered.
 template <int NT, class S, bool TMA>
-__global__ void __launch_bounds__(RZ_THREADS) resize_sep_kernel(const __grid_constant__ ResizeArgs a,
+__global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_constant__ ResizeArgs a,
                                                                  const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) float rz_smem[];
-  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ __align__(8) unsigned long long mbar[2];
+  __shared__ unsigned uses[2];  // copies issued into each staging buffer
   __shared__ int lo_t[3][RZ_MAXT];
-  __shared__ float w_t[3][RZ_MAXT][NT];
+  __shared__ float4 w_t[3][RZ_MAXT];  // NT <= 4 weights per output index
   __shared__ unsigned char inb_t[3][RZ_MAXT];
-  __shared__ int base_t[3];  // first staged node per axis
-  __shared__ int interior, fits;
+  __shared__ int gidx_t[3][RZ_MAXE];           // boundary items: node each staged position maps to
+  __shared__ signed char sgn_t[3][RZ_MAXE];    // ... and its sign
+  __shared__ RzItem cur, nxt;
   __shared__ bool tma_ok;
 
-  const int TX = a.tile[0], TY = a.tile[1], TZ = a.tile[2];
+  const int TX = a.tile[0], TY = a.tile[1];
   const int EX = a.ext[0], EY = a.ext[1], EZ = a.ext[2];
-  float* Sst = rz_smem;                 // [EX][EY][EZ]
-  float* T1 = Sst + EX * EY * EZ;       // [TX][EY][EZ]
-  float* T2 = T1 + TX * EY * EZ;        // [TX][TY][EZ]
-
-  int t = blockIdx.x;
-  const int tz = t % a.ntile[2]; t /= a.ntile[2];
-  const int ty = t % a.ntile[1]; t /= a.ntile[1];
-  const int tx = t % a.ntile[0];
-  const int n = t / a.ntile[0];
-  const int o0[3] = {tx * TX, ty * TY, tz * TZ};
-  int tn[3];
-  for (int d = 0; d < 3; ++d) tn[d] = min(a.tile[d], a.out_size[d] - o0[d]);
-
-  // 1. per-axis tables
-  for (int e = threadIdx.x; e < TX + TY + TZ; e += RZ_THREADS) {
-    const int d = e < TX ? 0 : (e < TX + TY ? 1 : 2);
-    const int i = e - (d == 0 ? 0 : (d == 1 ? TX : TX + TY));
-    float w[NT];
-    int lo;
-    bool inb;
-    axis_stencil<NT>(a, d, o0[d] + min(i, tn[d] - 1), lo, w, inb);
-    lo_t[d][i] = lo;
-#pragma unroll
-    for (int k = 0; k < NT; ++k) w_t[d][i][k] = w[k];
-    inb_t[d][i] = inb;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    bool in = true, fit = true;
-    for (int d = 0; d < 3; ++d) {
-      int b = lo_t[d][0];
-      if (d == 2) b &= ~3;  // TMA: the innermost coordinate on a 16-byte boundary
-      base_t[d] = b;
-      const int hi = lo_t[d][tn[d] - 1] + NT - 1;  // last node the tile reads
-      fit = fit && hi - b < a.ext[d];
-      in = in && b >= 0 && hi < a.in_size[d];
-    }
-    fits = fit;
-    interior = in && fit;
-    if (TMA && fit) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar)), "r"(1) : "memory");
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-  }
-  __syncthreads();
-  const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(n) * a.src_sN;
-  S* out_n = static_cast<S*>(a.out) + static_cast<int64_t>(n) * a.out_sN;
+  const int EZ4 = EZ / 4;
+  const int SZ = EX * EY * EZ;
+  // TMA writes shared memory at 128-byte boundaries: the staging buffers
+  // start at a 128-byte aligned base, one pitch (a multiple of 32 floats) apart
+  const int SP = (SZ + 31) & ~31;
+  float* smem = rz_smem + ((128u - (smem_addr(rz_smem) & 127u)) & 127u) / 4u;
+  float* T1 = smem + 2 * SP;  // [TX][EY][EZ]
+  float* T2 = T1 + TX * EY * EZ;  // [TX][TY][EZ]
+  const int nitems = a.ntile[0] * a.ntile[1] * a.ntile[2] * a.N * a.C;
+  const int lz = threadIdx.x & 31, lr = threadIdx.x >> 5;
   const bool oob_zero = !(a.extrapolate & 1);
-  if (!fits) {
-    // the nodes of this tile span more than its staged region (float
-    // rounding of the coordinates): every voxel straight from global memory
-    for (int e = threadIdx.x; e < TX * TY * TZ; e += RZ_THREADS) {
-      const int oz = e % TZ, r = e / TZ, oy = r % TY, ox = r / TY;
-      if (ox >= tn[0] || oy >= tn[1] || oz >= tn[2]) continue;
-      const bool zero = oob_zero && !(inb_t[0][ox] && inb_t[1][oy] && inb_t[2][oz]);
-      for (int c = 0; c < a.C; ++c) {
-        const S* sc = src_n + c * a.src_sC;
-        float acc = 0.f;
-        for (int k = 0; zero == false && k < NT; ++k) {
-          float accy = 0.f;
-          for (int j = 0; j < NT; ++j) {
-            float accx = 0.f;
-            for (int i = 0; i < NT; ++i) {
-              const int X = lo_t[0][ox] + i, Y = lo_t[1][oy] + j, Z = lo_t[2][oz] + k;
-              const int sgn = bound_sign<int>(a.bound[0], X, a.in_size[0]) *
-                              bound_sign<int>(a.bound[1], Y, a.in_size[1]) *
-                              bound_sign<int>(a.bound[2], Z, a.in_size[2]);
-              float v = 0.f;
-              if (sgn != 0)
-                v = static_cast<float>(sgn) *
-                    static_cast<float>(ldg_acc(sc + bound_index<int>(a.bound[0], X, a.in_size[0]) * a.src_s[0] +
-                                               bound_index<int>(a.bound[1], Y, a.in_size[1]) * a.src_s[1] +
-                                               bound_index<int>(a.bound[2], Z, a.in_size[2]) * a.src_s[2]));
-              accx = fmaf(w_t[0][ox][i], v, accx);
-            }
-            accy = fmaf(w_t[1][oy][j], accx, accy);
-          }
-          acc = fmaf(w_t[2][oz][k], accy, acc);
-        }
-        out_n[c * a.out_sC + (o0[0] + ox) * a.out_s[0] + (o0[1] + oy) * a.out_s[1] + (o0[2] + oz) * a.out_s[2]] =
-            from_acc<S>(acc);
-      }
-    }
-    return;
-  }
-  // TMA copies serve every tile (a box reaching outside the volume reads
-  // zeros there; those voxels are rewritten with their boundary value)
-  const bool use_tma = TMA;
-  const int bx = base_t[0], by = base_t[1], bz = base_t[2];
-  const unsigned bar = smem_addr(&mbar);
-  const unsigned box_bytes = static_cast<unsigned>(EX * EY * EZ * 4);
 
-  auto issue = [&](int c) {  // one thread: TMA copy of channel c's region
+  auto issue = [&](int buf, const RzItem& it) {  // one thread: TMA copy of an item's region
+    const unsigned bar = smem_addr(&mbar[buf]);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(box_bytes) : "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"(static_cast<unsigned>(SZ * 4))
+                 : "memory");
     asm volatile(
         "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
-            smem_addr(Sst)),
-        "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(bz), "r"(by), "r"(bx), "r"(n * a.C + c), "r"(bar)
+            smem_addr(smem + buf * SP)),
+        "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(it.base[2]), "r"(it.base[1]), "r"(it.base[0]),
+        "r"(it.n * a.C + it.c), "r"(bar)
         : "memory");
+    ++uses[buf];
   };
-  if (use_tma && threadIdx.x == 0) issue(0);
 
-  // thread (lz, lr): lanes along z (stride 32), warps along rows (stride 8)
-  const int lz = threadIdx.x & 31, lr = threadIdx.x >> 5;
-  for (int c = 0; c < a.C; ++c) {
-    // 2. staged region of channel c
-    const S* sc = src_n + c * a.src_sC;
-    // value of staged voxel (x, y, z) under the boundary condition
-    auto bounded = [&](int X, int Y, int Z) -> float {
+  int item = blockIdx.x;
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) {
+      if (TMA) {
+        for (int b = 0; b < 2; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&mbar[b])), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      }
+      uses[0] = uses[1] = 0;
+    }
+    if (item < nitems) {
+      rz_item<NT>(a, item, cur);
+      if (TMA && threadIdx.x == 0 && cur.fits) issue(0, cur);
+    }
+  }
+  __syncthreads();
+
+  for (int k = 0; item < nitems; item += gridDim.x, ++k) {
+    const int buf = k & 1;
+    float* Sst = smem + buf * SP;
+    // per-axis tables of this item's tile
+    for (int e = threadIdx.x; e < a.tile[0] + a.tile[1] + a.tile[2]; e += RZ_THREADS) {
+      const int d = e < a.tile[0] ? 0 : (e < a.tile[0] + a.tile[1] ? 1 : 2);
+      const int i = e - (d == 0 ? 0 : (d == 1 ? a.tile[0] : a.tile[0] + a.tile[1]));
+      float w[NT];
+      int lo;
+      bool inb;
+      axis_stencil<NT>(a, d, cur.o0[d] + min(i, cur.tn[d] - 1), lo, w, inb);
+      lo_t[d][i] = lo - cur.base[d];  // relative to the staged region
+      float4 w4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      w4.x = w[0];
+      if (NT > 1) w4.y = w[NT > 1 ? 1 : 0];
+      if (NT > 2) w4.z = w[NT > 2 ? 2 : 0];
+      if (NT > 3) w4.w = w[NT > 3 ? 3 : 0];
+      w_t[d][i] = w4;
+      inb_t[d][i] = inb;
+    }
+    if (cur.fits && !cur.interior) {
+      // per axis, where the boundary condition maps each staged position
+      for (int e = threadIdx.x; e < EX + EY + EZ; e += RZ_THREADS) {
+        const int d = e < EX ? 0 : (e < EX + EY ? 1 : 2);
+        const int i = e - (d == 0 ? 0 : (d == 1 ? EX : EX + EY));
+        const int P = cur.base[d] + i;
+        gidx_t[d][i] = bound_index<int>(a.bound[d], P, a.in_size[d]);
+        sgn_t[d][i] = static_cast<signed char>(bound_sign<int>(a.bound[d], P, a.in_size[d]));
+      }
+    }
+    // the next item: its copy goes into the other buffer (its last reader,
+    // item k - 1, has finished)
+    if (threadIdx.x < 32) {
+      const int ni = item + gridDim.x;
+      if (ni < nitems) {
+        rz_item<NT>(a, ni, nxt);
+        if (TMA && threadIdx.x == 0 && nxt.fits) issue(buf ^ 1, nxt);
+      }
+    }
+    const S* sc = static_cast<const S*>(a.src) + static_cast<int64_t>(cur.n) * a.src_sN + cur.c * a.src_sC;
+    const int bx = cur.base[0], by = cur.base[1], bz = cur.base[2];
+    auto bounded = [&](int X, int Y, int Z) -> float {  // staged value under the boundary condition
       const int sgn = bound_sign<int>(a.bound[0], X, a.in_size[0]) * bound_sign<int>(a.bound[1], Y, a.in_size[1]) *
                       bound_sign<int>(a.bound[2], Z, a.in_size[2]);
       if (sgn == 0) return 0.f;
@@ -225,95 +256,195 @@ __global__ void __launch_bounds__(RZ_THREADS) resize_sep_kernel(const __grid_con
                           bound_index<int>(a.bound[2], Z, a.in_size[2]) * a.src_s[2];
       return static_cast<float>(sgn) * static_cast<float>(ldg_acc(sc + off));
     };
-    if (use_tma) {
-      // one thread waits for the copy (the others sleep in the barrier),
-      // then every thread observes the completed phase once: acquire order
-      // on the copied data without 256 threads spinning
-      if (threadIdx.x == 0) tma_ok = mbar_wait(bar, static_cast<unsigned>(c & 1));
+    S* out_c = static_cast<S*>(a.out) + static_cast<int64_t>(cur.n) * a.out_sN + cur.c * a.out_sC;
+
+    if (!cur.fits) {
+      // the nodes of this tile span more than the staged region (float
+      // rounding of the coordinates): its voxels straight from global memory
       __syncthreads();
-      if (!tma_ok) {
-        if (threadIdx.x == 0) {
-          atomicOr(&g_resize_status, 1u);
-          mbar_wait(bar, static_cast<unsigned>(c & 1));  // the copy may still land: wait once more
+      for (int e = threadIdx.x; e < a.tile[0] * a.tile[1] * a.tile[2]; e += RZ_THREADS) {
+        const int oz = e % a.tile[2], r = e / a.tile[2], oy = r % TY, ox = r / TY;
+        if (ox >= cur.tn[0] || oy >= cur.tn[1] || oz >= cur.tn[2]) continue;
+        float acc = 0.f;
+        if (!oob_zero || (inb_t[0][ox] && inb_t[1][oy] && inb_t[2][oz])) {
+          const float* wx = &w_t[0][ox].x;
+          const float* wy = &w_t[1][oy].x;
+          const float* wz = &w_t[2][oz].x;
+          for (int kk = 0; kk < NT; ++kk) {
+            float accy = 0.f;
+            for (int j = 0; j < NT; ++j) {
+              float accx = 0.f;
+              for (int i = 0; i < NT; ++i)
+                accx = fmaf(wx[i], bounded(bx + lo_t[0][ox] + i, by + lo_t[1][oy] + j, bz + lo_t[2][oz] + kk), accx);
+              accy = fmaf(wy[j], accx, accy);
+            }
+            acc = fmaf(wz[kk], accy, acc);
+          }
         }
-        return;
+        out_c[(cur.o0[0] + ox) * a.out_s[0] + (cur.o0[1] + oy) * a.out_s[1] + (cur.o0[2] + oz) * a.out_s[2]] =
+            from_acc<S>(acc);
       }
-      mbar_wait(bar, static_cast<unsigned>(c & 1));
-      if (!interior) {
-        // rewrite the staged voxels that lie outside the volume
+    } else {
+      // staged region of this item
+      if (TMA) {
+        // one thread waits for the copy (the others sleep in the barrier),
+        // then every thread observes the completed phase once
+        const unsigned ph = (uses[buf] - 1) & 1u;
+        if (threadIdx.x == 0) tma_ok = mbar_wait(smem_addr(&mbar[buf]), ph);
+        __syncthreads();
+        if (!tma_ok) {
+          if (threadIdx.x == 0) {
+            atomicOr(&g_resize_status, 1u);
+            mbar_wait(smem_addr(&mbar[buf]), ph);  // the copy may still land: wait once more
+            if (TMA && item + gridDim.x < nitems && nxt.fits)
+              mbar_wait(smem_addr(&mbar[buf ^ 1]), (uses[buf ^ 1] - 1) & 1u);
+          }
+          return;
+        }
+        mbar_wait(smem_addr(&mbar[buf]), ph);
+      } else {
+        // stage the voxels inside the volume
+        __syncthreads();
         for (int r = lr; r < EX * EY; r += RZ_THREADS / 32) {
           const int x = r / EY, y = r - x * EY;
           const int X = bx + x, Y = by + y;
-          const bool row_in = X >= 0 && X < a.in_size[0] && Y >= 0 && Y < a.in_size[1];
+          if (X < 0 || X >= a.in_size[0] || Y < 0 || Y >= a.in_size[1]) continue;
+          const S* rowp = sc + X * a.src_s[0] + Y * a.src_s[1];
           for (int z = lz; z < EZ; z += 32) {
             const int Z = bz + z;
-            if (row_in && Z >= 0 && Z < a.in_size[2]) continue;
-            Sst[r * EZ + z] = bounded(X, Y, Z);
+            if (Z >= 0 && Z < a.in_size[2]) Sst[r * EZ + z] = static_cast<float>(ldg_acc(rowp + Z * a.src_s[2]));
+          }
+        }
+        __syncthreads();
+      }
+      if (!cur.interior) {
+        // the staged voxels outside the volume: the boundary condition maps
+        // each to a voxel inside it (times a sign), read from the staged
+        // region when it holds that voxel, else from global memory.  All
+        // threads share three segments: x planes outside the volume, then
+        // rows outside it in y, then the out-of-volume z of inside rows.
+        int lo3[3], hi3[3];  // staged positions inside the volume: [lo, hi)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          lo3[d] = min(max(-cur.base[d], 0), a.ext[d]);
+          hi3[d] = max(min(a.in_size[d] - cur.base[d], a.ext[d]), lo3[d]);
+        }
+        const int nxi = hi3[0] - lo3[0], nyi = hi3[1] - lo3[1], nzi = hi3[2] - lo3[2];
+        const int nyo = EY - nyi, nzo = EZ - nzi;
+        const int segA = (EX - nxi) * EY * EZ, segB = nxi * nyo * EZ, segC = nxi * nyi * nzo;
+        for (int e = threadIdx.x; e < segA + segB + segC; e += RZ_THREADS) {
+          int x, y, z;
+          if (e < segA) {
+            const int q = e / EZ;
+            z = e - q * EZ;
+            const int xo = q / EY;
+            y = q - xo * EY;
+            x = xo < lo3[0] ? xo : hi3[0] + (xo - lo3[0]);
+          } else if (e < segA + segB) {
+            const int f = e - segA, q = f / EZ;
+            z = f - q * EZ;
+            const int xi = q / nyo, yo = q - xi * nyo;
+            x = lo3[0] + xi;
+            y = yo < lo3[1] ? yo : hi3[1] + (yo - lo3[1]);
+          } else {
+            const int f = e - segA - segB, q = f / nzo, zo = f - q * nzo;
+            const int xi = q / nyi;
+            x = lo3[0] + xi;
+            y = lo3[1] + (q - xi * nyi);
+            z = zo < lo3[2] ? zo : hi3[2] + (zo - lo3[2]);
+          }
+          const int sgn = sgn_t[0][x] * sgn_t[1][y] * sgn_t[2][z];
+          float v = 0.f;
+          if (sgn != 0) {
+            const int gx = gidx_t[0][x], gy = gidx_t[1][y], gz = gidx_t[2][z];
+            const int mx = gx - bx, my = gy - by, mz = gz - bz;
+            const float u = (mx >= 0 && mx < EX && my >= 0 && my < EY && mz >= 0 && mz < EZ)
+                                ? Sst[(mx * EY + my) * EZ + mz]
+                                : static_cast<float>(ldg_acc(sc + gx * a.src_s[0] + gy * a.src_s[1] + gz * a.src_s[2]));
+            v = static_cast<float>(sgn) * u;
+          }
+          Sst[(x * EY + y) * EZ + z] = v;
+        }
+      }
+      __syncthreads();
+      // x pass over every staged (y, z), four z at a time: rows (ox, y),
+      // 2^zls lanes per row
+      const int ZL = 1 << a.zls, RW = 32 >> a.zls;
+      const int zl = lz & (ZL - 1), rs = lz >> a.zls;
+      {
+        const float4* S4 = reinterpret_cast<const float4*>(Sst);
+        float4* T14 = reinterpret_cast<float4*>(T1);
+        for (int r = lr * RW + rs; r < TX * EY; r += (RZ_THREADS / 32) * RW) {
+          const int ox = r / EY, y = r - ox * EY;
+          const float4 w = w_t[0][ox];
+          const float wi[4] = {w.x, w.y, w.z, w.w};
+          const float4* sp = S4 + (lo_t[0][ox] * EY + y) * EZ4;
+          for (int z = zl; z < EZ4; z += ZL) {
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < NT; ++i) {
+              const float4 v = sp[i * EY * EZ4 + z];
+              acc.x = fmaf(wi[i], v.x, acc.x);
+              acc.y = fmaf(wi[i], v.y, acc.y);
+              acc.z = fmaf(wi[i], v.z, acc.z);
+              acc.w = fmaf(wi[i], v.w, acc.w);
+            }
+            T14[r * EZ4 + z] = acc;
           }
         }
       }
-    } else {
-      for (int r = lr; r < EX * EY; r += RZ_THREADS / 32) {
-        const int x = r / EY, y = r - x * EY;
-        const int X = bx + x, Y = by + y;
-        const bool row_in = X >= 0 && X < a.in_size[0] && Y >= 0 && Y < a.in_size[1];
-        const S* rowp = sc + X * a.src_s[0] + Y * a.src_s[1];
-        for (int z = lz; z < EZ; z += 32) {
-          const int Z = bz + z;
-          Sst[r * EZ + z] = (row_in && Z >= 0 && Z < a.in_size[2]) ? static_cast<float>(ldg_acc(rowp + Z * a.src_s[2]))
-                                                                    : bounded(X, Y, Z);
+      __syncthreads();
+      // y pass, four z at a time: rows (ox, oy)
+      {
+        const float4* T14 = reinterpret_cast<const float4*>(T1);
+        float4* T24 = reinterpret_cast<float4*>(T2);
+        for (int r = lr * RW + rs; r < TX * TY; r += (RZ_THREADS / 32) * RW) {
+          const int ox = r / TY, oy = r - ox * TY;
+          const float4 w = w_t[1][oy];
+          const float wj[4] = {w.x, w.y, w.z, w.w};
+          const float4* tp = T14 + (ox * EY + lo_t[1][oy]) * EZ4;
+          for (int z = zl; z < EZ4; z += ZL) {
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+              const float4 v = tp[j * EZ4 + z];
+              acc.x = fmaf(wj[j], v.x, acc.x);
+              acc.y = fmaf(wj[j], v.y, acc.y);
+              acc.z = fmaf(wj[j], v.z, acc.z);
+              acc.w = fmaf(wj[j], v.w, acc.w);
+            }
+            T24[r * EZ4 + z] = acc;
+          }
+        }
+      }
+      __syncthreads();
+      // z pass and store: lanes along oz (the stencil of each lane's oz
+      // read once), warps over rows (ox, oy)
+      for (int oz = lz; oz < cur.tn[2]; oz += 32) {
+        const float4 w = w_t[2][oz];
+        const float wk[4] = {w.x, w.y, w.z, w.w};
+        const int lzo = lo_t[2][oz];
+        const bool inz = inb_t[2][oz];
+        S* oc = out_c + (cur.o0[2] + oz) * a.out_s[2];
+#pragma unroll 4
+        for (int r = lr; r < TX * TY; r += RZ_THREADS / 32) {
+          const int ox = r / TY, oy = r - ox * TY;
+          if (ox >= cur.tn[0] || oy >= cur.tn[1]) continue;
+          float acc = 0.f;
+          if (!oob_zero || (inz && inb_t[0][ox] && inb_t[1][oy])) {
+            const float* tz = T2 + r * EZ + lzo;
+#pragma unroll
+            for (int kk = 0; kk < NT; ++kk) acc = fmaf(wk[kk], tz[kk], acc);
+          }
+          oc[(cur.o0[0] + ox) * a.out_s[0] + (cur.o0[1] + oy) * a.out_s[1]] = from_acc<S>(acc);
         }
       }
     }
+    // order this item's generic-proxy writes to the staging buffer (the
+    // boundary fix-up) before the next TMA copy into it
+    if (TMA && cur.fits && !cur.interior) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
-    // 3a. x pass over every staged (y, z): rows (ox, y)
-    for (int r = lr; r < TX * EY; r += RZ_THREADS / 32) {
-      const int ox = r / EY, y = r - ox * EY;
-      float w[NT];
-#pragma unroll
-      for (int i = 0; i < NT; ++i) w[i] = w_t[0][ox][i];
-      const float* sp = Sst + ((lo_t[0][ox] - bx) * EY + y) * EZ;
-      for (int z = lz; z < EZ; z += 32) {
-        float acc = 0.f;
-#pragma unroll
-        for (int i = 0; i < NT; ++i) acc = fmaf(w[i], sp[i * EY * EZ + z], acc);
-        T1[r * EZ + z] = acc;
-      }
-    }
-    __syncthreads();
-    if (use_tma && c + 1 < a.C && threadIdx.x == 0) issue(c + 1);  // S is free again
-    // 3b. y pass: rows (ox, oy)
-    for (int r = lr; r < TX * TY; r += RZ_THREADS / 32) {
-      const int ox = r / TY, oy = r - ox * TY;
-      float w[NT];
-#pragma unroll
-      for (int j = 0; j < NT; ++j) w[j] = w_t[1][oy][j];
-      const float* tp = T1 + (ox * EY + (lo_t[1][oy] - by)) * EZ;
-      for (int z = lz; z < EZ; z += 32) {
-        float acc = 0.f;
-#pragma unroll
-        for (int j = 0; j < NT; ++j) acc = fmaf(w[j], tp[j * EZ + z], acc);
-        T2[r * EZ + z] = acc;
-      }
-    }
-    __syncthreads();
-    // 3c. z pass and store: rows (ox, oy), lanes along oz
-    for (int r = lr; r < TX * TY; r += RZ_THREADS / 32) {
-      const int ox = r / TY, oy = r - ox * TY;
-      if (ox >= tn[0] || oy >= tn[1]) continue;
-      const bool inxy = inb_t[0][ox] && inb_t[1][oy];
-      const float* tp = T2 + r * EZ - bz;
-      S* op = out_n + c * a.out_sC + (o0[0] + ox) * a.out_s[0] + (o0[1] + oy) * a.out_s[1] + o0[2] * a.out_s[2];
-      for (int oz = lz; oz < tn[2]; oz += 32) {
-        float acc = 0.f;
-        if (!oob_zero || (inxy && inb_t[2][oz])) {
-          const float* tz = tp + lo_t[2][oz];
-#pragma unroll
-          for (int k = 0; k < NT; ++k) acc = fmaf(w_t[2][oz][k], tz[k], acc);
-        }
-        op[oz * a.out_s[2]] = from_acc<S>(acc);
-      }
-    }
+    if (threadIdx.x == 0) cur = nxt;
     __syncthreads();
   }
 }
@@ -333,9 +464,11 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
+// Working set of a tile: two staging buffers (each padded to 128 bytes, plus
+// 128 bytes to align the first), the x-pass and y-pass results.
 size_t smem_floats(const int (&t)[3], const int (&e)[3]) {
-  return static_cast<size_t>(e[0]) * e[1] * e[2] + static_cast<size_t>(t[0]) * e[1] * e[2] +
-         static_cast<size_t>(t[0]) * t[1] * e[2];
+  const size_t sz = (static_cast<size_t>(e[0]) * e[1] * e[2] + 31) & ~static_cast<size_t>(31);
+  return 32 + 2 * sz + static_cast<size_t>(t[0]) * e[1] * e[2] + static_cast<size_t>(t[0]) * t[1] * e[2];
 }
 
 // Staged extent of a tile edge of T outputs at step `scale` for NT taps:
@@ -363,8 +496,9 @@ bool choose_tile(const double (&scale)[3], int NT, int (&t)[3], int (&e)[3], siz
   return false;
 }
 
-// Largest working set of a tile (floats of dynamic shared memory).
-constexpr size_t RZ_SMEM_FLOATS = 15 * 1024;
+// Largest working set of a tile (floats of dynamic shared memory): three
+// CTAs per SM.
+constexpr size_t RZ_SMEM_FLOATS = 16 * 1024;
 
 template <int NT, class S, bool TMA>
 cudaError_t launch_resize(const ResizeArgs& a, const CUtensorMap& map, size_t smem, int64_t ntiles, cudaStream_t st) {
@@ -381,8 +515,15 @@ cudaError_t launch_resize(const ResizeArgs& a, const CUtensorMap& map, size_t sm
     done.fetch_or(bit);
   }
   if (smem > RZ_SMEM_FLOATS * 4) return cudaErrorInvalidValue;
+  // persistent CTAs: as many as fit on the GPU at once
+  int sms = 0, per_sm = 0;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resize_sep_kernel<NT, S, TMA>, RZ_THREADS, smem)) !=
+      cudaSuccess)
+    return e;
+  const int64_t grid = std::min<int64_t>(ntiles, static_cast<int64_t>(std::max(1, sms * per_sm)));
   ppk::note_kernel(TMA ? "resize_sep_kernel tma" : "resize_sep_kernel", 0, NT - 1, 1);
-  resize_sep_kernel<NT, S, TMA><<<static_cast<unsigned>(ntiles), RZ_THREADS, smem, st>>>(a, map);
+  resize_sep_kernel<NT, S, TMA><<<static_cast<unsigned>(grid), RZ_THREADS, smem, st>>>(a, map);
   return cudaGetLastError();
 }
 
@@ -462,9 +603,10 @@ int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale,
     a.ntile[d] = (a.out_size[d] + tile[d] - 1) / tile[d];
     ntiles *= a.ntile[d];
   }
+  while ((1 << a.zls) < ext[2] / 4 && a.zls < 5) ++a.zls;
   a.order = order[0];
   a.extrapolate = opt->extrapolate;
-  if (ntiles >= (int64_t(1) << 31)) return fail(PP_ERR_UNSUPPORTED, "(): pp_resize: too many tiles");
+  if (ntiles * a.C >= (int64_t(1) << 31)) return fail(PP_ERR_UNSUPPORTED, "(): pp_resize: too many tiles");
 
   // TMA copies need a float32 image with the z axis contiguous, 16-byte
   // aligned rows and the batch and channel axes foldable into one.
@@ -492,8 +634,9 @@ int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale,
   a.use_tma = tma;
   const size_t smem = smem_floats(tile, ext) * 4;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  cudaError_t e = input->dtype == PP_FLOAT32 ? dispatch<float>(order[0], tma, a, map, smem, ntiles, st)
-                                             : dispatch<__nv_bfloat16>(order[0], false, a, map, smem, ntiles, st);
+  const int64_t nitems = ntiles * a.C;
+  cudaError_t e = input->dtype == PP_FLOAT32 ? dispatch<float>(order[0], tma, a, map, smem, nitems, st)
+                                             : dispatch<__nv_bfloat16>(order[0], false, a, map, smem, nitems, st);
   count_launch();
   return cuda_check(e, "resize launch");
 }
