@@ -282,12 +282,21 @@ HBM_SPEC_GBS = 8000.0  # B200 HBM3e specification (the measured copy bandwidth i
 SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a
-# kernel on the default workload (1x3x192^3, cubic, dct2, brick-major
-# order), from one ncu capture of that kernel, keyed by the kernel family /
-# mode / order / channel block that pp_last_kernel reports.  A kernel not
-# listed here reports traffic null.
-MEASURED_TRAFFIC = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one op call
+# on the default workload (1x3x192^3, cubic, dct2, brick-major order), from
+# one ncu capture of its kernels, keyed by the kernel string pp_last_kernel reports after the op.  Pull
+# backward sums its two kernels (brick scatter of the image gradient, brick
+# gather of the grid gradient); push counts the brick scatter alone (its
+# accumulator-to-output copy, store_interleaved_vox, is not included).  A
+# kernel not listed here reports traffic null.
+MEASURED_TRAFFIC = {
+    "pp_brick_gather_kernel mode=0 order=3 cb=3": 279_590_400,
+    "pp_brick_scatter_kernel mode=2 order=3 cb=3": 403_078_400,
+    "pp_kernel mode=4 order=3 cb=3": 485_229_056,
+    "pp_brick_gather_kernel mode=5 order=3 cb=3": 404_008_704 + 361_909_504,
+    # resize 1x3x256^3 -> 320^3, cubic, dct2
+    "resize_sep_kernel tma mode=0 order=3 cb=1": 566_675_200,
+}
 
 
 def roofline(ops, labels, nvox, C, ms_per_step, traffic):
@@ -296,7 +305,7 @@ def roofline(ops, labels, nvox, C, ms_per_step, traffic):
     kernel = ops[dom].get("kernel", "")
     traffic_src = "--traffic" if traffic is not None else None
     if traffic is None and kernel in MEASURED_TRAFFIC and nvox == 192 ** 3 and C == 3:
-        traffic, traffic_src = MEASURED_TRAFFIC[kernel], f"ncu capture of {kernel} on this workload"
+        traffic, traffic_src = MEASURED_TRAFFIC[kernel], f"ncu capture of the {dom} kernels (last: {kernel}) on this workload"
     per = algo_bytes(dom, 4, C) * nvox
     achieved = per / (ops[dom]["avg_ms"] * 1e-3) / 1e9
     step_bytes = sum(algo_bytes(k, 4, C) for k in labels) * nvox
@@ -412,7 +421,7 @@ def run_b200(args, rank, world, device):
         }
 
     chain = measure(step, OpTimer.CHAIN, True, args.traffic)
-    fused = measure(step_fused, OpTimer.FUSED, False, None)
+    fused = None if args.no_fused else measure(step_fused, OpTimer.FUSED, False, None)
     if rank != 0:
         return None
 
@@ -432,10 +441,11 @@ def run_b200(args, rank, world, device):
         "gpu_launches": chain["gpu_launches"],
         "gpu_launches_per_step": chain["gpu_launches_per_step"],
         "clocks": chain["clocks"],
-        "fused": {"api": "pull_push (fused normal operator, same outputs), autograd",
-                  **{k: fused[k] for k in ("value", "ms_per_step", "e2e", "roofline", "ops", "gpu_launches",
-                                           "gpu_launches_per_step")}},
     }
+    if fused is not None:
+        line["fused"] = {"api": "pull_push (fused normal operator, same outputs), autograd",
+                         **{k: fused[k] for k in ("value", "ms_per_step", "e2e", "roofline", "ops", "gpu_launches",
+                                                  "gpu_launches_per_step")}}
     if not args.no_reference_cuda and world == 1:
         line["reference_cuda"] = reference_cuda_leg(args, device, x, grid, w, chain["ms_per_step"])
     if not args.no_cpu_baseline:
@@ -668,13 +678,15 @@ def run_resize(args, rank, world, device):
             "kernel": kernel, "ms": round(sep, 4), "value": round(nvox / (sep * 1e-3) / 1e9, 3), "unit": "Gvox/s",
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "peak_source": src, "algorithmic_bytes_per_launch": algo,
-                         "traffic": None},
+                         "traffic": MEASURED_TRAFFIC.get(kernel)},
             "per_point_affine_pull_ms": round(per_point, 4), "speedup_over_per_point": round(per_point / sep, 2),
             "max_rel_diff_vs_per_point": diff, "resize_status": affine.resize_status()}
 
 
 def run_all(args, rank, world, device):
     import gc
+    if args.only_resize:
+        return {"resize": run_resize(args, rank, world, device)} if rank == 0 else None
     line = run_b200(args, rank, world, device)
     gc.collect()
     torch.cuda.empty_cache()
@@ -865,6 +877,8 @@ def main():
     ap.add_argument("--batch-volumes", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3)
     ap.add_argument("--no-svf", action="store_true")
+    ap.add_argument("--no-fused", action="store_true", help="skip the fused pull_push leg")
+    ap.add_argument("--only-resize", action="store_true", help="run the resize leg alone")
     ap.add_argument("--no-resize", action="store_true")
     ap.add_argument("--svf-steps", type=int, default=5)
     ap.add_argument("--traffic", type=float, default=None,
