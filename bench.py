@@ -789,17 +789,31 @@ def reference_cuda_leg(args, device, x, grid, w, ours_ms):
     b, o = [ref.BoundType.dct2], [ref.InterpolationType.cubic]
     l2buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
+    marks = []  # (op, event) after each op of a step
+
+    def mark(op):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        marks.append((op, ev))
+
     def chain():
         c = nb.spline_coeff_nd(x.detach(), ORDER, BOUND, dim=3)
+        mark("prefilter")
         y = ref.grid_pull(c, grid.detach(), b, o, 0)
+        mark("pull_fwd")
         z = ref.grid_push(y, grid.detach(), list(x.shape[2:]), b, o, 0)
+        mark("push_fwd")
         loss = (z * w).sum()
         yr = y.detach().requires_grad_(True)
         gr = grid.detach().requires_grad_(True)
+        mark("loss")
         dy, dg1 = ref.grid_push_backward(w, yr, gr, b, o, 0)
+        mark("push_bwd")
         cr = c.detach().requires_grad_(True)
         dc, dg2 = ref.grid_pull_backward(dy, cr, gr, b, o, 0)
+        mark("pull_bwd")
         dx = nb.spline_coeff_nd(dc, ORDER, BOUND, dim=3)
+        mark("prefilter_bwd")
         return z, dx, dg1 + dg2, loss
 
     for _ in range(max(1, min(args.warmup, 3))):
@@ -807,14 +821,23 @@ def reference_cuda_leg(args, device, x, grid, w, ours_ms):
     torch.cuda.synchronize()
     steps = max(1, min(args.steps, 5))
     ts = []
+    per_op = {}
+    clocks = ClockSampler(device.index or 0)
+    clocks.start()
     for _ in range(steps):
         l2buf.zero_()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        marks.clear()
         s.record()
         out = chain()
         e.record()
         torch.cuda.synchronize()
         ts.append(s.elapsed_time(e))
+        prev = s
+        for op, ev in marks:
+            per_op.setdefault(op, []).append(prev.elapsed_time(ev))
+            prev = ev
+    clk = clocks.stop()
     ms = float(np.mean(ts))
     # this library's outputs on the same inputs
     xr = x.detach().requires_grad_(True)
@@ -828,6 +851,7 @@ def reference_cuda_leg(args, device, x, grid, w, ours_ms):
     nvox = int(np.prod(x.shape[2:]))
     return {"ms_per_step": round(ms, 4), "value": round(nvox / (ms * 1e-3) / 1e9, 4), "unit": "Gvox/s",
             "steps": steps, "speedup_of_this_library": round(ms / ours_ms, 2),
+            "ops_ms": {k: round(float(np.mean(v)), 4) for k, v in per_op.items()}, "clocks": clk,
             "max_rel_diff_vs_this_library": diff,
             "note": "nitorch's CUDA pushpull_kernel built for sm_100a from the reference sources; "
                     "prefilter from this library"}
