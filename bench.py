@@ -284,16 +284,14 @@ SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one op call
 # on the default workload (1x3x192^3, cubic, dct2, brick-major order), from
-# one ncu capture of its kernels, keyed by the kernel string pp_last_kernel reports after the op.  Pull
-# backward sums its two kernels (brick scatter of the image gradient, brick
-# gather of the grid gradient); push counts the brick scatter alone (its
+# one ncu capture of its kernels, keyed by the kernel string pp_last_kernel
+# reports after the op.  Push counts the brick scatter alone (its
 # accumulator-to-output copy, store_interleaved_vox, is not included).  A
 # kernel not listed here reports traffic null.
 MEASURED_TRAFFIC = {
     "pp_brick_gather_kernel mode=0 order=3 cb=3": 279_590_400,
     "pp_brick_scatter_kernel mode=2 order=3 cb=3": 403_078_400,
     "pp_kernel mode=4 order=3 cb=3": 485_229_056,
-    "pp_brick_gather_kernel mode=5 order=3 cb=3": 404_008_704 + 361_909_504,
     # resize 1x3x256^3 -> 320^3, cubic, dct2
     "resize_sep_kernel tma mode=0 order=3 cb=1": 566_675_200,
 }

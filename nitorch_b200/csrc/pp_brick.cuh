@@ -31,6 +31,11 @@
 // applied per window voxel: value times sign), then each thread takes one
 // point and gathers its 64 taps from the window at compile-time offsets.
 //
+// pp_brick_pullbwd_kernel (the pull's backward pass with both outputs) does
+// the two in one pass over a brick's points: each point's coordinates and
+// incoming gradient are read once for the gather of the grid gradient and
+// the scatter of the image gradient.
+//
 // Points whose support leaves the window (sampling outside the volume with
 // extrapolation, or just below a volume edge) and points outside the field
 // of view run the per-point body pp_point with global memory instead.
@@ -192,6 +197,205 @@ __device__ __forceinline__ BrickPoint brick_point(const PPArgs& a, int p, const 
 }
 
 // ===========================================================================
+// Pieces shared by the brick kernels.
+// ===========================================================================
+
+// Weights, target values and window offset of one point, written to its
+// shared scatter record (layout above).
+__device__ __forceinline__ void write_record(const BrickPoint& q, const BrickPos& bp, const float (&w)[3][4],
+                                             const float (&t)[4], float* rr) {
+  using W = BrickWin;
+  *reinterpret_cast<float4*>(rr + 0) = make_float4(w[0][0], w[0][1], w[0][2], w[0][3]);
+  *reinterpret_cast<float4*>(rr + 4) = make_float4(w[1][0], w[1][1], w[1][2], w[1][3]);
+  *reinterpret_cast<float4*>(rr + 8) = make_float4(w[2][0], w[2][2], w[2][1], w[2][3]);
+  *reinterpret_cast<float4*>(rr + 12) = make_float4(t[0], t[1], t[2], t[3]);
+  rr[16] = __int_as_float((q.lo[0] - bp.ox) * W::PX + (q.lo[1] - bp.oy) * W::PY + (q.lo[2] - bp.oz));
+}
+
+// The warp walks its recorded points (bit set in `todo`) one at a time,
+// lane (i, j, kk) adding taps (i, j, kk) and (i, j, kk + 2) of the 4x4x4
+// support into the warp's accumulator window.
+template <int CP>
+__device__ __forceinline__ void scatter_recorded(float* acc, const float* rec, unsigned todo, int lane) {
+  using W = BrickWin;
+  const int ti = lane >> 3, tj = (lane >> 1) & 3, tk = lane & 1;
+  const int loff = ti * W::PX + tj * W::PY + tk;
+  while (todo) {
+    const int q = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const float* rr = rec + q * BRK_REC;
+    const float wxy = rr[ti] * rr[4 + tj];
+    const float2 zp = *reinterpret_cast<const float2*>(rr + 8 + 2 * tk);  // (wz_k, wz_k+2)
+    float t[CP];
+    {
+      const float4 tq = *reinterpret_cast<const float4*>(rr + 12);
+      const float tt[4] = {tq.x, tq.y, tq.z, tq.w};
+#pragma unroll
+      for (int c = 0; c < CP; ++c) t[c] = tt[c];
+    }
+    const int off0 = (__float_as_int(rr[16]) + loff) * CP;
+    vaxpy<CP>(acc + off0, wxy * zp.x, t);
+    vaxpy<CP>(acc + off0 + 2 * CP, wxy * zp.y, t);
+    __syncwarp();
+  }
+}
+
+// Add NACC accumulator windows (`stride` floats apart) of brick bp to the
+// output: one vector reduction per touched window voxel, boundary index and
+// sign applied; threads `tid` of `nthreads`.
+template <int CP, int NACC>
+__device__ __forceinline__ void flush_windows(const PPArgs& a, const BrickPos& bp, const float* acc, int stride,
+                                              int tid, int nthreads) {
+  using W = BrickWin;
+  float* out_n = static_cast<float*>(a.out) + static_cast<int64_t>(bp.n) * a.out_sN;
+  const bool vec = (a.flags & F_VEC) != 0;
+  const int64_t os[3] = {a.out_s[0], a.out_s[1], a.out_s[2]};
+  for (int e = tid; e < W::NE; e += nthreads) {
+    int wx, wy, wz;
+    win_coords(e, wx, wy, wz);
+    const int o = (wx * W::PX + wy * W::PY + wz) * CP;
+    float v[CP];
+    vload<CP>(acc + o, v);
+#pragma unroll
+    for (int k = 1; k < NACC; ++k) {
+      float u[CP];
+      vload<CP>(acc + k * stride + o, u);
+#pragma unroll
+      for (int c = 0; c < CP; ++c) v[c] += u[c];
+    }
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < CP; ++c) any = any || v[c] != 0.f;
+    if (!any) continue;
+    int sgn;
+    const int64_t off = bound_offset(a, bp.ox + wx, bp.oy + wy, bp.oz + wz, os, bp.interior, sgn);
+    if (sgn == 0) continue;
+    if (sgn < 0) {
+#pragma unroll
+      for (int c = 0; c < CP; ++c) v[c] = -v[c];
+    }
+    if constexpr (CP >= 2) {
+      if (vec) {
+        red_vec<CP>(out_n + off, v);
+        continue;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CP; ++c)
+      if (c < a.C && v[c] != 0.f) atomicAdd(out_n + c * a.out_sC + off, v[c]);
+  }
+}
+
+// Stage the source window of brick bp at GatherWin pitches (value times
+// boundary sign; 0 outside): every thread issues all of its loads before
+// its first shared store.
+template <int CB, int CP, class S>
+__device__ __forceinline__ void stage_window(const PPArgs& a, const BrickPos& bp, float* img) {
+  using W = BrickWin;
+  using G = GatherWin;
+  constexpr int NIT = (W::NE + BRK_GATHER_THREADS - 1) / BRK_GATHER_THREADS;
+  const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(bp.n) * a.src_sN;
+  const int64_t ss[3] = {a.src_s[0], a.src_s[1], a.src_s[2]};
+  float v[NIT][CP];
+  int dst[NIT];
+#pragma unroll
+  for (int it = 0; it < NIT; ++it) {
+    const int e = static_cast<int>(threadIdx.x) + it * BRK_GATHER_THREADS;
+#pragma unroll
+    for (int c = 0; c < CP; ++c) v[it][c] = 0.f;
+    dst[it] = -1;
+    if (e < W::NE) {
+      int wx, wy, wz;
+      win_coords(e, wx, wy, wz);
+      dst[it] = (wx * G::PX + wy * G::PY + wz) * CP;
+      int sgn;
+      const int64_t so = bound_offset(a, bp.ox + wx, bp.oy + wy, bp.oz + wz, ss, bp.interior, sgn);
+      if (sgn != 0) {
+#pragma unroll
+        for (int c = 0; c < CP; ++c)
+          if (c < CB && c < a.C)
+            v[it][c] = static_cast<float>(sgn) * static_cast<float>(ldg_acc(src_n + c * a.src_sC + so));
+      }
+    }
+  }
+#pragma unroll
+  for (int it = 0; it < NIT; ++it)
+    if (dst[it] >= 0) vstore<CP>(img + dst[it], v[it]);
+}
+
+// One point's 64-tap gather from the staged window `ib` (its lowest node):
+// separable partial sums, x innermost; per channel the interpolant (VAL),
+// and for the grid gradient (GG) the dot product with t under w and dw.
+template <int CB, int CP, bool VAL, bool GG>
+__device__ __forceinline__ void gather_taps(const float* ib, const float (&w)[3][4], const float (&g)[3][4],
+                                            const float (&t)[CP], float (&val)[CP], float& gx, float& gy,
+                                            float& gz) {
+  using G = GatherWin;
+  gx = gy = gz = 0.f;
+#pragma unroll
+  for (int c = 0; c < CP; ++c) val[c] = 0.f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float yv[CP], yw = 0.f, ygx = 0.f, ygy = 0.f;
+#pragma unroll
+    for (int c = 0; c < CP; ++c) yv[c] = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float xv[CP], sx = 0.f, sdx = 0.f;
+#pragma unroll
+      for (int c = 0; c < CP; ++c) xv[c] = 0.f;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        float iv[CP];
+        vload<CP>(ib + (i * G::PX + j * G::PY + k) * CP, iv);
+        if (VAL) {
+#pragma unroll
+          for (int c = 0; c < CP; ++c)
+            if (c < CB) xv[c] = fmaf(w[0][i], iv[c], xv[c]);
+        }
+        if (GG) {
+          float dot = 0.f;
+#pragma unroll
+          for (int c = 0; c < CP; ++c)
+            if (c < CB) dot = fmaf(t[c], iv[c], dot);
+          sx = fmaf(w[0][i], dot, sx);
+          sdx = fmaf(g[0][i], dot, sdx);
+        }
+      }
+      if (VAL) {
+#pragma unroll
+        for (int c = 0; c < CP; ++c)
+          if (c < CB) yv[c] = fmaf(w[1][j], xv[c], yv[c]);
+      }
+      if (GG) {
+        yw = fmaf(w[1][j], sx, yw);
+        ygx = fmaf(w[1][j], sdx, ygx);
+        ygy = fmaf(g[1][j], sx, ygy);
+      }
+    }
+    if (VAL) {
+#pragma unroll
+      for (int c = 0; c < CP; ++c)
+        if (c < CB) val[c] = fmaf(w[2][k], yv[c], val[c]);
+    }
+    if (GG) {
+      gx = fmaf(w[2][k], ygx, gx);
+      gy = fmaf(w[2][k], ygy, gy);
+      gz = fmaf(g[2][k], yw, gz);
+    }
+  }
+}
+
+// The target values of a point (CB channels, zero in the other slots).
+template <int CB, int NS, class S>
+__device__ __forceinline__ void load_target(const PPArgs& a, const BrickPoint& q, float (&t)[NS]) {
+  const S* tp = static_cast<const S*>(a.trgt) + static_cast<int64_t>(q.n) * a.trgt_sN + q.sub[0] * a.trgt_s[0] +
+                q.sub[1] * a.trgt_s[1] + q.sub[2] * a.trgt_s[2];
+#pragma unroll
+  for (int c = 0; c < NS; ++c) t[c] = (c < CB && c < a.C) ? static_cast<float>(ldg_acc(tp + c * a.trgt_sC)) : 0.f;
+}
+
+// ===========================================================================
 // Scatter: one warp per brick (see the file comment).  CB: channel block of
 // the per-point fallback body (= C for C <= 4); CP: channel slots per window
 // voxel (1 for C = 1, 2 for C = 2, 4 for C = 3-4).
@@ -219,10 +423,6 @@ __global__ void __launch_bounds__(32 * BRK_SCATTER_WARPS) pp_brick_scatter_kerne
   }
   __syncwarp();
 
-  // this lane's taps inside a point's 4x4x4 support
-  const int ti = lane >> 3, tj = (lane >> 1) & 3, tk = lane & 1;
-  const int loff = ti * W::PX + tj * W::PY + tk;
-
   for (int c0 = p0; c0 < p1; c0 += 32) {
     const int p = c0 + lane;
     bool mine = false;
@@ -237,72 +437,16 @@ __global__ void __launch_bounds__(32 * BRK_SCATTER_WARPS) pp_brick_scatter_kerne
         for (int d = 0; d < 3; ++d)
           bspline_stencil<4, false, false, float>(3, q.x[d] - static_cast<float>(q.lo[d] + 1), w[d], g[d], h[d]);
         float t[4] = {1.f, 0.f, 0.f, 0.f};
-        if (MODE != K_COUNT) {
-          const S* tp = static_cast<const S*>(a.trgt) + static_cast<int64_t>(q.n) * a.trgt_sN +
-                        q.sub[0] * a.trgt_s[0] + q.sub[1] * a.trgt_s[1] + q.sub[2] * a.trgt_s[2];
-#pragma unroll
-          for (int c = 0; c < 4; ++c) t[c] = (c < CB && c < a.C) ? static_cast<float>(ldg_acc(tp + c * a.trgt_sC)) : 0.f;
-        }
-        float* rr = rec + lane * BRK_REC;
-        *reinterpret_cast<float4*>(rr + 0) = make_float4(w[0][0], w[0][1], w[0][2], w[0][3]);
-        *reinterpret_cast<float4*>(rr + 4) = make_float4(w[1][0], w[1][1], w[1][2], w[1][3]);
-        *reinterpret_cast<float4*>(rr + 8) = make_float4(w[2][0], w[2][2], w[2][1], w[2][3]);
-        *reinterpret_cast<float4*>(rr + 12) = make_float4(t[0], t[1], t[2], t[3]);
-        rr[16] = __int_as_float((q.lo[0] - bp.ox) * W::PX + (q.lo[1] - bp.oy) * W::PY + (q.lo[2] - bp.oz));
+        if (MODE != K_COUNT) load_target<CB, 4, S>(a, q, t);
+        write_record(q, bp, w, t, rec + lane * BRK_REC);
       }
     }
-    unsigned todo = __ballot_sync(0xffffffffu, mine);
+    const unsigned todo = __ballot_sync(0xffffffffu, mine);
     __syncwarp();
-    while (todo) {
-      const int q = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const float* rr = rec + q * BRK_REC;
-      const float wxy = rr[ti] * rr[4 + tj];
-      const float2 zp = *reinterpret_cast<const float2*>(rr + 8 + 2 * tk);  // (wz_k, wz_k+2)
-      float t[CP];
-      {
-        const float4 tq = *reinterpret_cast<const float4*>(rr + 12);
-        const float tt[4] = {tq.x, tq.y, tq.z, tq.w};
-#pragma unroll
-        for (int c = 0; c < CP; ++c) t[c] = tt[c];
-      }
-      const int off0 = (__float_as_int(rr[16]) + loff) * CP;
-      vaxpy<CP>(acc + off0, wxy * zp.x, t);
-      vaxpy<CP>(acc + off0 + 2 * CP, wxy * zp.y, t);
-      __syncwarp();
-    }
+    scatter_recorded<CP>(acc, rec, todo, lane);
   }
 
-  // flush the accumulator window
-  float* out_n = static_cast<float*>(a.out) + static_cast<int64_t>(bp.n) * a.out_sN;
-  const bool vec = (a.flags & F_VEC) != 0;
-  const int64_t os[3] = {a.out_s[0], a.out_s[1], a.out_s[2]};
-  for (int e = lane; e < W::NE; e += 32) {
-    int wx, wy, wz;
-    win_coords(e, wx, wy, wz);
-    float v[CP];
-    vload<CP>(acc + (wx * W::PX + wy * W::PY + wz) * CP, v);
-    bool any = false;
-#pragma unroll
-    for (int c = 0; c < CP; ++c) any = any || v[c] != 0.f;
-    if (!any) continue;
-    int sgn;
-    const int64_t off = bound_offset(a, bp.ox + wx, bp.oy + wy, bp.oz + wz, os, bp.interior, sgn);
-    if (sgn == 0) continue;
-    if (sgn < 0) {
-#pragma unroll
-      for (int c = 0; c < CP; ++c) v[c] = -v[c];
-    }
-    if constexpr (CP >= 2) {
-      if (vec) {
-        red_vec<CP>(out_n + off, v);
-        continue;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < CP; ++c)
-      if (c < a.C && v[c] != 0.f) atomicAdd(out_n + c * a.out_sC + off, v[c]);
-  }
+  flush_windows<CP, 1>(a, bp, acc, 0, lane, 32);
 }
 
 // ===========================================================================
@@ -315,7 +459,6 @@ __global__ void __launch_bounds__(32 * BRK_SCATTER_WARPS) pp_brick_scatter_kerne
 template <int MODE, int CB, int CP, class S>
 __global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
     pp_brick_gather_kernel(const PPArgs a) {
-  using W = BrickWin;
   using G = GatherWin;
   static_assert(MODE == K_PULL || MODE == K_PUSHGRAD, "gather modes");
   constexpr bool GG = MODE != K_PULL;
@@ -329,38 +472,7 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
   constexpr bool want_val = MODE == K_PULL;
   const bool want_gg = GG && (a.flags & F_GRAD) != 0;
 
-  // stage the source window (value times boundary sign; 0 outside): every
-  // thread issues all of its loads before its first shared store
-  {
-    constexpr int NIT = (W::NE + BRK_GATHER_THREADS - 1) / BRK_GATHER_THREADS;
-    const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(bp.n) * a.src_sN;
-    const int64_t ss[3] = {a.src_s[0], a.src_s[1], a.src_s[2]};
-    float v[NIT][CP];
-    int dst[NIT];
-#pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int e = static_cast<int>(threadIdx.x) + it * BRK_GATHER_THREADS;
-#pragma unroll
-      for (int c = 0; c < CP; ++c) v[it][c] = 0.f;
-      dst[it] = -1;
-      if (e < W::NE) {
-        int wx, wy, wz;
-        win_coords(e, wx, wy, wz);
-        dst[it] = (wx * G::PX + wy * G::PY + wz) * CP;
-        int sgn;
-        const int64_t so = bound_offset(a, bp.ox + wx, bp.oy + wy, bp.oz + wz, ss, bp.interior, sgn);
-        if (sgn != 0) {
-#pragma unroll
-          for (int c = 0; c < CP; ++c)
-            if (c < CB && c < a.C)
-              v[it][c] = static_cast<float>(sgn) * static_cast<float>(ldg_acc(src_n + c * a.src_sC + so));
-        }
-      }
-    }
-#pragma unroll
-    for (int it = 0; it < NIT; ++it)
-      if (dst[it] >= 0) vstore<CP>(img + dst[it], v[it]);
-  }
+  stage_window<CB, CP, S>(a, bp, img);
   __syncthreads();
 
   for (int p = p0 + static_cast<int>(threadIdx.x); p < p1; p += BRK_GATHER_THREADS) {
@@ -376,70 +488,11 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
     float t[CP];
 #pragma unroll
     for (int c = 0; c < CP; ++c) t[c] = 0.f;
-    if (GG && want_gg) {
-      const S* tp = static_cast<const S*>(a.trgt) + static_cast<int64_t>(q.n) * a.trgt_sN +
-                    q.sub[0] * a.trgt_s[0] + q.sub[1] * a.trgt_s[1] + q.sub[2] * a.trgt_s[2];
-#pragma unroll
-      for (int c = 0; c < CP; ++c)
-        if (c < CB && c < a.C) t[c] = static_cast<float>(ldg_acc(tp + c * a.trgt_sC));
-    }
+    if (GG && want_gg) load_target<CB, CP, S>(a, q, t);
     const float* ib = img + ((q.lo[0] - bp.ox) * G::PX + (q.lo[1] - bp.oy) * G::PY + (q.lo[2] - bp.oz)) * CP;
-    // separable partial sums, x innermost: per channel the interpolant, and
-    // for the grid gradient the dot product with t under w and dw
-    float val[CP], gx = 0.f, gy = 0.f, gz = 0.f;
-#pragma unroll
-    for (int c = 0; c < CP; ++c) val[c] = 0.f;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      float yv[CP], yw = 0.f, ygx = 0.f, ygy = 0.f;
-#pragma unroll
-      for (int c = 0; c < CP; ++c) yv[c] = 0.f;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        float xv[CP], sx = 0.f, sdx = 0.f;
-#pragma unroll
-        for (int c = 0; c < CP; ++c) xv[c] = 0.f;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          float iv[CP];
-          vload<CP>(ib + (i * G::PX + j * G::PY + k) * CP, iv);
-          if (want_val) {
-#pragma unroll
-            for (int c = 0; c < CP; ++c)
-              if (c < CB) xv[c] = fmaf(w[0][i], iv[c], xv[c]);
-          }
-          if (GG && want_gg) {
-            float dot = 0.f;
-#pragma unroll
-            for (int c = 0; c < CP; ++c)
-              if (c < CB) dot = fmaf(t[c], iv[c], dot);
-            sx = fmaf(w[0][i], dot, sx);
-            sdx = fmaf(g[0][i], dot, sdx);
-          }
-        }
-        if (want_val) {
-#pragma unroll
-          for (int c = 0; c < CP; ++c)
-            if (c < CB) yv[c] = fmaf(w[1][j], xv[c], yv[c]);
-        }
-        if (GG && want_gg) {
-          yw = fmaf(w[1][j], sx, yw);
-          ygx = fmaf(w[1][j], sdx, ygx);
-          ygy = fmaf(g[1][j], sx, ygy);
-        }
-      }
-      if (want_val) {
-#pragma unroll
-        for (int c = 0; c < CP; ++c)
-          if (c < CB) val[c] = fmaf(w[2][k], yv[c], val[c]);
-      }
-      if (GG && want_gg) {
-        gx = fmaf(w[2][k], ygx, gx);
-        gy = fmaf(w[2][k], ygy, gy);
-        gz = fmaf(g[2][k], yw, gz);
-      }
-    }
+    float val[CP], gx, gy, gz;
     if (want_val) {
+      gather_taps<CB, CP, true, false>(ib, w, g, t, val, gx, gy, gz);
       S* op = static_cast<S*>(a.out) + static_cast<int64_t>(q.n) * a.out_sN + q.sub[0] * a.out_s[0] +
               q.sub[1] * a.out_s[1] + q.sub[2] * a.out_s[2];
 #pragma unroll
@@ -447,11 +500,90 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
         if (c < CB && c < a.C) op[c * a.out_sC] = from_acc<S>(val[c]);
     }
     if (GG && want_gg) {
+      gather_taps<CB, CP, false, true>(ib, w, g, t, val, gx, gy, gz);
       float* gg = static_cast<float*>(a.gg) + static_cast<int64_t>(q.n) * a.gg_sN + q.sub[0] * a.gg_s[0] +
                   q.sub[1] * a.gg_s[1] + q.sub[2] * a.gg_s[2];
       gg[0] = gx; gg[a.gg_sD] = gy; gg[2 * a.gg_sD] = gz;
     }
   }
+}
+
+// ===========================================================================
+// Pull backward in one pass over a brick's points (flags F_A and F_GRAD):
+// one CTA per brick, one thread per point.  Each point's coordinates and
+// incoming gradient t are read once and serve both outputs:
+//   grid gradient  gg_d = sum_c t[c] sum dw_d src[c]  (gather from the staged
+//                  source window, as pp_brick_gather_kernel)
+//   image gradient out[c] += w t[c]  (scatter: each warp records its lanes'
+//                  points and adds them into its own accumulator window, as
+//                  pp_brick_scatter_kernel; the four windows are summed and
+//                  flushed once at the end)
+// ===========================================================================
+template <int CB, int CP> struct PullBwdSmem {
+  static constexpr int ACC = BrickWin::NV * CP;  // floats per accumulator window
+  static constexpr int IMG = GatherWin::NV * CP;
+  static constexpr int NWARP = BRK_GATHER_THREADS / 32;
+  static constexpr size_t bytes = (size_t(IMG) + size_t(NWARP) * (ACC + 32 * BRK_REC)) * 4;
+};
+
+template <int CB, int CP, class S>
+__global__ void __launch_bounds__(BRK_GATHER_THREADS, 4) pp_brick_pullbwd_kernel(const PPArgs a) {
+  using W = BrickWin;
+  using G = GatherWin;
+  using SM = PullBwdSmem<CB, CP>;
+  extern __shared__ float4 brick_smem4[];
+  float* img = reinterpret_cast<float*>(brick_smem4);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  float* acc0 = img + SM::IMG;                 // NWARP windows, SM::ACC floats apart
+  float* acc = acc0 + wid * SM::ACC;
+  float* rec = acc0 + SM::NWARP * SM::ACC + wid * (32 * BRK_REC);
+
+  const int64_t b = blockIdx.x;
+  const int p0 = __ldg(a.brick_start + b), p1 = __ldg(a.brick_start + b + 1);
+  if (p0 >= p1) return;  // whole CTA
+  const BrickPos bp = brick_pos(a, b);
+
+  stage_window<CB, CP, S>(a, bp, img);
+  {
+    float4* a4 = reinterpret_cast<float4*>(acc0);
+    for (int e = threadIdx.x; e < SM::NWARP * SM::ACC / 4; e += BRK_GATHER_THREADS)
+      a4[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+
+  for (int c0 = p0; c0 < p1; c0 += BRK_GATHER_THREADS) {
+    const int p = c0 + static_cast<int>(threadIdx.x);
+    bool mine = false;
+    if (p < p1) {
+      const BrickPoint q = brick_point(a, p, bp);
+      if (!q.fits) {
+        pp_point<3, 3, CB, S, K_PUSHGRAD, int>(a, q.sub, q.n);  // both outputs, global memory
+      } else {
+        mine = true;
+        float w[3][4], g[3][4], h[3][4];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+          bspline_stencil<4, true, false, float>(3, q.x[d] - static_cast<float>(q.lo[d] + 1), w[d], g[d], h[d]);
+        float t4[4];
+        load_target<CB, 4, S>(a, q, t4);
+        float t[CP];
+#pragma unroll
+        for (int c = 0; c < CP; ++c) t[c] = t4[c];
+        const float* ib = img + ((q.lo[0] - bp.ox) * G::PX + (q.lo[1] - bp.oy) * G::PY + (q.lo[2] - bp.oz)) * CP;
+        float val[CP], gx, gy, gz;
+        gather_taps<CB, CP, false, true>(ib, w, g, t, val, gx, gy, gz);
+        float* gg = static_cast<float*>(a.gg) + static_cast<int64_t>(q.n) * a.gg_sN + q.sub[0] * a.gg_s[0] +
+                    q.sub[1] * a.gg_s[1] + q.sub[2] * a.gg_s[2];
+        gg[0] = gx; gg[a.gg_sD] = gy; gg[2 * a.gg_sD] = gz;
+        write_record(q, bp, w, t4, rec + lane * BRK_REC);
+      }
+    }
+    const unsigned todo = __ballot_sync(0xffffffffu, mine);
+    __syncwarp();
+    scatter_recorded<CP>(acc, rec, todo, lane);
+  }
+  __syncthreads();
+  flush_windows<CP, SM::NWARP>(a, bp, acc0, SM::ACC, static_cast<int>(threadIdx.x), BRK_GATHER_THREADS);
 }
 
 }  // namespace ppk

@@ -1307,9 +1307,24 @@ inline cudaError_t launch_brick_gather(const PPArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <int CB, class S>
+inline cudaError_t launch_brick_pullbwd(const PPArgs& a, cudaStream_t st) {
+  constexpr int CP = CB == 1 ? 1 : (CB == 2 ? 2 : 4);
+  constexpr size_t bytes = PullBwdSmem<CB, CP>::bytes;
+  const int64_t nb = a.N * a.nbrick[0] * a.nbrick[1] * a.nbrick[2];
+  if (nb <= 0) return cudaSuccess;
+  if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  static std::atomic<unsigned long long> optin_done{0};
+  cudaError_t e = brick_smem_optin(pp_brick_pullbwd_kernel<CB, CP, S>, bytes, optin_done);
+  if (e != cudaSuccess) return e;
+  note_kernel("pp_brick_pullbwd_kernel", K_PUSHGRAD, 3, CB);
+  pp_brick_pullbwd_kernel<CB, CP, S><<<static_cast<unsigned>(nb), BRK_GATHER_THREADS, bytes, st>>>(a);
+  return cudaGetLastError();
+}
+
 // Brick kernels of one mode: push / count scatter; pull gather; pull
 // backward = the scatter of the incoming gradient (image gradient) plus the
-// gather of the grid gradient.
+// gather of the grid gradient, in one kernel when both are wanted.
 template <int MODE, int CB, class S>
 inline cudaError_t launch_brick(const PPArgs& a, cudaStream_t st) {
   if constexpr (MODE == K_PUSH || MODE == K_COUNT) {
@@ -1318,6 +1333,7 @@ inline cudaError_t launch_brick(const PPArgs& a, cudaStream_t st) {
     return launch_brick_gather<MODE, CB, S>(a, st);
   } else {
     static_assert(MODE == K_PUSHGRAD, "brick modes");
+    if ((a.flags & F_A) && (a.flags & F_GRAD)) return launch_brick_pullbwd<CB, S>(a, st);
     if (a.flags & F_A) {
       PPArgs s = a;
       s.flags &= ~F_GRAD;

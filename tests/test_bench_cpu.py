@@ -37,7 +37,7 @@ def test_clock_parse_falls_back_to_the_last_sample():
     assert bench.ClockSampler.parse(["garbage\n"], skip=0) is None
 
 
-KERNEL = "pp_brick_gather_kernel mode=5 order=3 cb=3"
+KERNEL = "pp_brick_pullbwd_kernel mode=5 order=3 cb=3"
 
 
 def _ops(pull_bwd_ms):

@@ -75,7 +75,7 @@ def test_config2_pull_and_grid_gradients_pointwise():
 
     cr = c.detach().requires_grad_(True)
     _, dg2 = spatial.grid_pull_backward(t, cr, gr, B, OR, 0)
-    assert _lib.last_kernel().startswith("pp_brick_gather_kernel"), _lib.last_kernel()
+    assert _lib.last_kernel().startswith("pp_brick_pullbwd_kernel"), _lib.last_kernel()
     tsub = _at(t, d["pts"]).reshape(1, 3, 512, 1, 1)
     ref2 = O.grid_pull_backward(tsub, d["c64"], gsub, [2], [3], 0, need_input=False)[0].reshape(1, 512, 3)
     assert relerr(_at_grid(dg2, d["pts"]), ref2) < 1e-5
