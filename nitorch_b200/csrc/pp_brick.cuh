@@ -523,6 +523,7 @@ template <int CB, int CP> struct PullBwdSmem {
   static constexpr int ACC = BrickWin::NV * CP;  // floats per accumulator window
   static constexpr int IMG = GatherWin::NV * CP;
   static constexpr int NWARP = BRK_GATHER_THREADS / 32;
+  static_assert(NWARP == 4, "the scatter shares points out by k mod 4 (mask 0x11111111 << warp)");
   static constexpr size_t bytes = (size_t(IMG) + size_t(NWARP) * (ACC + 32 * BRK_REC)) * 4;
 };
 
@@ -532,11 +533,12 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, 4) pp_brick_pullbwd_kernel
   using G = GatherWin;
   using SM = PullBwdSmem<CB, CP>;
   extern __shared__ float4 brick_smem4[];
+  __shared__ unsigned recorded[SM::NWARP];     // per warp: lanes that recorded a point
   float* img = reinterpret_cast<float*>(brick_smem4);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float* acc0 = img + SM::IMG;                 // NWARP windows, SM::ACC floats apart
   float* acc = acc0 + wid * SM::ACC;
-  float* rec = acc0 + SM::NWARP * SM::ACC + wid * (32 * BRK_REC);
+  float* rec = acc0 + SM::NWARP * SM::ACC;     // one record per thread of the CTA
 
   const int64_t b = blockIdx.x;
   const int p0 = __ldg(a.brick_start + b), p1 = __ldg(a.brick_start + b + 1);
@@ -575,14 +577,18 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, 4) pp_brick_pullbwd_kernel
         float* gg = static_cast<float*>(a.gg) + static_cast<int64_t>(q.n) * a.gg_sN + q.sub[0] * a.gg_s[0] +
                     q.sub[1] * a.gg_s[1] + q.sub[2] * a.gg_s[2];
         gg[0] = gx; gg[a.gg_sD] = gy; gg[2 * a.gg_sD] = gz;
-        write_record(q, bp, w, t4, rec + lane * BRK_REC);
+        write_record(q, bp, w, t4, rec + threadIdx.x * BRK_REC);
       }
     }
-    const unsigned todo = __ballot_sync(0xffffffffu, mine);
-    __syncwarp();
-    scatter_recorded<CP>(acc, rec, todo, lane);
+    const unsigned m = __ballot_sync(0xffffffffu, mine);
+    if (lane == 0) recorded[wid] = m;
+    __syncthreads();
+    // warp w adds the recorded points k = w (mod NWARP) of this pass into
+    // its own window: an even share whatever the number of points
+    for (int s = 0; s < SM::NWARP; ++s)
+      scatter_recorded<CP>(acc, rec + s * 32 * BRK_REC, recorded[s] & (0x11111111u << wid), lane);
+    __syncthreads();  // records and masks are rewritten by the next pass
   }
-  __syncthreads();
   flush_windows<CP, SM::NWARP>(a, bp, acc0, SM::ACC, static_cast<int>(threadIdx.x), BRK_GATHER_THREADS);
 }
 
