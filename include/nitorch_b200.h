@@ -242,6 +242,19 @@ PP_API int pp_resize(const pp_tensor* input, const pp_tensor* out, const double*
  * gave up; 0 in normal operation).  Synchronous. */
 PP_API int pp_resize_status(uint32_t* status);
 
+/* Multigrid prolongation / restriction between the grids of `input`
+ * (N, C, *inshape) and `out` (N, C, *shape) of nitorch's native
+ * fmg_prolongation / fmg_restriction (nitorch/_C/src/multires.h:10-19,
+ * impl/multires_common.cpp:419-500 and 587-660): with scale = inshape /
+ * shape per axis, output voxel o reads the input at x = (o + 1/2) scale -
+ * 1/2; prolongation weights the three nodes around x by the quadratic
+ * B-spline, restriction the four nodes from floor(x) - 1 by the linear
+ * B-spline of width `scale` (divided by `scale`).  No field-of-view test;
+ * opt->bound per axis (opt->order and opt->extrapolate are not read).
+ * 3-D float32 or bfloat16; the same separable kernel as pp_resize. */
+PP_API int pp_fmg_prolongation(const pp_tensor* input, const pp_tensor* out, const pp_options* opt, void* stream);
+PP_API int pp_fmg_restriction(const pp_tensor* input, const pp_tensor* out, const pp_options* opt, void* stream);
+
 /* ---- Jacobians of transformation / displacement fields ----------------
  * nitorch.spatial.grid_jacobian / grid_jacdet (nitorch/spatial/_grid.py:
  * 917-1013) without `sample`: central finite differences of the

@@ -13,6 +13,9 @@ Entry points:
                             coordinates computed in the kernel (no grid)
   nitorch_b200.svf.exp      velocity exponentiation (scaling and squaring)
   nitorch_b200.grid_jacobian / grid_jacdet   Jacobians of transformation fields
+  nitorch_b200.prolong / restrict            the multigrid solvers' resampling;
+  nitorch_b200.multires     native fmg_prolongation / fmg_restriction, ni::resize
+                            (modes, adjoint, normalisation) and their wrappers
   nitorch_b200.spatial      drop-in for the ``nitorch._C.spatial`` module
   nitorch_b200.ops          the same as torch.library operators (torch.ops.nitorch_b200.*)
   nitorch_b200.coeff        drop-in for ``interpol.coeff``
@@ -21,14 +24,16 @@ Entry points:
 """
 from .api import (affine_grid, affine_pull, affine_push, grid_count, grid_grad, grid_pull, grid_push,
                   identity_grid, pull_push, reslice, resize, spline_coeff, spline_coeff_nd)
-from .enums import BoundType, InterpolationType
+from .enums import BoundType, GridAlignType, InterpolationType
 from .jacobian import grid_jacdet, grid_jacobian
+from .multires import fmg_prolongation, fmg_restriction, prolong, restrict
 from .spatial import get_deterministic, set_deterministic
-from . import spatial, coeff, grid, svf, ops
+from . import spatial, coeff, grid, svf, ops, multires
 from .integration import install
 
 __all__ = ["grid_pull", "grid_push", "grid_count", "grid_grad", "pull_push", "affine_grid", "affine_pull",
            "affine_push", "resize", "reslice", "svf", "grid_jacobian", "grid_jacdet", "spline_coeff",
-           "spline_coeff_nd", "identity_grid", "BoundType", "InterpolationType",
+           "spline_coeff_nd", "identity_grid", "BoundType", "InterpolationType", "GridAlignType",
+           "prolong", "restrict", "fmg_prolongation", "fmg_restriction", "multires",
            "set_deterministic", "get_deterministic", "spatial", "coeff", "grid",
            "install"]

@@ -74,6 +74,7 @@ EXPORTS = (
     "pp_batch_plan_bytes", "pp_batch_scratch_bytes", "pp_batch_plan", "pp_batch_run",
     "pp_svf_compose", "pp_svf_compose_backward", "pp_affine_pull", "pp_affine_push",
     "pp_affine_grad_workspace_bytes", "pp_affine_grad_matrix", "pp_resize", "pp_resize_status",
+    "pp_fmg_prolongation", "pp_fmg_restriction",
     "pp_grid_jacobian", "pp_grid_jacobian_backward", "pp_jacobian_det",
 )
 
@@ -118,6 +119,8 @@ def _declare(L):
     D3 = ctypes.c_double * 3
     L.pp_resize.argtypes = [T, T, D3, D3, O, vp]
     L.pp_resize_status.argtypes = [ctypes.POINTER(ctypes.c_uint32)]
+    L.pp_fmg_prolongation.argtypes = [T, T, O, vp]
+    L.pp_fmg_restriction.argtypes = [T, T, O, vp]
     L.pp_batch_plan_bytes.argtypes = [ctypes.c_int32]
     L.pp_batch_plan_bytes.restype = sz
     L.pp_batch_scratch_bytes.argtypes = [ctypes.POINTER(PPBatchEntry), ctypes.c_int32, ctypes.c_int32]

@@ -384,7 +384,7 @@ int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const u
 
 extern "C" {
 
-int pp_abi_version(void) { return 101; }
+int pp_abi_version(void) { return 102; }
 
 const char* pp_last_error(void) { return g_err.c_str(); }
 

@@ -58,6 +58,8 @@ struct ResizeArgs {
   float scale[3], shift[3];
   int bound[3], order;
   int extrapolate;
+  int kind;  // 0: B-spline at scale * o + shift (field-of-view test); 1: multigrid
+             // restriction, 2: multigrid prolongation (both at (o + 1/2) scale - 1/2)
   int tile[3];  // TX, TY, TZ
   int ext[3];   // staged extents EX, EY, EZ (EZ a multiple of 4: the TMA box)
   int ntile[3];
@@ -87,12 +89,34 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned phase) {
 }
 
 // Per-axis stencil of output index o: lowest node, weights, field of view.
+// Kinds 1 and 2 follow nitorch's multigrid operators
+// (nitorch/_C/src/impl/multires_common.cpp:419-500, 587-660): the output
+// voxel centre maps to x = (o + 1/2) scale - 1/2 in input voxels, with no
+// field-of-view test; restriction (kind 1) weights the four nodes from
+// floor(x) - 1 by the linear B-spline of width `scale`, L(|x - i| / scale) /
+// scale; prolongation (kind 2) is the quadratic B-spline at x.
 template <int NT>
 __device__ __forceinline__ void axis_stencil(const ResizeArgs& a, int d, int o, int& lo, float (&w)[NT], bool& inb) {
-  float x = fmaf(a.scale[d], static_cast<float>(o), a.shift[d]);
-  const float tol = (a.extrapolate & 2) ? 0.55f : 0.05f;
-  inb = in_fov<float>(x, a.in_size[d], tol);
+  float x;
+  if (a.kind == 0) {
+    x = fmaf(a.scale[d], static_cast<float>(o), a.shift[d]);
+    const float tol = (a.extrapolate & 2) ? 0.55f : 0.05f;
+    inb = in_fov<float>(x, a.in_size[d], tol);
+  } else {
+    x = (static_cast<float>(o) + 0.5f) * a.scale[d] - 0.5f;
+    inb = true;
+  }
   x = fminf(fmaxf(x, -1073741824.f), 1073741824.f);
+  if (NT == 4 && a.kind == 1) {
+    const float s = a.scale[d];
+    lo = static_cast<int>(floorf(x)) - 1;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+      const float t = fabsf(x - static_cast<float>(lo + k)) / s;
+      w[k] = (t < 1.f ? 1.f - t : 0.f) / s;
+    }
+    return;
+  }
   lo = support_low<int, float>(a.order, x);
   const float f = (x - static_cast<float>(lo)) - 0.5f * static_cast<float>(a.order - 1);
   float g[NT], h[NT];
@@ -522,7 +546,7 @@ cudaError_t launch_resize(const ResizeArgs& a, const CUtensorMap& map, size_t sm
       cudaSuccess)
     return e;
   const int64_t grid = std::min<int64_t>(ntiles, static_cast<int64_t>(std::max(1, sms * per_sm)));
-  ppk::note_kernel(TMA ? "resize_sep_kernel tma" : "resize_sep_kernel", 0, NT - 1, 1);
+  ppk::note_kernel(TMA ? "resize_sep_kernel tma" : "resize_sep_kernel", a.kind, NT - 1, 1);
   resize_sep_kernel<NT, S, TMA><<<static_cast<unsigned>(grid), RZ_THREADS, smem, st>>>(a, map);
   return cudaGetLastError();
 }
@@ -541,12 +565,8 @@ cudaError_t dispatch(int order, bool tma, const ResizeArgs& a, const CUtensorMap
   return cudaErrorInvalidValue;
 }
 
-}  // namespace
-
-extern "C" {
-
-int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale, const double* shift,
-              const pp_options* opt, void* stream) {
+int resize_launch(const pp_tensor* input, const pp_tensor* out, const double* scale, const double* shift,
+                  const int (&bound)[3], int order, int extrapolate, int kind, void* stream) {
   using namespace ppc;
   int rc;
   if ((rc = check_tensor(input, "input")) || (rc = check_tensor(out, "output"))) return rc;
@@ -557,11 +577,6 @@ int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale,
   if (input->dtype != out->dtype) return fail(PP_ERR_DTYPE, "(): output dtype must match input");
   if (input->dtype != PP_FLOAT32 && input->dtype != PP_BFLOAT16)
     return fail(PP_ERR_UNSUPPORTED, "(): pp_resize takes float32 or bfloat16 images");
-  if (!scale || !shift) return fail(PP_ERR_ARG, "(): expected scale and shift");
-  int bound[3], order[3];
-  if ((rc = read_options(opt, 3, bound, order))) return rc;
-  if (order[1] != order[0] || order[2] != order[0] || order[0] > 3)
-    return fail(PP_ERR_UNSUPPORTED, "(): pp_resize takes one B-spline order of at most 3 for all axes");
   for (int d = 0; d < 3; ++d) {
     if (!(scale[d] > 0.0) || !std::isfinite(scale[d]) || !std::isfinite(shift[d]))
       return fail(PP_ERR_UNSUPPORTED, "(): pp_resize takes positive finite scales and finite shifts");
@@ -572,7 +587,7 @@ int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale,
   if (max_offset(input, 0) >= (int64_t(1) << 31) || max_offset(out, 0) >= (int64_t(1) << 31) ||
       input->sizes[0] * input->sizes[1] >= (int64_t(1) << 31))
     return fail(PP_ERR_UNSUPPORTED, "(): pp_resize needs 32-bit element offsets");
-  const int NT = order[0] == 0 ? 1 : order[0] + 1;
+  const int NT = kind == 1 ? 4 : (order == 0 ? 1 : order + 1);
   int tile[3], ext[3];
   const double sc3[3] = {scale[0], scale[1], scale[2]};
   if (!choose_tile(sc3, NT, tile, ext, RZ_SMEM_FLOATS))
@@ -604,8 +619,9 @@ int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale,
     ntiles *= a.ntile[d];
   }
   while ((1 << a.zls) < ext[2] / 4 && a.zls < 5) ++a.zls;
-  a.order = order[0];
-  a.extrapolate = opt->extrapolate;
+  a.order = order;
+  a.extrapolate = extrapolate;
+  a.kind = kind;
   if (ntiles * a.C >= (int64_t(1) << 31)) return fail(PP_ERR_UNSUPPORTED, "(): pp_resize: too many tiles");
 
   // TMA copies need a float32 image with the z axis contiguous, 16-byte
@@ -635,10 +651,52 @@ int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale,
   const size_t smem = smem_floats(tile, ext) * 4;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int64_t nitems = ntiles * a.C;
-  cudaError_t e = input->dtype == PP_FLOAT32 ? dispatch<float>(order[0], tma, a, map, smem, nitems, st)
-                                             : dispatch<__nv_bfloat16>(order[0], false, a, map, smem, nitems, st);
+  const int tap_order = NT - 1;  // the instance: NT taps
+  cudaError_t e = input->dtype == PP_FLOAT32 ? dispatch<float>(tap_order, tma, a, map, smem, nitems, st)
+                                             : dispatch<__nv_bfloat16>(tap_order, false, a, map, smem, nitems, st);
   count_launch();
   return cuda_check(e, "resize launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+int pp_resize(const pp_tensor* input, const pp_tensor* out, const double* scale, const double* shift,
+              const pp_options* opt, void* stream) {
+  using namespace ppc;
+  if (!scale || !shift) return fail(PP_ERR_ARG, "(): expected scale and shift");
+  int bound[3], order[3], rc;
+  if ((rc = read_options(opt, 3, bound, order))) return rc;
+  if (order[1] != order[0] || order[2] != order[0] || order[0] > 3)
+    return fail(PP_ERR_UNSUPPORTED, "(): pp_resize takes one B-spline order of at most 3 for all axes");
+  return resize_launch(input, out, scale, shift, bound, order[0], opt->extrapolate, 0, stream);
+}
+
+// Multigrid prolongation / restriction between the grids of `input` and
+// `out`: scale = input size / output size per axis.
+static int multires(const pp_tensor* input, const pp_tensor* out, const pp_options* opt, int kind, void* stream) {
+  using namespace ppc;
+  int rc;
+  if ((rc = check_tensor(input, "input")) || (rc = check_tensor(out, "output"))) return rc;
+  if (input->ndim != 5 || out->ndim != 5)
+    return fail(PP_ERR_UNSUPPORTED, "(): expected 3-D images (N, C, X, Y, Z)");
+  int bound[3], order[3];
+  if ((rc = read_options(opt, 3, bound, order))) return rc;
+  double scale[3], shift[3] = {0., 0., 0.};
+  for (int d = 0; d < 3; ++d) {
+    if (input->sizes[2 + d] <= 0 || out->sizes[2 + d] <= 0) return fail(PP_ERR_ARG, "(): expected non-empty sizes");
+    scale[d] = static_cast<double>(input->sizes[2 + d]) / static_cast<double>(out->sizes[2 + d]);
+  }
+  return resize_launch(input, out, scale, shift, bound, kind == 1 ? 1 : 2, 1, kind, stream);
+}
+
+int pp_fmg_prolongation(const pp_tensor* input, const pp_tensor* out, const pp_options* opt, void* stream) {
+  return multires(input, out, opt, 2, stream);
+}
+
+int pp_fmg_restriction(const pp_tensor* input, const pp_tensor* out, const pp_options* opt, void* stream) {
+  return multires(input, out, opt, 1, stream);
 }
 
 int pp_resize_status(uint32_t* status) {

@@ -49,6 +49,15 @@ class InterpolationType(_CodeEnum):
     seventh = 7
 
 
+class GridAlignType(_CodeEnum):
+    """Lattice alignment of nitorch's native resize (nitorch/_C/src/
+    grid_align.h:7-12; values as the compiled backend exports them)."""
+    edge = 0      # outer edges of the corner voxels
+    center = 1    # centres of the corner voxels
+    first = 2     # centre of the first voxel (factor kept)
+    last = 3      # centre of the last voxel (factor kept)
+
+
 # Prefilter integer bound codes (nitorch/_C/_ts/bounds.py:7-14), used by the
 # interpol-compatible spline_coeff entry points.
 TS_BOUND = {BoundType.zero: 0, BoundType.replicate: 1, BoundType.dct1: 2,

@@ -12,6 +12,14 @@ of ``nitorch/_C/spatial.cpp:82-89`` (C++: ``nitorch/_C/src/pushpull.h:10-57``):
     grid_grad(input, grid, bound, interpolation, extrapolate) -> Tensor
     grid_grad_backward(grad, input, grid, bound, interpolation, extrapolate) -> list
 
+and the native multigrid resampling the same module binds
+(``nitorch/_C/spatial.cpp:101-110``; defined in ``nitorch_b200.multires``):
+
+    resize(input, output, factor, bound, interpolation, mode, do_adjoint, normalize)
+    resize_backward / prolongation / prolongation_backward / restriction /
+    restriction_backward / fmg_prolongation(input, output, bound) / fmg_restriction
+    and the enum GridAlignType
+
 ``bound`` / ``interpolation`` are lists (one entry per axis, padded with the
 last one); ``extrapolate`` is an int bit field.  As in the reference, the
 backward functions read ``requires_grad`` of ``input`` / ``grid`` to decide
@@ -531,3 +539,18 @@ def grid_pull_push_backward(grad, input, grid, bound, interpolation, extrapolate
     if gg is not None:
         out.append(gg.to(grid.dtype))
     return out
+
+
+# The native multigrid resampling of the same compiled module, resolved on
+# first use (nitorch_b200.multires imports this module's launch helpers).
+from .enums import GridAlignType  # noqa: E402
+
+_MULTIRES = ("fmg_prolongation", "fmg_restriction", "prolongation", "prolongation_backward", "resize",
+             "resize_backward", "restriction", "restriction_backward")
+
+
+def __getattr__(name):
+    if name in _MULTIRES:
+        from . import multires
+        return getattr(multires, name)
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")

@@ -411,3 +411,208 @@ def grid_jacobian(grid, bound="dft", voxel_size=1, type="grid", add_identity=Tru
 def grid_jacdet(grid, bound="dft", voxel_size=1, type="grid", add_identity=True):
     """nitorch/spatial/_grid.py:972-1013: det of grid_jacobian."""
     return np.linalg.det(grid_jacobian(grid, bound, voxel_size, type, add_identity))
+
+
+# ---------------------------------------------------------------------------
+# Multigrid prolongation / restriction and nitorch's native resize
+# ---------------------------------------------------------------------------
+
+def _bound_index(b, i, n):
+    """Node i of an n-voxel axis under bound code b (nitorch/_C/src/
+    bounds_common.h:26-120: replicate clamps; dct1 reflects about the end
+    centres, period 2(n-1); dct2 / dst2 about the end edges, period 2n;
+    dst1 antisymmetric about the centres, period 2(n+1); dft wraps)."""
+    if b == 0:
+        return min(max(i, 0), n - 1)
+    if b == 1:
+        if n == 1:
+            return 0
+        p = 2 * (n - 1)
+        i = abs(i) % p
+        return p - i if i >= n else i
+    if b in (2, 4):
+        p = 2 * n
+        i = (p - ((-i - 1) % p) - 1) if i < 0 else i % p
+        return p - i - 1 if i >= n else i
+    if b == 3:
+        if n == 1:
+            return 0
+        p = 2 * (n + 1)
+        i = 0 if i == -1 else (-i - 2 if i < 0 else i)
+        i %= p
+        return n - 1 if i == n else (p - i - 2 if i > n else i)
+    if b == 5:
+        return i % n
+    return i
+
+
+def _bound_sign(b, i, n):
+    """Sign of node i under bound code b (bounds_common.h:122-160): dst1 is
+    zero on its mirror nodes and alternates between periods, dst2
+    alternates, zero is 0 outside the axis."""
+    if b == 3:
+        if n == 1:
+            return 1
+        p = 2 * (n + 1)
+        i = n - i - 1 if i < 0 else i
+        i %= p
+        if i % (n + 1) == n:
+            return 0
+        return -1 if (i // (n + 1)) % 2 else 1
+    if b == 4:
+        i = n - i - 1 if i < 0 else i
+        return -1 if (i // n) % 2 else 1
+    if b == 7:
+        return 0 if (i < 0 or i >= n) else 1
+    return 1
+
+
+def _quadratic(d):
+    """Quadratic B-spline (interpolation_common.h, order 2)."""
+    d = abs(d)
+    if d < 0.5:
+        return 0.75 - d * d
+    if d < 1.5:
+        return 0.5 * (1.5 - d) ** 2
+    return 0.0
+
+
+def _multires_matrix(n_in, n_out, b, restrict):
+    """(n_out, n_in) matrix of one axis of fmg_prolongation / fmg_restriction
+    (nitorch/_C/src/impl/multires_common.cpp:419-500 and 587-660): output
+    voxel o reads x = (o + 1/2) s - 1/2, s = n_in / n_out.  Prolongation:
+    nodes floor(x + 1/2) - 1 .. + 1, quadratic B-spline weights.
+    Restriction: nodes floor(x) - 1 .. + 2, weight L(|x - i| / s) / s with
+    L the linear B-spline.  Boundary index and sign per node."""
+    s = n_in / n_out
+    M = np.zeros((n_out, n_in))
+    for o in range(n_out):
+        x = (o + 0.5) * s - 0.5
+        if restrict:
+            i1 = int(np.floor(x))
+            nodes = [(i, max(0.0, 1.0 - abs(x - i) / s) / s) for i in range(i1 - 1, i1 + 3)]
+        else:
+            i1 = int(np.floor(x + 0.5))
+            nodes = [(i, _quadratic(x - i)) for i in range(i1 - 1, i1 + 2)]
+        for i, w in nodes:
+            sg = _bound_sign(b, i, n_in)
+            if sg:
+                M[o, _bound_index(b, i, n_in)] += sg * w
+    return M
+
+
+def _apply_axes(x, mats):
+    """Apply one matrix per spatial axis of x (N, C, *spatial)."""
+    y = np.asarray(x, np.float64)
+    for d, M in enumerate(mats):
+        y = np.moveaxis(np.tensordot(M, np.moveaxis(y, 2 + d, 0), axes=(1, 0)), 0, 2 + d)
+    return y
+
+
+def fmg_prolongation(inp, bound=(2,), shape=None):
+    """nitorch's native fmg_prolongation (nitorch/_C/src/multires.cpp:24-48):
+    inp (N, C, *spatial) with 1-3 spatial axes; output shape floor(2 s) per
+    axis unless `shape` is given."""
+    sp = inp.shape[2:]
+    shape = shape or [int(np.floor(2.0 * s)) for s in sp]
+    b = _pad(list(bound), len(sp))
+    return _apply_axes(inp, [_multires_matrix(sp[d], shape[d], b[d], False) for d in range(len(sp))])
+
+
+def fmg_restriction(inp, bound=(2,), shape=None):
+    """nitorch's native fmg_restriction (multires.cpp:50-74): output shape
+    ceil(s / 2) per axis unless `shape` is given."""
+    sp = inp.shape[2:]
+    shape = shape or [int(np.ceil(s / 2.0)) for s in sp]
+    b = _pad(list(bound), len(sp))
+    return _apply_axes(inp, [_multires_matrix(sp[d], shape[d], b[d], True) for d in range(len(sp))])
+
+
+def _padf(v, n):
+    v = list(v) if isinstance(v, (list, tuple)) else [v]
+    return [float(x) for x in (v + v[-1:] * max(0, n - len(v)))[:n]]
+
+
+def resize_affine(factor, n_src, n_tgt, mode):
+    """(shift, scale) of one axis of ni::resize (nitorch/_C/src/impl/
+    resize_common.cpp:1547-1566): target voxel w reads source x = scale w +
+    shift.  Modes: 0 edge, 1 center, 2 first, 3 last.  IEEE division, as
+    there: a one-voxel axis gives inf / nan in the center and last modes."""
+    f, ns, nt = np.float64(factor), np.float64(n_src), np.float64(n_tgt)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        shift, scale = np.float64(0.0), 1.0 / f
+        if mode == 0:
+            shift, scale = 0.5 * (ns / nt - 1), ns / nt
+        elif mode == 1:
+            shift, scale = np.float64(0.0), (ns - 1) / (nt - 1)
+        elif mode == 3:
+            shift = f * (ns - 1) / (nt - 1)
+    return float(shift), float(scale)
+
+
+def resize_native(inp, out_shape=None, factor=(1.0,), bound=(2,), order=(1,), mode=(1,), adjoint=False,
+                  normalize=False):
+    """nitorch's native resize (nitorch/_C/src/resize.cpp:19-60,
+    impl/resize_common.cpp:1488-1660) on inp (N, C, *spatial): the pull of
+    the source at the target lattice's diagonal map, always extrapolating,
+    or (adjoint) the push of the target into the source lattice, then the
+    optional normalisation by the product of the scales.  The reference
+    runs 3-D inputs only (1-D / 2-D ones raise an index error in its
+    allocator); here the 1-D / 2-D normalisation is the product over the
+    real axes."""
+    D = inp.ndim - 2
+    f = _padf(factor, 3)
+    if adjoint:
+        f = [1.0 / v for v in f]
+    if adjoint:
+        tgt_shape = list(inp.shape[2:])
+        src_shape = list(out_shape) if out_shape else [int(np.ceil(s * f[d])) for d, s in enumerate(tgt_shape)]
+    else:
+        src_shape = list(inp.shape[2:])
+        tgt_shape = list(out_shape) if out_shape else [int(np.floor(s * f[d])) for d, s in enumerate(src_shape)]
+    m = _pad(list(mode), 3)
+    m = m[:D] + [m[D - 1]] * (3 - D)
+    full_src = src_shape + [1] * (3 - D)
+    full_tgt = tgt_shape + [1] * (3 - D)
+    aff = [resize_affine(f[d], float(full_src[d]), float(full_tgt[d]), m[d]) for d in range(3)]
+    axes = [np.arange(tgt_shape[d], dtype=np.float64) * aff[d][1] + aff[d][0] for d in range(D)]
+    grid = np.stack(np.meshgrid(*axes, indexing="ij"), -1)[None]
+    grid = np.broadcast_to(grid, (inp.shape[0],) + grid.shape[1:]).copy()
+    if adjoint:
+        out = grid_push(inp, grid, src_shape, bound, order, 1)
+    else:
+        out = grid_pull(inp, grid, bound, order, 1)
+    if normalize:
+        out = out * float(np.prod([aff[d][1] for d in range(D)]))
+    return out
+
+
+def _edge_grid(src_shape, tgt_shape, N):
+    """(N, *tgt, D) coordinates of the edge-aligned map of the multigrid
+    solvers (nitorch/spatial/_solvers.py:170-177): arange(tgt) * src / tgt +
+    0.5 (src / tgt - 1) per axis, in the input's dtype (float64 here)."""
+    axes = [np.arange(t, dtype=np.float64) * (s / t) + 0.5 * (s / t - 1) for s, t in zip(src_shape, tgt_shape)]
+    g = np.stack(np.meshgrid(*axes, indexing="ij"), -1)[None]
+    return np.broadcast_to(g, (N,) + g.shape[1:]).copy()
+
+
+def solver_prolong(x, shape=None, bound=2, order=2):
+    """nitorch/spatial/_solvers.py:147-181: x (N, *spatial, K) pulled at the
+    edge-aligned map of a `shape` lattice (default 2 * spatial), order 2,
+    extrapolating."""
+    sp = x.shape[1:-1]
+    shape = list(shape) if shape else [2 * s for s in sp]
+    grid = _edge_grid(sp, shape, x.shape[0])
+    y = grid_pull(np.moveaxis(x, -1, 1), grid, [bound], [order], 1)
+    return np.moveaxis(y, 1, -1)
+
+
+def solver_restrict(x, shape=None, bound=2, order=1):
+    """nitorch/spatial/_solvers.py:184-224: x (N, *spatial, K) pushed from
+    the edge-aligned map onto a `shape` lattice (default ceil(spatial / 2)),
+    order 1, extrapolating, times prod(shape) / prod(spatial)."""
+    sp = x.shape[1:-1]
+    shape = list(shape) if shape else [int(np.ceil(s / 2)) for s in sp]
+    grid = _edge_grid(shape, sp, x.shape[0])
+    y = grid_push(np.moveaxis(x, -1, 1), grid, shape, [bound], [order], 1)
+    return np.moveaxis(y, 1, -1) * (np.prod(shape) / np.prod(sp))

@@ -15,6 +15,12 @@ Writes
                         spline_coeff_nd volumes.
   config1_golden.npz  : checksums of the reference's pull / push on the
                         seeded config-1 workload (1x1x64^3, order 1, dct2).
+  multires_golden.npz : outputs of the reference's multigrid resampling
+                        (native fmg_prolongation / fmg_restriction, native
+                        resize with modes / adjoint / normalisation, the
+                        prolongation / restriction wrappers, the multigrid
+                        solvers' prolong / restrict) on seeded float64
+                        inputs (`python tests/golden/make_golden.py multires`).
   spatial_golden.npz  : outputs of the reference's nitorch.spatial callers of
                         the path (grid_jacobian / grid_jacdet, resize,
                         reslice, exp of a velocity field and its autograd
@@ -202,7 +208,78 @@ def spatial(S):
     return {k: np.asarray(v) for k, v in out.items()}
 
 
+def multires(ref, S):
+    """nitorch's multigrid resampling, float64: the native fmg_prolongation /
+    fmg_restriction (3-D: the reference raises on 1-D / 2-D inputs), the
+    native resize with its alignment modes, adjoint and normalisation, the
+    native prolongation / restriction wrappers and their backward, the
+    displacement-grid wrappers of nitorch/_C/resize.py and the multigrid
+    solvers' prolong / restrict (nitorch/spatial/_solvers.py)."""
+    import nitorch._C.resize as CR
+    import nitorch.spatial._solvers as SV
+    out = {}
+    g = torch.Generator().manual_seed(91)
+    BT = {0: ref.BoundType.replicate, 1: ref.BoundType.dct1, 2: ref.BoundType.dct2, 3: ref.BoundType.dst1,
+          4: ref.BoundType.dst2, 5: ref.BoundType.dft, 7: ref.BoundType.zero}
+    IT = [ref.InterpolationType.nearest, ref.InterpolationType.linear, ref.InterpolationType.quadratic,
+          ref.InterpolationType.cubic]
+    GA = [ref.GridAlignType.edge, ref.GridAlignType.center, ref.GridAlignType.first, ref.GridAlignType.last]
+    shapes = [(1, 2, 5, 6, 7), (2, 1, 9, 4, 3), (1, 1, 1, 8, 3), (1, 2, 6, 6, 6)]
+    for k, sh in enumerate(shapes):
+        x = torch.randn(sh, generator=g, dtype=torch.float64)
+        out[f"fmg_x{k}"] = x.numpy()
+        for b, bt in BT.items():
+            out[f"fmg_pro{k}_b{b}"] = ref.fmg_prolongation(x, torch.Tensor(), [bt]).numpy()
+            out[f"fmg_res{k}_b{b}"] = ref.fmg_restriction(x, torch.Tensor(), [bt]).numpy()
+    x = torch.randn((1, 2, 5, 6, 7), generator=g, dtype=torch.float64)
+    out["rz_x"] = x.numpy()
+    for mode in range(4):
+        for adj in (0, 1):
+            for norm in (0, 1):
+                for kf, fac in enumerate((2.0, 0.7)):
+                    for order in (1, 3):
+                        key = f"rz_m{mode}_a{adj}_n{norm}_f{kf}_o{order}"
+                        out[key] = ref.resize(x, torch.Tensor(), [fac], [BT[2]], [IT[order]], [GA[mode]],
+                                              bool(adj), bool(norm)).numpy()
+    # the native wrappers with an output lattice given
+    xf = torch.randn((1, 2, 10, 12, 14), generator=g, dtype=torch.float64)
+    out["wrap_fine"] = xf.numpy()
+    out["wrap_prolongation"] = ref.prolongation(x, torch.zeros((1, 2, 10, 12, 14), dtype=torch.float64),
+                                                [], []).numpy()
+    out["wrap_prolongation_backward"] = ref.prolongation_backward(
+        xf, torch.zeros((1, 2, 5, 6, 7), dtype=torch.float64), [], []).numpy()
+    out["wrap_restriction"] = ref.restriction(xf, torch.zeros((1, 2, 5, 6, 7), dtype=torch.float64),
+                                              [], []).numpy()
+    out["wrap_restriction_backward"] = ref.restriction_backward(
+        x, torch.zeros((1, 2, 10, 12, 14), dtype=torch.float64), [], []).numpy()
+    # nitorch/_C/resize.py wrappers (factor / shape, displacement grids)
+    out["c_prolongation"] = CR.c_prolongation(x, factor=2., bound="dct1").numpy()
+    out["c_restriction"] = CR.c_restriction(xf, factor=2., bound="dft").numpy()
+    out["c_restriction_shape"] = CR.c_restriction(xf, shape=(4, 7, 5)).numpy()
+    v = torch.randn((1, 5, 6, 7, 3), generator=g, dtype=torch.float64)
+    vf = torch.randn((1, 10, 12, 14, 3), generator=g, dtype=torch.float64)
+    out["grid_coarse"], out["grid_fine"] = v.numpy(), vf.numpy()
+    out["c_prolongation_grid"] = CR.c_prolongation_grid(v.clone()).numpy()
+    out["c_restriction_grid"] = CR.c_restriction_grid(vf.clone()).numpy()
+    # multigrid solvers' prolong / restrict (channel-last)
+    out["sv_prolong"] = SV.prolong(v.clone(), dim=3).numpy()
+    out["sv_prolong_o3"] = SV.prolong(v.clone(), order=3, bound="dft", dim=3).numpy()
+    out["sv_restrict"] = SV.restrict(vf.clone(), dim=3).numpy()
+    out["sv_restrict_shape"] = SV.restrict(vf.clone(), shape=(4, 5, 8), dim=3).numpy()
+    out["sv_prolong_nobatch"] = SV.prolong(v[0].clone()).numpy()  # (*spatial, K): dim = 3 by default
+    return {k: np.asarray(v) for k, v in out.items()}
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "multires":
+        S = R.load_spatial()
+        ref = R.load_compiled()
+        if S is None or ref is None:
+            raise SystemExit("reference tree / compiled backend not found")
+        torch.set_num_threads(1)
+        np.savez_compressed(os.path.join(HERE, "multires_golden.npz"), **multires(ref, S))
+        print("multires_golden.npz", os.path.getsize(os.path.join(HERE, "multires_golden.npz")))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "spatial":
         S = R.load_spatial()
         if S is None:
