@@ -158,6 +158,14 @@ PP_API int pp_grid_count_backward(const pp_tensor* grad, const pp_tensor* grid,
 PP_API int pp_grid_grad(const pp_tensor* input, const pp_tensor* grid,
                  const pp_tensor* out, const pp_options* opt, void* stream);
 
+/* Fused forward of pull and grid_grad: out (N, C, *grid) = pull(input, grid)
+ * and out_grad (N, C, *grid, D) = grid_grad(input, grid) from one pass over
+ * each point's taps (the two values ni::grid_pull and ni::grid_grad,
+ * nitorch/_C/src/pushpull.h:10-13 and 40-43, compute separately).  Same
+ * arguments and checks as pp_grid_grad, plus `out`. */
+PP_API int pp_grid_pull_grad(const pp_tensor* input, const pp_tensor* grid, const pp_tensor* out,
+                             const pp_tensor* out_grad, const pp_options* opt, void* stream);
+
 /* ni::grid_grad_backward (pushpull.h:45-48): grad (N,C,*grid,D). */
 PP_API int pp_grid_grad_backward(const pp_tensor* grad, const pp_tensor* input,
                           const pp_tensor* grid, const pp_tensor* grad_input,

@@ -9,6 +9,7 @@ Entry points:
   nitorch_b200.grid_pull / grid_push / grid_count / grid_grad /
   spline_coeff / spline_coeff_nd / identity_grid   (nitorch.spatial API)
   nitorch_b200.pull_push    fused push(pull(.)) (normal operator), one pass
+  nitorch_b200.grid_pull_grad  grid_pull and grid_grad of one input and grid, one pass
   nitorch_b200.resize / reslice / affine_pull / affine_push   affine sampling,
                             coordinates computed in the kernel (no grid)
   nitorch_b200.svf.exp      velocity exponentiation (scaling and squaring)
@@ -22,7 +23,7 @@ Entry points:
   nitorch_b200.batch        many uneven volumes in one persistent launch
   nitorch_b200.install()    route an installed nitorch through this backend
 """
-from .api import (affine_grid, affine_pull, affine_push, grid_count, grid_grad, grid_pull, grid_push,
+from .api import (affine_grid, affine_pull, affine_push, grid_count, grid_grad, grid_pull, grid_pull_grad, grid_push,
                   identity_grid, pull_push, reslice, resize, spline_coeff, spline_coeff_nd)
 from .enums import BoundType, GridAlignType, InterpolationType
 from .jacobian import grid_jacdet, grid_jacobian
@@ -31,7 +32,7 @@ from .spatial import get_deterministic, set_deterministic
 from . import spatial, coeff, grid, svf, ops, multires
 from .integration import install
 
-__all__ = ["grid_pull", "grid_push", "grid_count", "grid_grad", "pull_push", "affine_grid", "affine_pull",
+__all__ = ["grid_pull", "grid_push", "grid_count", "grid_grad", "grid_pull_grad", "pull_push", "affine_grid", "affine_pull",
            "affine_push", "resize", "reslice", "svf", "grid_jacobian", "grid_jacdet", "spline_coeff",
            "spline_coeff_nd", "identity_grid", "BoundType", "InterpolationType", "GridAlignType",
            "prolong", "restrict", "fmg_prolongation", "fmg_restriction", "multires",

@@ -67,7 +67,7 @@ EXPORTS = (
     "pp_abi_version", "pp_last_error", "pp_kernel_launches", "pp_last_kernel", "pp_push_workspace_bytes",
     "pp_grid_pull", "pp_grid_pull_backward", "pp_grid_push",
     "pp_grid_push_backward", "pp_grid_count", "pp_grid_count_backward",
-    "pp_grid_grad", "pp_grid_grad_backward", "pp_spline_coeff",
+    "pp_grid_grad", "pp_grid_grad_backward", "pp_grid_pull_grad", "pp_spline_coeff",
     "pp_spline_coeff_nd", "pp_sample_order_workspace_bytes", "pp_sample_order",
     "pp_sample_order_noalloc", "pp_brick_count", "pp_brick_order_workspace_bytes", "pp_brick_order",
     "pp_grid_pull_push", "pp_grid_pull_push_backward",
@@ -101,6 +101,7 @@ def _declare(L):
     L.pp_grid_count.argtypes = [T, T, O, vp, vp, sz]
     L.pp_grid_count_backward.argtypes = [T, T, T, O, vp]
     L.pp_grid_grad.argtypes = [T, T, T, O, vp]
+    L.pp_grid_pull_grad.argtypes = [T, T, T, T, O, vp]
     L.pp_grid_grad_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]
     L.pp_grid_pull_push.argtypes = [T, T, T, O, vp, vp, sz]
     L.pp_grid_pull_push_backward.argtypes = [T, T, T, T, T, O, vp, vp, sz]

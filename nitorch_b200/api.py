@@ -10,7 +10,7 @@ Same signatures, defaults, broadcasting and output shapes as
 import torch
 
 from .affine import affine_pull, affine_push, resize_pull, resize_supported
-from .grid import GridCount, GridGrad, GridPull, GridPullPush, GridPush, SplineCoeff, SplineCoeffND
+from .grid import GridCount, GridGrad, GridPull, GridPullGrad, GridPullPush, GridPush, SplineCoeff, SplineCoeffND
 
 
 class _Layout:
@@ -138,6 +138,18 @@ def grid_grad(input, grid, interpolation="linear", bound="zero", extrapolate=Fal
     if prefilter:
         input = spline_coeff_nd(input, interpolation, bound, layout.dim)
     return layout.restore(GridGrad.apply(input, grid, interpolation, bound, extrapolate))
+
+
+def grid_pull_grad(input, grid, interpolation="linear", bound="zero", extrapolate=False,
+                   prefilter=False):
+    """grid_pull and grid_grad of the same input and grid from one pass over
+    each point's taps: ((..., [channel], *outshape), (..., [channel],
+    *outshape, dim)), each equal to the separate call's result."""
+    grid, input, layout = _fold(grid, input)
+    if prefilter:
+        input = spline_coeff_nd(input, interpolation, bound, layout.dim)
+    pulled, grad = GridPullGrad.apply(input, grid, interpolation, bound, extrapolate)
+    return layout.restore(pulled), layout.restore(grad)
 
 
 def spline_coeff(input, interpolation="linear", bound="dct2", dim=-1, inplace=False):

@@ -384,7 +384,7 @@ int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const u
 
 extern "C" {
 
-int pp_abi_version(void) { return 102; }
+int pp_abi_version(void) { return 103; }
 
 const char* pp_last_error(void) { return g_err.c_str(); }
 
@@ -442,6 +442,36 @@ int pp_grid_grad(const pp_tensor* input, const pp_tensor* grid, const pp_tensor*
   set_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
   k.a.out_sK = out->strides[2 + k.D];
   return run(k, ppk::K_SGRAD, need_wide(k, {input, out}), static_cast<cudaStream_t>(stream));
+}
+
+int pp_grid_pull_grad(const pp_tensor* input, const pp_tensor* grid, const pp_tensor* out,
+                      const pp_tensor* out_grad, const pp_options* opt, void* stream) {
+  Call k;
+  int rc = prepare(k, grid, opt);
+  if (rc) return rc;
+  if ((rc = check_image(input, "input", k.D, grid->dtype))) return rc;
+  if (input->sizes[0] != grid->sizes[0])
+    return fail(PP_ERR_ARG, "(): expected input and grid to have the same batch size");
+  if ((rc = check_tensor(out, "output")) || (rc = check_tensor(out_grad, "output gradient"))) return rc;
+  int64_t osz[6] = {grid->sizes[0], input->sizes[1], 1, 1, 1, 1};
+  for (int a = 0; a < k.D; ++a) osz[2 + a] = grid->sizes[1 + a];
+  if ((rc = check_same_sizes(out, osz, k.D + 2, "output"))) return rc;
+  osz[2 + k.D] = k.D;
+  if ((rc = check_same_sizes(out_grad, osz, k.D + 3, "output gradient"))) return rc;
+  if (out->dtype != input->dtype || out_grad->dtype != input->dtype)
+    return fail(PP_ERR_DTYPE, "(): output dtype must match input");
+  k.dtype = input->dtype;
+  k.a.src = input->data;
+  k.a.C = input->sizes[1];
+  for (int a = 0; a < 3; ++a) k.a.src_size[a] = a < k.D ? input->sizes[2 + a] : 1;
+  set_image(input, k.D, k.a.src_sN, k.a.src_sC, k.a.src_s);
+  k.a.out = out_grad->data;
+  set_image(out_grad, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
+  k.a.out_sK = out_grad->strides[2 + k.D];
+  k.a.aux = out->data;  // the pulled values, at the target strides
+  set_image(out, k.D, k.a.trgt_sN, k.a.trgt_sC, k.a.trgt_s);
+  k.a.flags |= ppk::F_A;
+  return run(k, ppk::K_SGRAD, need_wide(k, {input, out, out_grad}), static_cast<cudaStream_t>(stream));
 }
 
 // Scatter helper: push `trgt` (N,C,*grid[,K]) into `out` (N,C,*shape) with

@@ -58,6 +58,7 @@ struct PPArgs {
   const void* grid;  // (N, *trgt_size, D)
   void* out;         // pull/sgrad: (N, C, *trgt_size[, D]); push/count: (N, C, *src_size)
   void* gg;          // grid gradient (N, *trgt_size, D)
+  void* aux;         // K_SGRAD with F_A: the interpolated values (N, C, *trgt_size) at the trgt_* strides
   int64_t N, C;
   int64_t src_size[3], trgt_size[3];
   int64_t src_sN, src_sC, src_s[3];
@@ -263,6 +264,7 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
           if (MODE == K_SGRAD) {
 #pragma unroll
             for (int d = 0; d < D; ++d) op[c * a.out_sC + d * a.out_sK] = from_acc<S>(T(0));
+            if (do_a) (static_cast<S*>(a.aux) + tvox)[c * a.trgt_sC] = from_acc<S>(T(0));
           } else {
             op[c * a.out_sC] = from_acc<S>(T(0));
           }
@@ -458,7 +460,10 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
   }
 
   if constexpr (MODE == K_SGRAD) {
+    // spatial gradient; with F_A also the interpolated value (the fused
+    // pull + grid_grad forward), the gw sum of the same taps
     S* op = static_cast<S*>(a.out) + ovox;
+    S* vp = do_a ? static_cast<S*>(a.aux) + tvox : nullptr;
     for (int64_t c0 = 0; c0 < C; c0 += CB) {
       const int nc = C - c0 < CB ? static_cast<int>(C - c0) : CB;
       const S* sp = src_n + c0 * a.src_sC;
@@ -470,6 +475,7 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
           oc[0] = from_acc<S>(gx[cb]);
           if (D > 1) oc[a.out_sK] = from_acc<S>(gy[cb]);
           if (D > 2) oc[2 * a.out_sK] = from_acc<S>(gz[cb]);
+          if (vp) vp[(c0 + cb) * a.trgt_sC] = from_acc<S>(gw[cb]);
         }
       }
     }

@@ -204,6 +204,32 @@ class GridGrad(torch.autograd.Function):
         return grad_input, grad_grid, None, None, None
 
 
+class GridPullGrad(torch.autograd.Function):
+    """pull and grid_grad of one input at one grid, computed in one pass;
+    the backward adds the two backward passes."""
+
+    @staticmethod
+    def forward(ctx, input, grid, interpolation, bound, extrapolate):
+        opt = _opt(bound, interpolation, extrapolate)
+        pulled, grad = _spatial.grid_pull_grad(input, grid, *opt)
+        ctx.opt = opt
+        ctx.save_for_backward(input, grid)
+        return pulled, grad
+
+    @staticmethod
+    def backward(ctx, g_pull, g_grad):
+        var = ctx.saved_tensors
+        grad_input = grad_grid = None
+        if ctx.needs_input_grad[0] or ctx.needs_input_grad[1]:
+            for g, fn in ((g_pull, _spatial.grid_pull_backward), (g_grad, _spatial.grid_grad_backward)):
+                if g is None:
+                    continue
+                gi, gg = _unpack(ctx, fn(g.contiguous(), *var, *ctx.opt))
+                grad_input = gi if grad_input is None else grad_input + gi
+                grad_grid = gg if grad_grid is None else grad_grid + gg
+        return grad_input, grad_grid, None, None, None
+
+
 class SplineCoeff(torch.autograd.Function):
 
     @staticmethod

@@ -465,6 +465,27 @@ def grid_grad(input, grid, bound, interpolation, extrapolate):
     return out
 
 
+def grid_pull_grad(input, grid, bound, interpolation, extrapolate):
+    """grid_pull and grid_grad of the same input and grid from one pass over
+    the taps (pp_grid_pull_grad): [pulled (N, C, *grid), grad (N, C, *grid,
+    D)]."""
+    _check_pair(input, grid)
+    _check_opts(bound, interpolation)
+    _require_cuda(input)
+    L = _lib.load()
+    g = _grid32(grid)
+    opt = _opts(bound, interpolation, extrapolate, g, input.shape[2:])
+    dim = grid.dim() - 2
+    out = torch.empty((grid.shape[0], input.shape[1], *grid.shape[1:-1]), dtype=input.dtype,
+                      device=input.device)
+    og = torch.empty((*out.shape, dim), dtype=input.dtype, device=input.device)
+    with _On(input):
+        _lib.check(L.pp_grid_pull_grad(ctypes.byref(_lib.desc(input)), ctypes.byref(_lib.desc(g)),
+                                       ctypes.byref(_lib.desc(out)), ctypes.byref(_lib.desc(og)),
+                                       ctypes.byref(opt), _lib.stream_of(input)))
+    return [out, og]
+
+
 def grid_grad_backward(grad, input, grid, bound, interpolation, extrapolate):
     _check_pair(input, grid)
     _check_opts(bound, interpolation)
