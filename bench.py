@@ -285,13 +285,14 @@ SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one op call
 # on the default workload (1x3x192^3, cubic, dct2, brick-major order), from
 # one ncu capture of its kernels, keyed by the kernel string pp_last_kernel
-# reports after the op.  Push counts the brick scatter alone (its
-# accumulator-to-output copy, store_interleaved_vox, is not included).  A
-# kernel not listed here reports traffic null.
+# reports after the op.  Push and pull backward include the copy of their
+# channel-interleaved accumulator into the output (store_interleaved_vox).
+# A kernel not listed here reports traffic null.
 MEASURED_TRAFFIC = {
-    "pp_brick_gather_kernel mode=0 order=3 cb=3": 279_590_400,
-    "pp_brick_scatter_kernel mode=2 order=3 cb=3": 403_078_400,
-    "pp_kernel mode=4 order=3 cb=3": 485_229_056,
+    "pp_brick_gather_kernel mode=0 order=3 cb=3": 280_530_688,
+    "pp_brick_scatter_kernel mode=2 order=3 cb=3": 413_369_344 + 152_478_976,
+    "pp_kernel mode=4 order=3 cb=3": 491_643_392,
+    "pp_brick_pullbwd_kernel mode=5 order=3 cb=3": 583_121_408 + 150_514_176,
     # resize 1x3x256^3 -> 320^3, cubic, dct2
     "resize_sep_kernel tma mode=0 order=3 cb=1": 566_675_200,
 }

@@ -100,6 +100,14 @@ typedef struct pp_options {
                                     accumulate each brick of the scatter
                                     target in on-chip memory.  NULL = no
                                     brick pass.                           */
+  const float* brick_records;    /* optional device array with brick_start:
+                                    the records pp_brick_order wrote for
+                                    the same float32 grid (4 floats per
+                                    sample, in perm order).  The brick
+                                    kernels then read each sample's
+                                    coordinates and index in one coalesced
+                                    16-byte load.  NULL = read perm and the
+                                    grid.                                 */
 } pp_options;
 
 /* Version of this ABI (major * 100 + minor). */
@@ -301,23 +309,27 @@ PP_API int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32
                            void* workspace, size_t workspace_bytes, void* stream);
 
 /* Brick-major processing order (no counterpart in the reference; a
- * scheduling aid for the cubic 3-D scatters).  The source volume (spatial
+ * scheduling aid for the cubic 3-D brick kernels).  The source volume (spatial
  * size `src_size`, 3 entries) is cut into bricks of PP_BRICK_X x PP_BRICK_Y
  * x PP_BRICK_Z voxels, nb = prod(ceil(src_size / brick)) per batch item.
  * Writes to `perm` (int32, N*prod(grid spatial) entries) the sample
  * indices sorted by (batch item, brick, voxel in brick) of the source voxel
  * floor(coordinate) they fall in (clamped into the volume), and to
  * `brick_start` (int32, N*nb + 1 entries) where each brick's samples start
- * in `perm` (the last entry is the number of samples).  Pass both in
- * pp_options.  3-D grids only; needs pp_brick_order_workspace_bytes()
- * bytes of device workspace.  pp_brick_count() gives N*nb. */
+ * in `perm` (the last entry is the number of samples).  Optional
+ * `records` (float32 grids only; 4 * N*prod(grid spatial) floats, 16-byte
+ * aligned, or NULL) receives, in perm order, each sample's coordinates and
+ * its index (x, y, z, index as int32 bits).  Pass all three in pp_options.
+ * 3-D grids only; needs pp_brick_order_workspace_bytes() bytes of device
+ * workspace.  pp_brick_count() gives N*nb. */
 #define PP_BRICK_X 4
 #define PP_BRICK_Y 4
 #define PP_BRICK_Z 6
 PP_API int64_t pp_brick_count(const pp_tensor* grid, const int64_t* src_size);
 PP_API size_t pp_brick_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_size);
 PP_API int pp_brick_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
-                          int32_t* brick_start, void* workspace, size_t workspace_bytes, void* stream);
+                          int32_t* brick_start, float* records, void* workspace, size_t workspace_bytes,
+                          void* stream);
 
 /* pp_sample_order without any device allocation or caller workspace (no
  * counterpart in the reference).  For callers that cannot allocate device

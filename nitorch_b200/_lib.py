@@ -53,6 +53,7 @@ class PPOptions(ctypes.Structure):
         ("flags", ctypes.c_int32),
         ("sample_order", ctypes.c_void_p),
         ("brick_start", ctypes.c_void_p),
+        ("brick_records", ctypes.c_void_p),
     ]
 
 
@@ -142,7 +143,7 @@ def _declare(L):
     L.pp_brick_count.restype = ctypes.c_int64
     L.pp_brick_order_workspace_bytes.argtypes = [T, I64P]
     L.pp_brick_order_workspace_bytes.restype = sz
-    L.pp_brick_order.argtypes = [T, I64P, vp, vp, vp, sz, vp]
+    L.pp_brick_order.argtypes = [T, I64P, vp, vp, vp, vp, sz, vp]
     for name in EXPORTS:
         if name not in ("pp_last_error", "pp_last_kernel", "pp_push_workspace_bytes", "pp_kernel_launches",
                         "pp_sample_order_workspace_bytes", "pp_batch_plan_bytes", "pp_batch_scratch_bytes",
@@ -205,10 +206,11 @@ def ref(d):
     return None if d is None else ctypes.byref(d)
 
 
-def options(bound, order, extrapolate, flags=0, sample_order=None, brick_start=None):
+def options(bound, order, extrapolate, flags=0, sample_order=None, brick_start=None, brick_records=None):
     o = PPOptions()
     o.sample_order = sample_order
     o.brick_start = brick_start
+    o.brick_records = brick_records
     b = [int(x) for x in bound][:3]
     i = [int(x) for x in order][:3]
     o.nbound = len(b)

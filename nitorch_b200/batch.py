@@ -179,6 +179,7 @@ class PullPushBatch:
             pws = max(pws, L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(z)), 0),
                       L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(dx)), 0))
         self.starts_flat, self.starts = _arena([(n,) for n in nb], torch.int32, dev)
+        self.recs_flat, self.recs = _arena([(n, 4) for n in npts], torch.float32, dev)
         self.sort_ws = torch.empty(ws, dtype=torch.uint8, device=dev)
         self.push_ws = torch.empty(pws, dtype=torch.uint8, device=dev)
         self.plans = {}
@@ -197,9 +198,11 @@ class PullPushBatch:
                 src = (ctypes.c_int64 * 3)(*self.shapes[i])
                 B.check(L.pp_brick_order(ref(self.grid[i]), src, ctypes.c_void_p(self.perm[i].data_ptr()),
                                          ctypes.c_void_p(self.starts[i].data_ptr()),
+                                         ctypes.c_void_p(self.recs[i].data_ptr()),
                                          ctypes.c_void_p(self.sort_ws.data_ptr()), self.sort_ws.numel(), stream))
                 opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, 0,
-                                      self.perm[i].data_ptr(), self.starts[i].data_ptr()))
+                                      self.perm[i].data_ptr(), self.starts[i].data_ptr(),
+                                      self.recs[i].data_ptr()))
             else:
                 opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, 0))
         for i in range(self.n):

@@ -10,8 +10,8 @@
 // pp_sample_order computes that order -- a permutation of the grid's sample
 // indices sorted by the linear index (batch item, then the source voxel
 // floor(coords) clamped into the volume, last axis fastest) -- with a
-// counting sort.  (A brick-major key, 4x4x16 bricks, measured ~18 % slower
-// for the scatter kernels on B200 and gains nothing for the gathers.)
+// counting sort.  (3-D grids of the cubic brick kernels use the brick-major
+// order of pp_brick_order below instead.)
 // Steps:
 //   1. key / rank: key = source voxel, rank = atomicAdd(&count[key], 1);
 //   2. exclusive scan of count (block reduce, scan of block sums, apply);
@@ -251,6 +251,30 @@ __global__ void brick_keys(KeyArgs a, int nbx, int nby, int nbz, int32_t* count,
   ranks[s] = atomicAdd(count + key, 1);
 }
 
+// The brick pass's scatter: perm[pos] = s and, when `rec` is given, the
+// sample's coordinates and index as one 16-byte record at the same position
+// (read here once, coalesced by s, so that the brick kernels read each
+// sample's data in brick order without the perm -> grid indirection).
+__global__ void brick_scatter(KeyArgs a, const int32_t* keys, const int32_t* ranks, const int32_t* offset,
+                              int32_t* perm, float4* rec) {
+  const unsigned s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= static_cast<unsigned>(a.nvox)) return;
+  const int32_t pos = offset[keys[s]] + ranks[s];
+  perm[pos] = static_cast<int32_t>(s);
+  if (rec) {
+    int v = static_cast<int>(s), sub[3];
+    for (int d = 2; d >= 0; --d) {
+      const int n = static_cast<int>(a.size[d]);
+      const int q = v / n;
+      sub[d] = v - q * n;
+      v = q;
+    }
+    const float* g = static_cast<const float*>(a.grid) + static_cast<int64_t>(v) * a.gsN;
+    for (int d = 0; d < 3; ++d) g += static_cast<int64_t>(sub[d]) * a.gs[d];
+    rec[pos] = make_float4(g[0], g[a.gsD], g[2 * a.gsD], __int_as_float(static_cast<int>(s)));
+  }
+}
+
 // brick_start[b] = offset of brick b's first key; brick_start[nb] = nvox
 __global__ void brick_starts(const int32_t* offset, int64_t nbricks, int32_t nvox, int32_t* start) {
   const int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -289,12 +313,14 @@ size_t pp_brick_order_workspace_bytes(const pp_tensor* grid, const int64_t* src_
 }
 
 int pp_brick_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm, int32_t* brick_start,
-                   void* workspace, size_t workspace_bytes, void* stream) {
+                   float* records, void* workspace, size_t workspace_bytes, void* stream) {
   int64_t nvox;
   BrickGeom g;
   int rc = brick_sizes_of(grid, src_size, nvox, g);
   if (rc) return rc;
   if (!perm || !brick_start) return ppc::fail(PP_ERR_ARG, "(): expected an output permutation and brick offsets");
+  if (records && (grid->dtype != PP_FLOAT32 || reinterpret_cast<uintptr_t>(records) % 16 != 0))
+    return ppc::fail(PP_ERR_ARG, "(): brick records need a float32 grid and a 16-byte aligned buffer");
   const Layout L = layout(nvox, g.nkeys);
   if (!workspace || workspace_bytes < L.total)
     return ppc::fail(PP_ERR_WORKSPACE, "(): brick ordering needs %zu bytes of workspace", L.total);
@@ -329,7 +355,7 @@ int pp_brick_order(const pp_tensor* grid, const int64_t* src_size, int32_t* perm
     scan_reduce<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, g.nkeys, partial);
     scan_partials<<<1, SCAN_THREADS, 0, st>>>(partial, ntile);
     scan_apply<<<static_cast<unsigned>(ntile), SCAN_THREADS, 0, st>>>(count, g.nkeys, partial);
-    order_scatter<<<nb, 256, 0, st>>>(keys, ranks, count, nvox, perm);
+    brick_scatter<<<nb, 256, 0, st>>>(a, keys, ranks, count, perm, reinterpret_cast<float4*>(records));
     ppc::count_launch(5);
   }
   brick_starts<<<static_cast<unsigned>((nbricks + 1 + 255) / 256), 256, 0, st>>>(count, nbricks,

@@ -167,18 +167,18 @@ struct BrickPoint {
   int lo[3];
   bool fits;
 };
-__device__ __forceinline__ BrickPoint brick_point(const PPArgs& a, int p, const BrickPos& bp) {
+// The point of sample index v at coordinates x (batch item, grid voxel, fit).
+__device__ __forceinline__ BrickPoint brick_point_of(const PPArgs& a, int v, float x0, float x1, float x2,
+                                                     const BrickPos& bp) {
   using W = BrickWin;
   BrickPoint q;
-  int v = __ldg(a.perm + p);
+  q.x[0] = x0;
+  q.x[1] = x1;
+  q.x[2] = x2;
   q.sub[2] = v % static_cast<int>(a.trgt_size[2]); v /= static_cast<int>(a.trgt_size[2]);
   q.sub[1] = v % static_cast<int>(a.trgt_size[1]); v /= static_cast<int>(a.trgt_size[1]);
   q.sub[0] = v % static_cast<int>(a.trgt_size[0]);
   q.n = v / static_cast<int>(a.trgt_size[0]);
-  const float* gp = static_cast<const float*>(a.grid) + static_cast<int64_t>(q.n) * a.grid_sN +
-                    q.sub[0] * a.grid_s[0] + q.sub[1] * a.grid_s[1] + q.sub[2] * a.grid_s[2];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) q.x[d] = __ldg(gp + d * a.grid_sD);
   const float tol = (a.extrapolate & 2) ? 0.55f : 0.05f;
   bool inb = true;
 #pragma unroll
@@ -194,6 +194,23 @@ __device__ __forceinline__ BrickPoint brick_point(const PPArgs& a, int p, const 
     q.fits = q.fits && q.lo[d] >= o && q.lo[d] <= o + e - 4;
   }
   return q;
+}
+
+// Sample p (in brick order): from its record, or through perm and the grid.
+__device__ __forceinline__ BrickPoint brick_point(const PPArgs& a, int p, const BrickPos& bp) {
+  if (a.brec) {  // coordinates and index in one record, in brick order
+    const float4 r = __ldg(a.brec + p);
+    return brick_point_of(a, __float_as_int(r.w), r.x, r.y, r.z, bp);
+  }
+  const int v = __ldg(a.perm + p);
+  int r = v;
+  const int s2 = r % static_cast<int>(a.trgt_size[2]); r /= static_cast<int>(a.trgt_size[2]);
+  const int s1 = r % static_cast<int>(a.trgt_size[1]); r /= static_cast<int>(a.trgt_size[1]);
+  const int s0 = r % static_cast<int>(a.trgt_size[0]);
+  const int n = r / static_cast<int>(a.trgt_size[0]);
+  const float* gp = static_cast<const float*>(a.grid) + static_cast<int64_t>(n) * a.grid_sN + s0 * a.grid_s[0] +
+                    s1 * a.grid_s[1] + s2 * a.grid_s[2];
+  return brick_point_of(a, v, __ldg(gp), __ldg(gp + a.grid_sD), __ldg(gp + 2 * a.grid_sD), bp);
 }
 
 // ===========================================================================
@@ -286,21 +303,23 @@ __device__ __forceinline__ void flush_windows(const PPArgs& a, const BrickPos& b
   }
 }
 
-// Stage the source window of brick bp at GatherWin pitches (value times
-// boundary sign; 0 outside): every thread issues all of its loads before
-// its first shared store.
-template <int CB, int CP, class S>
-__device__ __forceinline__ void stage_window(const PPArgs& a, const BrickPos& bp, float* img) {
+// The source window of brick bp at GatherWin pitches (value times boundary
+// sign; 0 outside), in two halves: window_load issues every load of this
+// thread into registers, window_store writes them to shared memory.
+template <int NTHR> struct WinRegs {
+  static constexpr int NIT = (BrickWin::NE + NTHR - 1) / NTHR;
+};
+template <int CB, int CP, class S, int NTHR>
+__device__ __forceinline__ void window_load(const PPArgs& a, const BrickPos& bp,
+                                            float (&v)[WinRegs<NTHR>::NIT][CP], int (&dst)[WinRegs<NTHR>::NIT]) {
   using W = BrickWin;
   using G = GatherWin;
-  constexpr int NIT = (W::NE + BRK_GATHER_THREADS - 1) / BRK_GATHER_THREADS;
+  constexpr int NIT = WinRegs<NTHR>::NIT;
   const S* src_n = static_cast<const S*>(a.src) + static_cast<int64_t>(bp.n) * a.src_sN;
   const int64_t ss[3] = {a.src_s[0], a.src_s[1], a.src_s[2]};
-  float v[NIT][CP];
-  int dst[NIT];
 #pragma unroll
   for (int it = 0; it < NIT; ++it) {
-    const int e = static_cast<int>(threadIdx.x) + it * BRK_GATHER_THREADS;
+    const int e = static_cast<int>(threadIdx.x) + it * NTHR;
 #pragma unroll
     for (int c = 0; c < CP; ++c) v[it][c] = 0.f;
     dst[it] = -1;
@@ -318,9 +337,23 @@ __device__ __forceinline__ void stage_window(const PPArgs& a, const BrickPos& bp
       }
     }
   }
+}
+template <int CP, int NTHR>
+__device__ __forceinline__ void window_store(float* img, const float (&v)[WinRegs<NTHR>::NIT][CP],
+                                             const int (&dst)[WinRegs<NTHR>::NIT]) {
 #pragma unroll
-  for (int it = 0; it < NIT; ++it)
+  for (int it = 0; it < WinRegs<NTHR>::NIT; ++it)
     if (dst[it] >= 0) vstore<CP>(img + dst[it], v[it]);
+}
+
+// Stage the source window of brick bp: every thread issues all of its loads
+// before its first shared store.
+template <int CB, int CP, class S, int NTHR>
+__device__ __forceinline__ void stage_window(const PPArgs& a, const BrickPos& bp, float* img) {
+  float v[WinRegs<NTHR>::NIT][CP];
+  int dst[WinRegs<NTHR>::NIT];
+  window_load<CB, CP, S, NTHR>(a, bp, v, dst);
+  window_store<CP, NTHR>(img, v, dst);
 }
 
 // One point's 64-tap gather from the staged window `ib` (its lowest node):
@@ -472,7 +505,7 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
   constexpr bool want_val = MODE == K_PULL;
   const bool want_gg = GG && (a.flags & F_GRAD) != 0;
 
-  stage_window<CB, CP, S>(a, bp, img);
+  stage_window<CB, CP, S, BRK_GATHER_THREADS>(a, bp, img);
   __syncthreads();
 
   for (int p = p0 + static_cast<int>(threadIdx.x); p < p1; p += BRK_GATHER_THREADS) {
@@ -545,7 +578,7 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, 4) pp_brick_pullbwd_kernel
   if (p0 >= p1) return;  // whole CTA
   const BrickPos bp = brick_pos(a, b);
 
-  stage_window<CB, CP, S>(a, bp, img);
+  stage_window<CB, CP, S, BRK_GATHER_THREADS>(a, bp, img);
   {
     float4* a4 = reinterpret_cast<float4*>(acc0);
     for (int e = threadIdx.x; e < SM::NWARP * SM::ACC / 4; e += BRK_GATHER_THREADS)

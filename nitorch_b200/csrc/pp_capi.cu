@@ -181,6 +181,7 @@ int prepare(Call& k, const pp_tensor* grid, const pp_options* opt) {
   k.a.extrapolate = opt->extrapolate;
   k.a.perm = opt->sample_order;
   k.a.brick_start = (k.D == 3 && opt->sample_order) ? opt->brick_start : nullptr;
+  k.a.brec = k.a.brick_start ? reinterpret_cast<const float4*>(opt->brick_records) : nullptr;
   k.a.grid = grid->data;
   set_grid(grid, k.D, k.a.grid_sN, k.a.grid_s, k.a.grid_sD);
   k.a.N = grid->sizes[0];
@@ -384,7 +385,7 @@ int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const u
 
 extern "C" {
 
-int pp_abi_version(void) { return 103; }
+int pp_abi_version(void) { return 104; }
 
 const char* pp_last_error(void) { return g_err.c_str(); }
 

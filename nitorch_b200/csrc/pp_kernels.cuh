@@ -85,6 +85,9 @@ struct PPArgs {
   // nbrick[] bricks per axis of the scatter target / gathered source.
   const int32_t* brick_start;
   int64_t nbrick[3];
+  // With brick_start: the samples' coordinates and indices in perm order
+  // (pp_brick_order's records), or NULL to read perm and the grid.
+  const float4* brec;
 };
 
 // Power-of-two scale of the deterministic accumulators: bound * scale < 2^61.

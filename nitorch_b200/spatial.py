@@ -125,8 +125,10 @@ def sample_order(grid, src_size):
 
 def brick_order(grid, src_size):
     """Brick-major processing order of a 3-D grid's sampling points for a
-    source of spatial size `src_size`: (perm, brick_start), int32 device
-    tensors (see pp_brick_order)."""
+    source of spatial size `src_size`: (perm, brick_start, records), int32
+    device tensors and, for a float32 grid, the (samples, 4) float32 records
+    of coordinates and indices in perm order (else None); see
+    pp_brick_order."""
     L = _lib.load()
     src = (ctypes.c_int64 * 3)(*[int(v) for v in src_size])
     d = _lib.desc(grid)
@@ -137,12 +139,14 @@ def brick_order(grid, src_size):
     nvox = grid.numel() // grid.shape[-1]
     perm = torch.empty(nvox, dtype=torch.int32, device=grid.device)
     starts = torch.empty(nb + 1, dtype=torch.int32, device=grid.device)
+    recs = torch.empty((nvox, 4), dtype=torch.float32, device=grid.device) if grid.dtype == torch.float32 else None
     ws = torch.empty(nbytes, dtype=torch.uint8, device=grid.device)
     with _On(grid):
         _lib.check(L.pp_brick_order(ctypes.byref(d), src, ctypes.c_void_p(perm.data_ptr()),
-                                    ctypes.c_void_p(starts.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
-                                    nbytes, _lib.stream_of(grid)))
-    return perm, starts
+                                    ctypes.c_void_p(starts.data_ptr()),
+                                    None if recs is None else ctypes.c_void_p(recs.data_ptr()),
+                                    ctypes.c_void_p(ws.data_ptr()), nbytes, _lib.stream_of(grid)))
+    return perm, starts, recs
 
 
 def _brick_keys_fit(grid, src_size):
@@ -157,21 +161,21 @@ _BRICK = (4, 4, 6)  # PP_BRICK_X, PP_BRICK_Y, PP_BRICK_Z
 
 
 def _order_for(grid, src_size):
-    """(perm, brick_start) for the call, or (None, None) for the natural
+    """(perm, brick_start, records) for the call, or Nones for the natural
     order.  3-D grids get the brick-major order (it also drives the brick
-    scatters); 1-D / 2-D grids the source-sorted one."""
+    kernels); 1-D / 2-D grids the source-sorted one."""
     mode = _sample_order_mode
     if mode == "natural":
-        return None, None
+        return None, None, None
     nvox = grid.numel() // grid.shape[-1]
     if mode == "auto" and nvox < _SORT_MIN_SAMPLES:
-        return None, None
+        return None, None, None
     if nvox >= (1 << 31):
-        return None, None
+        return None, None, None
     bricks = grid.dim() == 5 and _brick_keys_fit(grid, src_size)
     entry = _orders.get(grid, src_size)
     if entry is None:
-        entry = brick_order(grid, src_size) if bricks else (sample_order(grid, src_size), None)
+        entry = brick_order(grid, src_size) if bricks else (sample_order(grid, src_size), None, None)
         _orders.put(grid, src_size, entry)
     return entry
 
@@ -266,12 +270,14 @@ def _grid32(grid):
 
 def _opts(bound, interpolation, extrapolate, grid=None, src_size=None):
     _check_opts(bound, interpolation)
-    perm, starts = _order_for(grid, src_size) if grid is not None and grid.is_cuda else (None, None)
+    perm, starts, recs = (_order_for(grid, src_size) if grid is not None and grid.is_cuda
+                          else (None, None, None))
     o = _lib.options([int(b) for b in bound], [int(i) for i in interpolation],
                      int(extrapolate), _lib.PP_DETERMINISTIC if _deterministic else 0,
                      None if perm is None else perm.data_ptr(),
-                     None if starts is None else starts.data_ptr())
-    o._keep = (perm, starts)  # keep the order alive for the call
+                     None if starts is None else starts.data_ptr(),
+                     None if recs is None else recs.data_ptr())
+    o._keep = (perm, starts, recs)  # keep the order alive for the call
     return o
 
 

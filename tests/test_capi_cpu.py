@@ -36,7 +36,7 @@ def test_library_exports_every_symbol():
 
 def test_abi_version_and_error_state():
     L = _lib.load()
-    assert L.pp_abi_version() == 103
+    assert L.pp_abi_version() == 104
     assert isinstance(L.pp_last_error(), bytes)
 
 
@@ -149,5 +149,5 @@ def test_brick_order_geometry():
     g2 = _t((1, 5, 6, 2))
     assert L.pp_brick_count(ctypes.byref(g2), src) == -1
     assert b"3-D" in L.pp_last_error()
-    rc = L.pp_brick_order(ctypes.byref(grid), src, None, None, None, 0, None)
+    rc = L.pp_brick_order(ctypes.byref(grid), src, None, None, None, None, 0, None)
     assert rc == _lib.PP_ERR_ARG
