@@ -534,6 +534,8 @@ def run_batched(args, rank, world, device):
                "plain_per_call": {"value": round(total_points * args.batch_steps / (ms_plain * 1e-3) / 1e9, 4),
                                   "unit": "Gvox/s", "ms_per_step": round(ms_plain / args.batch_steps, 3)},
                "speedup": round(ms_plain / ms_graph, 3),
+               "roofline": batched_roofline(shapes, chans, 4 if dtype == torch.float32 else 2,
+                                            ms_graph / args.batch_steps, world),
                "autotune": {"form": form, "ctas": ctas, "sorted_order": srt, "candidates_ms": tried}}
         if rank == 0 and dtype == torch.float32:
             res["max_rel_err_vs_plain"] = batched_vs_plain(b)
@@ -546,6 +548,19 @@ def run_batched(args, rank, world, device):
         gc.collect()
         torch.cuda.empty_cache()
     return out
+
+
+def batched_roofline(shapes, chans, s, ms_per_step, world):
+    """Algorithmic HBM bytes of the batched step (every volume's pull, push
+    and both backward passes, each tensor read or written once: algo_bytes
+    per point with the volume's channel count and storage size s) against
+    the measured copy bandwidth of all ranks."""
+    hbm, src = peaks()
+    labels = ("pull_fwd", "push_fwd", "push_bwd", "pull_bwd")
+    step_bytes = sum(int(np.prod(sh)) * sum(algo_bytes(k, s, c) for k in labels) for sh, c in zip(shapes, chans))
+    achieved = step_bytes / (ms_per_step * 1e-3) / 1e9
+    return {"bound": "hbm", "algorithmic_bytes_per_step": int(step_bytes), "achieved": round(achieved, 1),
+            "peak": hbm * world, "unit": "GB/s", "frac": round(achieved / (hbm * world), 4), "peak_source": src}
 
 
 def batched_vs_plain(b):

@@ -83,3 +83,15 @@ def test_roofline_traffic_only_for_the_captured_workload():
     assert r["traffic"] is None and r["traffic_source"] is None
     r = bench.roofline(_ops(2.4), ["pull_bwd"], 192 ** 3, 3, 6.4, 1.0e9)
     assert r["traffic"] == 1.0e9 and r["traffic_source"] == "--traffic"
+
+
+def test_batched_roofline():
+    """Algorithmic bytes of the batched step: per volume, points x the chain's
+    per-point bytes at the volume's channel count and storage size."""
+    import bench
+    r = bench.batched_roofline([(10, 20, 30), (5, 5, 5)], [3, 1], 4, 2.0, 2)
+    per = sum(bench.algo_bytes(k, 4, 3) for k in ("pull_fwd", "push_fwd", "push_bwd", "pull_bwd")) * 6000
+    per += sum(bench.algo_bytes(k, 4, 1) for k in ("pull_fwd", "push_fwd", "push_bwd", "pull_bwd")) * 125
+    assert r["algorithmic_bytes_per_step"] == per
+    assert r["achieved"] == pytest.approx(per / 2e-3 / 1e9, rel=1e-3)
+    assert r["frac"] == pytest.approx(r["achieved"] / r["peak"], abs=1e-4)
