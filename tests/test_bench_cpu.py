@@ -89,9 +89,9 @@ def test_batched_roofline():
     """Algorithmic bytes of the batched step: per volume, points x the chain's
     per-point bytes at the volume's channel count and storage size."""
     import bench
-    r = bench.batched_roofline([(10, 20, 30), (5, 5, 5)], [3, 1], 4, 2.0, 2)
+    r = bench.batched_roofline([(10, 20, 30), (5, 5, 5)], [3, 1], 4, 0.002, 2)
     per = sum(bench.algo_bytes(k, 4, 3) for k in ("pull_fwd", "push_fwd", "push_bwd", "pull_bwd")) * 6000
     per += sum(bench.algo_bytes(k, 4, 1) for k in ("pull_fwd", "push_fwd", "push_bwd", "pull_bwd")) * 125
     assert r["algorithmic_bytes_per_step"] == per
-    assert r["achieved"] == pytest.approx(per / 2e-3 / 1e9, rel=1e-3)
+    assert r["achieved"] == pytest.approx(per / 2e-6 / 1e9, rel=1e-3)
     assert r["frac"] == pytest.approx(r["achieved"] / r["peak"], abs=1e-4)
