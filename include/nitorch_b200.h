@@ -333,14 +333,16 @@ PP_API int pp_brick_order(const pp_tensor* grid, const int64_t* src_size, int32_
 
 /* pp_sample_order without any device allocation or caller workspace (no
  * counterpart in the reference).  For callers that cannot allocate device
- * memory when they need an order -- inside a CUDA graph capture, or from a
- * host runtime that owns all device memory up front.  Uses a fixed 16 MiB
+ * memory when they need an order -- a host runtime that owns all device
+ * memory up front, or one that works under a fixed budget.  Uses a fixed 16 MiB
  * scratch array compiled into the library (held on every device that loads
  * it): 4 bytes per source voxel (times the batch) plus 8 bytes per sampling
  * point must fit, else PP_ERR_WORKSPACE.  The first call on a device looks
  * up the scratch address for that device; make that first call before any
- * stream capture.  All calls share the scratch: calls that overlap on the
- * GPU race and must be serialised by the caller. */
+ * stream capture.  Only the device's primary context is supported, and no
+ * cudaDeviceReset may follow the first call on that device.  All calls
+ * share the scratch: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 PP_API int pp_sample_order_noalloc(const pp_tensor* grid, const int64_t* src_size, int32_t* perm,
                                    void* stream);
 

@@ -421,12 +421,11 @@ int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* per
 // Sample ordering without any device allocation.
 //
 // Some callers cannot allocate device memory at the moment they need an
-// order: code running while a stream is being captured into a CUDA graph
-// (cudaMalloc is not allowed there), and hosts that drive this library
-// through its C ABI from a runtime that owns all device memory up front or
-// works under a fixed memory budget (plugins of another framework, real-time
-// pipelines).  For them, pp_sample_order_noalloc uses a scratch area that is
-// part of the library image instead of a caller-provided workspace.
+// order: hosts that drive this library through its C ABI from a runtime that
+// owns all device memory up front or works under a fixed memory budget
+// (plugins of another framework, real-time pipelines).  For them,
+// pp_sample_order_noalloc uses a scratch area that is part of the library
+// image instead of a caller-provided workspace.
 //
 // The scratch is a file-scope device array of NOALLOC_SCRATCH_BYTES (16 MiB);
 // every GPU that loads the library holds it until the process exits.  It
@@ -435,7 +434,10 @@ int pp_sample_order(const pp_tensor* grid, const int64_t* src_size, int32_t* per
 // sampling points into a ~1.3 M-voxel source.  Larger requests are rejected
 // with PP_ERR_WORKSPACE.  All calls share the one array: calls whose work
 // overlaps on the GPU (different streams, or several host threads) race and
-// must be serialised by the caller.
+// must be serialised by the caller.  The scratch address is looked up once
+// per device number, in the context current at the first call: callers must
+// use the device's primary context (the runtime API's), and no
+// cudaDeviceReset may follow the first call on that device.
 // ---------------------------------------------------------------------------
 namespace {
 

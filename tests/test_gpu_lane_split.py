@@ -49,3 +49,29 @@ def test_lane_split_pull_backward_vs_oracle(order, C, bound, ex):
                     assert relerr(np64(out[k]), ref_grid) < 1e-5, (mode, "grid")
         finally:
             spatial.set_sample_order(prev)
+
+
+@pytest.mark.parametrize("C", [2, 3, 4])
+@pytest.mark.parametrize("mode", ["natural", "sorted"])
+def test_lane_split_pull_backward_bf16_vs_oracle(C, mode):
+    """bfloat16 cubic images of 2-4 channels (the vector-reduction lane-split
+    kernel in natural order, the brick kernels in sorted order) against the
+    oracle on the stored (rounded) inputs: the bfloat16 image gradient within
+    2^-8 + 1e-5, the float32 grid gradient within 1e-5."""
+    vol, grid = make_case(3, seed=950 + C, in_size=11, out_size=9, C=C, N=2)
+    grad = np.random.default_rng(C).standard_normal((2, C) + grid.shape[1:-1])
+    V = cu(vol, torch.bfloat16, True)
+    T = cu(grad, torch.bfloat16)
+    G = cu(grid, torch.float32, True, grid=True)
+    ref_in, ref_grid = O.grid_pull_backward(np64(T), np64(V), grid.astype(np.float32).astype(np.float64),
+                                            [2], [3], 1)
+    b, o = enums(2, 3)
+    prev = spatial._sample_order_mode
+    spatial.set_sample_order(mode)
+    try:
+        gi, gg = spatial.grid_pull_backward(T, V, G, b, o, 1)
+    finally:
+        spatial.set_sample_order(prev)
+    assert gi.dtype == torch.bfloat16
+    assert relerr(np64(gi), ref_in) < 2.0 ** -8 + 1e-5
+    assert relerr(np64(gg), ref_grid) < 1e-5

@@ -1,8 +1,8 @@
 """pp_sample_order_noalloc: the sample ordering for callers that cannot
-allocate device memory when they need it (for example while a stream is
-being captured into a CUDA graph, or from a host runtime that owns all
-device memory up front).  It works out of a fixed scratch array compiled
-into the library instead of a caller workspace.
+allocate device memory when they need it (for example a host runtime that
+owns all device memory up front, or one under a fixed budget).  It works out
+of a fixed scratch array compiled into the library instead of a caller
+workspace.
 
 Called through the C ABI, twice in a row (the scratch keeps the previous
 call's contents, so the second call checks that the state it needs is
