@@ -168,9 +168,9 @@ __device__ void rz_item(const ResizeArgs& a, int item, RzItem& it) {
   __syncwarp();
 }
 
-// Persistent CTAs walk the (tile, channel) items with two staging buffers:
-// the TMA copy of the next item is in flight while the current one is
-// filtered.
+// Persistent CTAs walk the (tile, channel) items, a tile's channels in a row,
+// with two staging buffers: the TMA copy of the next item is in flight while
+// the current one is filtered.
 template <int NT, class S, bool TMA>
 __global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_constant__ ResizeArgs a,
                                                                  const __grid_constant__ CUtensorMap tmap) {
@@ -195,7 +195,11 @@ __global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_
   float* smem = rz_smem + ((128u - (smem_addr(rz_smem) & 127u)) & 127u) / 4u;
   float* T1 = smem + 2 * SP;  // [TX][EY][EZ]
   float* T2 = T1 + TX * EY * EZ;  // [TX][TY][EZ]
-  const int nitems = a.ntile[0] * a.ntile[1] * a.ntile[2] * a.N * a.C;
+  // CTA j walks the tiles j, j + G, ... and each tile's channels in turn:
+  // its k-th item is channel k mod C of tile j + (k / C) G (items are
+  // numbered tile * C + channel); a tile's tables serve all its channels
+  const int ntiles = a.ntile[0] * a.ntile[1] * a.ntile[2] * a.N;
+  auto item_of = [&](int k) { return (static_cast<int>(blockIdx.x) + (k / a.C) * static_cast<int>(gridDim.x)) * a.C + k % a.C; };
   const int lz = threadIdx.x & 31, lr = threadIdx.x >> 5;
   const bool oob_zero = !(a.extrapolate & 1);
 
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_
     ++uses[buf];
   };
 
-  int item = blockIdx.x;
+  int item = item_of(0);
   if (threadIdx.x < 32) {
     if (threadIdx.x == 0) {
       if (TMA) {
@@ -223,18 +227,18 @@ __global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_
       }
       uses[0] = uses[1] = 0;
     }
-    if (item < nitems) {
+    if (item / a.C < ntiles) {
       rz_item<NT>(a, item, cur);
       if (TMA && threadIdx.x == 0 && cur.fits) issue(0, cur);
     }
   }
   __syncthreads();
 
-  for (int k = 0; item < nitems; item += gridDim.x, ++k) {
+  for (int k = 0; item / a.C < ntiles; ++k, item = item_of(k)) {
     const int buf = k & 1;
     float* Sst = smem + buf * SP;
-    // per-axis tables of this item's tile
-    for (int e = threadIdx.x; e < a.tile[0] + a.tile[1] + a.tile[2]; e += RZ_THREADS) {
+    // per-axis tables of this item's tile (its first channel)
+    for (int e = threadIdx.x; cur.c == 0 && e < a.tile[0] + a.tile[1] + a.tile[2]; e += RZ_THREADS) {
       const int d = e < a.tile[0] ? 0 : (e < a.tile[0] + a.tile[1] ? 1 : 2);
       const int i = e - (d == 0 ? 0 : (d == 1 ? a.tile[0] : a.tile[0] + a.tile[1]));
       float w[NT];
@@ -250,7 +254,7 @@ __global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_
       w_t[d][i] = w4;
       inb_t[d][i] = inb;
     }
-    if (cur.fits && !cur.interior) {
+    if (cur.c == 0 && cur.fits && !cur.interior) {
       // per axis, where the boundary condition maps each staged position
       for (int e = threadIdx.x; e < EX + EY + EZ; e += RZ_THREADS) {
         const int d = e < EX ? 0 : (e < EX + EY ? 1 : 2);
@@ -262,12 +266,20 @@ __global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_
     }
     // the next item: its copy goes into the other buffer (its last reader,
     // item k - 1, has finished)
-    if (threadIdx.x < 32) {
-      const int ni = item + gridDim.x;
-      if (ni < nitems) {
+    const int ni = item_of(k + 1);
+    const bool has_next = ni / a.C < ntiles;
+    if (threadIdx.x < 32 && has_next) {
+      if (ni % a.C != 0) {
+        // the next channel of the same tile: the same staged region
+        if (threadIdx.x == 0) {
+          nxt = cur;
+          nxt.c = cur.c + 1;
+        }
+        __syncwarp();
+      } else {
         rz_item<NT>(a, ni, nxt);
-        if (TMA && threadIdx.x == 0 && nxt.fits) issue(buf ^ 1, nxt);
       }
+      if (TMA && threadIdx.x == 0 && nxt.fits) issue(buf ^ 1, nxt);
     }
     const S* sc = static_cast<const S*>(a.src) + static_cast<int64_t>(cur.n) * a.src_sN + cur.c * a.src_sC;
     const int bx = cur.base[0], by = cur.base[1], bz = cur.base[2];
@@ -320,7 +332,7 @@ __global__ void __launch_bounds__(RZ_THREADS, 3) resize_sep_kernel(const __grid_
           if (threadIdx.x == 0) {
             atomicOr(&g_resize_status, 1u);
             mbar_wait(smem_addr(&mbar[buf]), ph);  // the copy may still land: wait once more
-            if (TMA && item + gridDim.x < nitems && nxt.fits)
+            if (TMA && has_next && nxt.fits)
               mbar_wait(smem_addr(&mbar[buf ^ 1]), (uses[buf ^ 1] - 1) & 1u);
           }
           return;
@@ -650,10 +662,10 @@ int resize_launch(const pp_tensor* input, const pp_tensor* out, const double* sc
   a.use_tma = tma;
   const size_t smem = smem_floats(tile, ext) * 4;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int64_t nitems = ntiles * a.C;
   const int tap_order = NT - 1;  // the instance: NT taps
-  cudaError_t e = input->dtype == PP_FLOAT32 ? dispatch<float>(tap_order, tma, a, map, smem, nitems, st)
-                                             : dispatch<__nv_bfloat16>(tap_order, false, a, map, smem, nitems, st);
+  // persistent CTAs: at most one per tile (each walks its tiles' channels)
+  cudaError_t e = input->dtype == PP_FLOAT32 ? dispatch<float>(tap_order, tma, a, map, smem, ntiles, st)
+                                             : dispatch<__nv_bfloat16>(tap_order, false, a, map, smem, ntiles, st);
   count_launch();
   return cuda_check(e, "resize launch");
 }
