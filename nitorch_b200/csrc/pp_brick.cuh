@@ -112,6 +112,26 @@ template <int CP> __device__ __forceinline__ void vaxpy(float* p, float w, const
   vstore<CP>(p, v);
 }
 
+// Accumulator windows of the scatters, by voxel: CP = 1, 2, 4 channel slots
+// interleaved per voxel; CP = 3 three channel planes BrickWin::NV floats
+// apart (no padding slot: a quarter less shared-memory traffic per tap).
+template <int CP> __device__ __forceinline__ void win_axpy(float* acc, int vox, float w, const float (&t)[CP]) {
+  if constexpr (CP == 3) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[c * BrickWin::NV + vox] = fmaf(w, t[c], acc[c * BrickWin::NV + vox]);
+  } else {
+    vaxpy<CP>(acc + vox * CP, w, t);
+  }
+}
+template <int CP> __device__ __forceinline__ void win_get(const float* acc, int vox, float (&v)[CP]) {
+  if constexpr (CP == 3) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = acc[c * BrickWin::NV + vox];
+  } else {
+    vload<CP>(acc + vox * CP, v);
+  }
+}
+
 // Brick b of the scatter target / gathered source: batch item, window origin
 // (absolute voxel of window voxel 0) and whether the window lies inside the
 // volume on every axis.
@@ -250,9 +270,9 @@ __device__ __forceinline__ void scatter_recorded(float* acc, const float* rec, u
 #pragma unroll
       for (int c = 0; c < CP; ++c) t[c] = tt[c];
     }
-    const int off0 = (__float_as_int(rr[16]) + loff) * CP;
-    vaxpy<CP>(acc + off0, wxy * zp.x, t);
-    vaxpy<CP>(acc + off0 + 2 * CP, wxy * zp.y, t);
+    const int vox0 = __float_as_int(rr[16]) + loff;
+    win_axpy<CP>(acc, vox0, wxy * zp.x, t);
+    win_axpy<CP>(acc, vox0 + 2, wxy * zp.y, t);
     __syncwarp();
   }
 }
@@ -270,13 +290,13 @@ __device__ __forceinline__ void flush_windows(const PPArgs& a, const BrickPos& b
   for (int e = tid; e < W::NE; e += nthreads) {
     int wx, wy, wz;
     win_coords(e, wx, wy, wz);
-    const int o = (wx * W::PX + wy * W::PY + wz) * CP;
+    const int vox = wx * W::PX + wy * W::PY + wz;
     float v[CP];
-    vload<CP>(acc + o, v);
+    win_get<CP>(acc, vox, v);
 #pragma unroll
     for (int k = 1; k < NACC; ++k) {
       float u[CP];
-      vload<CP>(acc + k * stride + o, u);
+      win_get<CP>(acc + k * stride, vox, u);
 #pragma unroll
       for (int c = 0; c < CP; ++c) v[c] += u[c];
     }
@@ -291,7 +311,13 @@ __device__ __forceinline__ void flush_windows(const PPArgs& a, const BrickPos& b
 #pragma unroll
       for (int c = 0; c < CP; ++c) v[c] = -v[c];
     }
-    if constexpr (CP >= 2) {
+    if constexpr (CP == 3) {
+      if (vec) {  // the interleaved accumulator has four slots for three channels
+        const float v4[4] = {v[0], v[1], v[2], 0.f};
+        red_vec<4>(out_n + off, v4);
+        continue;
+      }
+    } else if constexpr (CP >= 2) {
       if (vec) {
         red_vec<CP>(out_n + off, v);
         continue;
@@ -553,7 +579,8 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
 //                  flushed once at the end)
 // ===========================================================================
 template <int CB, int CP> struct PullBwdSmem {
-  static constexpr int ACC = BrickWin::NV * CP;  // floats per accumulator window
+  static constexpr int CPS = CB == 3 ? 3 : CP;     // accumulator layout (3: channel planes)
+  static constexpr int ACC = BrickWin::NV * CPS;   // floats per accumulator window
   static constexpr int IMG = GatherWin::NV * CP;
   static constexpr int NWARP = BRK_GATHER_THREADS / 32;
   static_assert(NWARP == 4, "the scatter shares points out by k mod 4 (mask 0x11111111 << warp)");
@@ -619,10 +646,10 @@ __global__ void __launch_bounds__(BRK_GATHER_THREADS, 4) pp_brick_pullbwd_kernel
     // warp w adds the recorded points k = w (mod NWARP) of this pass into
     // its own window: an even share whatever the number of points
     for (int s = 0; s < SM::NWARP; ++s)
-      scatter_recorded<CP>(acc, rec + s * 32 * BRK_REC, recorded[s] & (0x11111111u << wid), lane);
+      scatter_recorded<SM::CPS>(acc, rec + s * 32 * BRK_REC, recorded[s] & (0x11111111u << wid), lane);
     __syncthreads();  // records and masks are rewritten by the next pass
   }
-  flush_windows<CP, SM::NWARP>(a, bp, acc0, SM::ACC, static_cast<int>(threadIdx.x), BRK_GATHER_THREADS);
+  flush_windows<SM::CPS, SM::NWARP>(a, bp, acc0, SM::ACC, static_cast<int>(threadIdx.x), BRK_GATHER_THREADS);
 }
 
 }  // namespace ppk

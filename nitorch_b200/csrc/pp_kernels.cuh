@@ -1287,7 +1287,7 @@ inline cudaError_t brick_smem_optin(K kernel, size_t bytes, std::atomic<unsigned
 
 template <int MODE, int CB, class S>
 inline cudaError_t launch_brick_scatter(const PPArgs& a, cudaStream_t st) {
-  constexpr int CP = CB == 1 ? 1 : (CB == 2 ? 2 : 4);
+  constexpr int CP = CB == 1 ? 1 : (CB == 2 ? 2 : (CB == 3 ? 3 : 4));  // 3: channel planes
   constexpr size_t bytes = BrickScatterSmem<CP>::bytes;
   const int64_t nb = a.N * a.nbrick[0] * a.nbrick[1] * a.nbrick[2];
   const int64_t grid = (nb + BRK_SCATTER_WARPS - 1) / BRK_SCATTER_WARPS;
