@@ -701,6 +701,9 @@ def run_all(args, rank, world, device):
     import gc
     if args.only_resize:
         return {"resize": run_resize(args, rank, world, device)} if rank == 0 else None
+    if args.only_svf:
+        r = run_svf(args, rank, world, device)
+        return {"svf": r} if rank == 0 else None
     line = run_b200(args, rank, world, device)
     gc.collect()
     torch.cuda.empty_cache()
@@ -917,6 +920,7 @@ def main():
     ap.add_argument("--no-svf", action="store_true")
     ap.add_argument("--no-fused", action="store_true", help="skip the fused pull_push leg")
     ap.add_argument("--only-resize", action="store_true", help="run the resize leg alone")
+    ap.add_argument("--only-svf", action="store_true", help="run the config-5 leg alone")
     ap.add_argument("--no-resize", action="store_true")
     ap.add_argument("--svf-steps", type=int, default=5)
     ap.add_argument("--traffic", type=float, default=None,

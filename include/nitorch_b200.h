@@ -211,9 +211,16 @@ PP_API int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_
 
 /* Gradient of <grad, u + pull(u, id + u)> with respect to u (the exact
  * adjoint of pp_svf_compose), written to grad_disp (disp's sizes, zero-filled
- * by the call, must not alias the inputs).  No deterministic mode. */
+ * by the call, must not alias the inputs).  No deterministic mode.  With a
+ * 16-byte aligned workspace of pp_svf_workspace_bytes(disp) bytes (3-D
+ * float32 fields, linear or cubic), the push of the gradient goes to a
+ * four-slot channel-interleaved accumulator with one vector reduction per
+ * tap and is copied to grad_disp afterwards; with NULL / too small, one
+ * reduction per component and tap into grad_disp. */
+PP_API size_t pp_svf_workspace_bytes(const pp_tensor* disp);
 PP_API int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp,
-                                   const pp_tensor* grad_disp, const pp_options* opt, void* stream);
+                                   const pp_tensor* grad_disp, const pp_options* opt, void* stream,
+                                   void* workspace, size_t workspace_bytes);
 
 /* ---- Affine sampling without a materialised grid ----------------------
  * nitorch builds affine_grid(mat, shape) (nitorch/spatial/_grid.py:579-615)

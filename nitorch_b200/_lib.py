@@ -73,7 +73,7 @@ EXPORTS = (
     "pp_sample_order_noalloc", "pp_brick_count", "pp_brick_order_workspace_bytes", "pp_brick_order",
     "pp_grid_pull_push", "pp_grid_pull_push_backward",
     "pp_batch_plan_bytes", "pp_batch_scratch_bytes", "pp_batch_plan", "pp_batch_run",
-    "pp_svf_compose", "pp_svf_compose_backward", "pp_affine_pull", "pp_affine_push",
+    "pp_svf_compose", "pp_svf_compose_backward", "pp_svf_workspace_bytes", "pp_affine_pull", "pp_affine_push",
     "pp_affine_grad_workspace_bytes", "pp_affine_grad_matrix", "pp_resize", "pp_resize_status",
     "pp_fmg_prolongation", "pp_fmg_restriction",
     "pp_grid_jacobian", "pp_grid_jacobian_backward", "pp_jacobian_det",
@@ -112,7 +112,9 @@ def _declare(L):
     L.pp_grid_jacobian_backward.argtypes = [T, T, T, T, i32, DP, i32, i32, vp]
     L.pp_jacobian_det.argtypes = [T, T, T, T, vp]
     L.pp_svf_compose.argtypes = [T, T, O, vp]
-    L.pp_svf_compose_backward.argtypes = [T, T, T, O, vp]
+    L.pp_svf_compose_backward.argtypes = [T, T, T, O, vp, vp, sz]
+    L.pp_svf_workspace_bytes.argtypes = [T]
+    L.pp_svf_workspace_bytes.restype = sz
     L.pp_affine_pull.argtypes = [T, T, T, O, vp]
     L.pp_affine_push.argtypes = [T, T, T, O, vp, vp, sz]
     L.pp_affine_grad_workspace_bytes.argtypes = [T]

@@ -285,6 +285,49 @@ int store_interleaved_fast(const float* acc, S* dst, int64_t N, int64_t V, int C
   return cuda_check(cudaGetLastError(), "interleaved store");
 }
 
+// A 4-slot channel-interleaved accumulator -> a float32 (N, X, Y, Z, 3)
+// field: contiguous fields copy three floats per voxel, others go through
+// the strided store on an (N, 3, X, Y, Z) view of the field.
+__global__ void store_field3(const float4* __restrict__ acc, float* __restrict__ dst, int64_t nvox) {
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < nvox; v += step) {
+    const float4 q = acc[v];
+    dst[3 * v] = q.x;
+    dst[3 * v + 1] = q.y;
+    dst[3 * v + 2] = q.z;
+  }
+}
+
+int store_interleaved_to(const float* acc, const pp_tensor* out, int CP, cudaStream_t st);
+
+int store_field_from4(const float* acc, const pp_tensor* field, cudaStream_t st) {
+  const int64_t n = numel(field);
+  if (n == 0) return PP_OK;
+  bool contiguous = true;
+  {
+    int64_t e = 1;
+    for (int i = field->ndim - 1; i >= 0 && contiguous; --i) {
+      if (field->sizes[i] > 1 && field->strides[i] != e) contiguous = false;
+      e *= field->sizes[i];
+    }
+  }
+  if (contiguous) {
+    const int64_t nvox = n / 3, want = (nvox + 255) / 256;
+    const unsigned nb = static_cast<unsigned>(want < 148 * 16 ? (want > 0 ? want : 1) : 148 * 16);
+    store_field3<<<nb, 256, 0, st>>>(reinterpret_cast<const float4*>(acc), static_cast<float*>(field->data), nvox);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "field store");
+  }
+  pp_tensor view = *field;  // (N, X, Y, Z, 3) as (N, 3, X, Y, Z)
+  view.sizes[1] = 3;
+  view.strides[1] = field->strides[4];
+  for (int d = 0; d < 3; ++d) {
+    view.sizes[2 + d] = field->sizes[1 + d];
+    view.strides[2 + d] = field->strides[1 + d];
+  }
+  return store_interleaved_to(acc, &view, 4, st);
+}
+
 int store_interleaved_to(const float* acc, const pp_tensor* out, int CP, cudaStream_t st) {
   const int64_t n = numel(out);
   if (n == 0) return PP_OK;
@@ -385,7 +428,7 @@ int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const u
 
 extern "C" {
 
-int pp_abi_version(void) { return 104; }
+int pp_abi_version(void) { return 105; }
 
 const char* pp_last_error(void) { return g_err.c_str(); }
 
@@ -837,8 +880,14 @@ int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_options
 // Its backward: grad_disp = g + push(g, id + u) + sum_c g_c grad(u_c)(id + u),
 // the gradient of <g, u + pull(u, id + u)> with respect to u, in one pass
 // (the push and the point's own terms accumulate atomically).
+size_t pp_svf_workspace_bytes(const pp_tensor* disp) {
+  if (!disp || disp->ndim != 5 || disp->sizes[4] != 3 || disp->dtype != PP_FLOAT32) return 0;
+  const int64_t vox = numel(disp) / 3;
+  return ((static_cast<size_t>(vox) * 16 + 255) / 256) * 256;
+}
+
 int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const pp_tensor* grad_disp,
-                            const pp_options* opt, void* stream) {
+                            const pp_options* opt, void* stream, void* workspace, size_t workspace_bytes) {
   Call k;
   int rc = prepare(k, disp, opt);
   if (rc) return rc;
@@ -864,8 +913,29 @@ int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const 
   field_as_image(grad_disp, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
   k.a.flags = ppk::F_A | ppk::F_GRAD | ppk::F_IDGRID | ppk::F_ADDSELF;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool wide = need_wide(k, {disp, grad, grad_disp});
+  const int iso = iso_order(k.D, k.order);
+  const size_t need = pp_svf_workspace_bytes(disp);
+  if (need && workspace && workspace_bytes >= need && reinterpret_cast<uintptr_t>(workspace) % 16 == 0 &&
+      (iso == 1 || iso == 3) && !wide && ppk::lanes_enabled() && grad_disp->dtype == PP_FLOAT32 &&
+      fits32(numel(disp) / 3 * 4)) {
+    // channel-interleaved accumulator (4 slots per voxel), one vector
+    // reduction per tap, then copied to the field
+    float* acc = static_cast<float*>(workspace);
+    const int64_t vox = numel(disp) / 3, V = vox / disp->sizes[0];
+    if ((rc = cuda_check(cudaMemsetAsync(acc, 0, static_cast<size_t>(vox) * 16, st), "workspace clear"))) return rc;
+    k.a.out = acc;
+    k.a.out_sN = V * 4;
+    k.a.out_sC = 1;
+    k.a.out_s[2] = 4;
+    k.a.out_s[1] = disp->sizes[3] * 4;
+    k.a.out_s[0] = disp->sizes[2] * disp->sizes[3] * 4;
+    k.a.flags |= ppk::F_VEC;
+    if ((rc = run(k, ppk::K_PUSHGRAD, wide, st))) return rc;
+    return store_field_from4(acc, grad_disp, st);
+  }
   if ((rc = zero_fill(grad_disp, st))) return rc;
-  return run(k, ppk::K_PUSHGRAD, need_wide(k, {disp, grad, grad_disp}), st);
+  return run(k, ppk::K_PUSHGRAD, wide, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -1390,7 +1390,7 @@ inline cudaError_t launch_one(const PPArgs& a, cudaStream_t st) {
     if (lanes_enabled() && a.det_acc == nullptr && !(a.flags & (F_AFFINE | F_NOTRGT)) && nb <= 0x7fffffffLL) {
       // pull backward into the interleaved accumulator: lane-split kernel
       if constexpr (CB >= 2) {
-        if ((a.flags & F_VEC) && !(a.flags & (F_IDGRID | F_ADDSELF))) {
+        if (a.flags & F_VEC) {
           note_kernel("pp_lanes_pullbwd_kernel", MODE, ORD, CB);
           pp_lanes_pullbwd_kernel<ORD, S, I, (CB == 2 ? 2 : 4), CB>
               <<<static_cast<unsigned>(nb), PP_THREADS, 0, st>>>(a);

@@ -63,9 +63,13 @@ def compose_backward(grad, disp, interpolation="linear", bound="dft", extrapolat
     g = grad.reshape(u.shape)
     out = torch.empty(u.shape, dtype=u.dtype, device=u.device)
     opt = _options(interpolation, bound, extrapolate)
+    du = _lib.desc(u)
+    nws = L.pp_svf_workspace_bytes(ctypes.byref(du))
+    ws = torch.empty(nws, dtype=torch.uint8, device=u.device) if nws else None  # the vector-reduction accumulator
     with _On(u):
-        _lib.check(L.pp_svf_compose_backward(ctypes.byref(_lib.desc(g)), ctypes.byref(_lib.desc(u)),
-                                             ctypes.byref(_lib.desc(out)), ctypes.byref(opt), _lib.stream_of(u)))
+        _lib.check(L.pp_svf_compose_backward(ctypes.byref(_lib.desc(g)), ctypes.byref(du),
+                                             ctypes.byref(_lib.desc(out)), ctypes.byref(opt), _lib.stream_of(u),
+                                             None if ws is None else ctypes.c_void_p(ws.data_ptr()), nws))
     return out[0] if unbatched else out.reshape(disp.shape)
 
 

@@ -36,7 +36,7 @@ def test_library_exports_every_symbol():
 
 def test_abi_version_and_error_state():
     L = _lib.load()
-    assert L.pp_abi_version() == 104
+    assert L.pp_abi_version() == 105
     assert isinstance(L.pp_last_error(), bytes)
 
 

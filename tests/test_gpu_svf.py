@@ -54,6 +54,38 @@ def test_compose_float32_and_channel_strides():
     assert relerr(svf.compose(uc).double().cpu().numpy(), ref) < 1e-5
 
 
+@pytest.mark.parametrize("order", [1, 3])
+@pytest.mark.parametrize("bound", ["dft", "dct2"])
+def test_compose_backward_float32_paths(order, bound):
+    """float32 3-D fields: the vector-reduction path (workspace given, field
+    contiguous or components first) and the per-component path (no
+    workspace) against the FP64 oracle."""
+    import ctypes
+    from nitorch_b200 import _lib
+    L = _lib.load()
+    u = _vel((21, 19, 17), seed=11 + order, scale=2.0)
+    g = _vel((21, 19, 17), seed=12, scale=1.0)
+    for ex in (True, False):
+        gref = O.svf_compose_backward(g.cpu().numpy(), u.cpu().numpy(), BOUNDS[bound], order, int(ex))
+        u32, g32 = u.float(), g.float()
+        assert relerr(svf.compose_backward(g32, u32, order, bound, ex).double().cpu().numpy(), gref) < 1e-5
+        opt = svf._options(order, bound, ex)
+        du, dg = _lib.desc(u32), _lib.desc(g32)
+        nws = L.pp_svf_workspace_bytes(ctypes.byref(du))
+        assert nws >= u32.numel() // 3 * 16
+        ws = torch.empty(nws, dtype=torch.uint8, device="cuda")
+        outs = {
+            "strided": torch.full((1, 3, 21, 19, 17), 7.0, device="cuda").movedim(1, -1),
+            "plain": torch.full_like(u32, 7.0),
+        }
+        for name, out in outs.items():
+            for w, n in ((ctypes.c_void_p(ws.data_ptr()), nws), (None, 0)):
+                _lib.check(L.pp_svf_compose_backward(ctypes.byref(dg), ctypes.byref(du),
+                                                     ctypes.byref(_lib.desc(out)), ctypes.byref(opt),
+                                                     _lib.stream_of(u32), w, n))
+                assert relerr(out.double().cpu().numpy(), gref) < 1e-5, (name, n, ex)
+
+
 @pytest.mark.parametrize("inverse", [False, True])
 def test_exp_vs_oracle(inverse):
     v = _vel((12, 11, 10), seed=5, scale=3.0)
