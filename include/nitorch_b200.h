@@ -210,14 +210,20 @@ PP_API int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_
                           void* stream);
 
 /* Gradient of <grad, u + pull(u, id + u)> with respect to u (the exact
- * adjoint of pp_svf_compose), written to grad_disp (disp's sizes, zero-filled
- * by the call, must not alias the inputs).  No deterministic mode.  With a
- * 16-byte aligned workspace of pp_svf_workspace_bytes(disp) bytes (3-D
- * float32 fields, linear or cubic), the push of the gradient goes to a
- * four-slot channel-interleaved accumulator with one vector reduction per
- * tap and is copied to grad_disp afterwards; with NULL / too small, one
- * reduction per component and tap into grad_disp. */
-PP_API size_t pp_svf_workspace_bytes(const pp_tensor* disp);
+ * adjoint of pp_svf_compose), written to grad_disp (disp's sizes, every
+ * element overwritten, must not alias the inputs).  Workspace: 16-byte
+ * aligned, pp_svf_workspace_bytes(disp, opt->flags) bytes.
+ *  - PP_DETERMINISTIC (float32 / float64 fields, workspace required): the
+ *    push of the gradient accumulates in int64 fixed point (scaled from
+ *    max |grad| and the voxel count) and each voxel's identity and
+ *    grid-gradient terms are stored by its own point, so the result is
+ *    bit-identical from run to run.
+ *  - otherwise, for 3-D float32 fields at orders 1 and 3, the push goes to a
+ *    four-slot channel-interleaved accumulator with one vector reduction
+ *    per tap and is copied to grad_disp afterwards; with NULL / too small a
+ *    workspace (or other fields), one reduction per component and tap
+ *    straight into grad_disp. */
+PP_API size_t pp_svf_workspace_bytes(const pp_tensor* disp, int32_t flags);
 PP_API int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp,
                                    const pp_tensor* grad_disp, const pp_options* opt, void* stream,
                                    void* workspace, size_t workspace_bytes);
@@ -372,8 +378,12 @@ PP_API int pp_sample_order_noalloc(const pp_tensor* grid, const int64_t* src_siz
  *   PP_BATCH_PULL_PUSH     src -> out = push(pull(src)) (scatter, src shaped)
  *   PP_BATCH_PULL_PUSH_BACKWARD src, trgt = d loss/d out laid out like src
  *                          -> out = d loss/d src (scatter, optional), gg
- * opt.sample_order (optional) is read when the plan runs.  Deterministic
- * mode is not available here. */
+ * opt.sample_order (optional) is read when the plan runs.  An entry with
+ * PP_DETERMINISTIC in opt.flags scatters into an int64 fixed-point
+ * accumulator in the scratch (pp_batch_scratch_bytes counts it; the plan
+ * fails with PP_ERR_WORKSPACE without it), scaled from max |pushed values|
+ * taken when the plan runs, and is finalized into `out`: bit-identical
+ * results from run to run. */
 #define PP_BATCH_PULL 0
 #define PP_BATCH_PUSH 2
 #define PP_BATCH_PUSH_BACKWARD 4
@@ -389,7 +399,8 @@ typedef struct pp_batch_entry {
 /* Host bytes of a plan for `nvol` volumes. */
 PP_API size_t pp_batch_plan_bytes(int32_t nvol);
 /* Device scratch (bytes) that lets the scatter entries of 2-4 channels at
- * orders 2-3 accumulate with vector reductions (0 if no entry does). */
+ * orders 2-3 accumulate with vector reductions, plus the fixed-point
+ * accumulators of deterministic scatter entries (0 if no entry needs any). */
 PP_API size_t pp_batch_scratch_bytes(const pp_batch_entry* entries, int32_t nvol, int32_t mode);
 /* Validates the entries and writes a plan into `plan` (host memory of
  * pp_batch_plan_bytes(nvol) bytes, owned by the caller).  ctas = 0: one CTA

@@ -113,7 +113,7 @@ def _declare(L):
     L.pp_jacobian_det.argtypes = [T, T, T, T, vp]
     L.pp_svf_compose.argtypes = [T, T, O, vp]
     L.pp_svf_compose_backward.argtypes = [T, T, T, O, vp, vp, sz]
-    L.pp_svf_workspace_bytes.argtypes = [T]
+    L.pp_svf_workspace_bytes.argtypes = [T, ctypes.c_int32]
     L.pp_svf_workspace_bytes.restype = sz
     L.pp_affine_pull.argtypes = [T, T, T, O, vp]
     L.pp_affine_push.argtypes = [T, T, T, O, vp, vp, sz]

@@ -102,8 +102,11 @@ class PullPushBatch:
     FORMS = ("fused", "chain", "percall")
 
     def __init__(self, shapes, channels, orders, bound="dct2", extrapolate=False,
-                 dtype=torch.float32, device=None, sorted_order=True, ctas=0, fused=True, form=None):
+                 dtype=torch.float32, device=None, sorted_order=True, ctas=0, fused=True, form=None,
+                 deterministic=False):
         self.device = torch.device(device or "cuda")
+        # scatters in int64 fixed point: bit-identical results from run to run
+        self.flags = _lib.PP_DETERMINISTIC if deterministic else 0
         self.n = len(shapes)
         self.shapes = [tuple(int(v) for v in s) for s in shapes]
         self.channels = [int(c) for c in channels]
@@ -176,8 +179,8 @@ class PullPushBatch:
             src = (ctypes.c_int64 * 3)(*s)
             nb.append(int(L.pp_brick_count(ctypes.byref(_lib.desc(g)), src)) + 1)
             ws = max(ws, L.pp_brick_order_workspace_bytes(ctypes.byref(_lib.desc(g)), src))
-            pws = max(pws, L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(z)), 0),
-                      L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(dx)), 0))
+            pws = max(pws, L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(z)), self.flags),
+                      L.pp_push_workspace_bytes(ctypes.byref(_lib.desc(dx)), self.flags))
         self.starts_flat, self.starts = _arena([(n,) for n in nb], torch.int32, dev)
         self.recs_flat, self.recs = _arena([(n, 4) for n in npts], torch.float32, dev)
         self.sort_ws = torch.empty(ws, dtype=torch.uint8, device=dev)
@@ -200,11 +203,11 @@ class PullPushBatch:
                                          ctypes.c_void_p(self.starts[i].data_ptr()),
                                          ctypes.c_void_p(self.recs[i].data_ptr()),
                                          ctypes.c_void_p(self.sort_ws.data_ptr()), self.sort_ws.numel(), stream))
-                opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, 0,
+                opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, self.flags,
                                       self.perm[i].data_ptr(), self.starts[i].data_ptr(),
                                       self.recs[i].data_ptr()))
             else:
-                opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, 0))
+                opts.append(B.options([self.bound], [self.orders[i]], self.extrapolate, self.flags))
         for i in range(self.n):
             o = ctypes.byref(opts[i])
             B.check(L.pp_grid_pull(ref(self.x[i]), ref(self.grid[i]), ref(self.y[i]), o, stream))
@@ -222,7 +225,7 @@ class PullPushBatch:
     # -- plans ---------------------------------------------------------------
     def _opt(self, i):
         perm = self.perm[i].data_ptr() if self.sorted_order else None
-        return _lib.options([self.bound], [self.orders[i]], self.extrapolate, 0, perm)
+        return _lib.options([self.bound], [self.orders[i]], self.extrapolate, self.flags, perm)
 
     def _build_plans(self):
         B = _lib

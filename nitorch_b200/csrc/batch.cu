@@ -80,9 +80,19 @@ __global__ void __launch_bounds__(256) batch_store_kernel(const __grid_constant_
 }
 
 
+// Deterministic scatter entry: its int64 fixed-point accumulator (after a
+// 256-byte header holding max |t| as float bits) in the scratch, the tensor
+// that max is taken over, and the output the accumulator is finalized into.
+struct DetJob {
+  unsigned int* mx;
+  unsigned long long* acc;
+  double bound;
+  pp_tensor tmax, out;
+};
+
 struct PlanHeader {
   uint32_t magic;
-  int32_t mode, ctas, nvol, dtype, ngroups, nfill, nstore;
+  int32_t mode, ctas, nvol, dtype, ngroups, nfill, nstore, ndet, pad;
   int32_t gfirst[kMaxGroups], gcount[kMaxGroups], gorder[kMaxGroups], gcb[kMaxGroups];
 };
 
@@ -92,10 +102,16 @@ struct Fill {  // a byte range to zero before the launches
 };
 
 // Layout of the host plan buffer: header, then per volume its PPArgs and its
-// item count (sorted by group), the fill ranges, then the interleaved stores.
+// item count (sorted by group), the fill ranges, the interleaved stores,
+// then the deterministic entries.
 inline size_t plan_bytes(int nvol) {
-  return sizeof(PlanHeader) +
-         static_cast<size_t>(nvol) * (sizeof(ppk::PPArgs) + sizeof(int64_t) + sizeof(Fill) + sizeof(VecStore));
+  return sizeof(PlanHeader) + static_cast<size_t>(nvol) * (sizeof(ppk::PPArgs) + sizeof(int64_t) + sizeof(Fill) +
+                                                           sizeof(VecStore) + sizeof(DetJob));
+}
+
+// Scratch of a deterministic scatter entry: header + int64 per output element.
+inline size_t det_bytes(const pp_tensor& out) {
+  return 256 + ((static_cast<size_t>(ppc::numel(&out)) * 8 + 255) / 256) * 256;
 }
 
 // Channel slots of the interleaved accumulator of a scatter entry (0: the
@@ -121,13 +137,18 @@ extern "C" {
 size_t pp_batch_plan_bytes(int32_t nvol) { return nvol > 0 ? plan_bytes(nvol) : 0; }
 
 // Device scratch for the channel-interleaved accumulators of the entries
-// that scatter with vector reductions (0 if none does).
+// that scatter with vector reductions and the fixed-point accumulators of
+// the deterministic scatter entries (0 if there are none).
 size_t pp_batch_scratch_bytes(const pp_batch_entry* items, int32_t nvol, int32_t mode) {
   if (!items || nvol <= 0) return 0;
   size_t total = 0;
   for (int v = 0; v < nvol; ++v) {
     const pp_batch_entry& it = items[v];
     if (!it.out.data || it.out.ndim != 5) continue;
+    if (it.opt.flags & PP_DETERMINISTIC) {
+      if (is_scatter(mode)) total += det_bytes(it.out);
+      continue;
+    }
     int bound[3], ord[3];
     if (read_options(&it.opt, 3, bound, ord)) continue;
     const int iso = (ord[0] == ord[1] && ord[0] == ord[2]) ? ord[0] : -1;
@@ -153,6 +174,7 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
   std::vector<int64_t> nitems(nvol);
   std::vector<Fill> fills;
   std::vector<VecStore> stores;
+  std::vector<DetJob> dets;
   size_t scratch_used = 0;
   const bool use_scratch = scratch && scratch_bytes >= pp_batch_scratch_bytes(items, nvol, mode) &&
                            reinterpret_cast<uintptr_t>(scratch) % 256 == 0;
@@ -166,8 +188,7 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
     if (!grid->data || grid->ndim != 5 || grid->sizes[4] != 3 || grid->sizes[0] != 1)
       return fail(PP_ERR_ARG, "(): batch entry %d: expected a (1, X, Y, Z, 3) grid", v);
     if (grid->dtype != PP_FLOAT32) return fail(PP_ERR_DTYPE, "(): batch entry %d: grid must be float32", v);
-    if (it.opt.flags & PP_DETERMINISTIC)
-      return fail(PP_ERR_UNSUPPORTED, "(): batch entry %d: batched launches have no deterministic mode", v);
+    const bool det = (it.opt.flags & PP_DETERMINISTIC) != 0;
     int bound[3], ord[3];
     int rc = read_options(&it.opt, 3, bound, ord);
     if (rc) return rc;
@@ -262,8 +283,33 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
     order[v] = iso;
     cbs[v] = static_cast<int>(a.C >= 4 ? 4 : a.C);
     nitems[v] = (a.nvox + kBatchPoints - 1) / kBatchPoints;
-    const int CP = scatter && out && use_scratch ? entry_slots(mode, a.C, iso) : 0;
-    if (CP) {
+    const int CP = scatter && out && use_scratch && !det ? entry_slots(mode, a.C, iso) : 0;
+    if (scatter && out && det) {
+      // order-independent int64 fixed-point accumulation (scale from
+      // max |pushed values| and the point count), finalized into `out`
+      if (!use_scratch)
+        return fail(PP_ERR_WORKSPACE, "(): batch entry %d: the deterministic mode needs the plan's scratch", v);
+      unsigned char* w = static_cast<unsigned char*>(scratch) + scratch_used;
+      scratch_used += det_bytes(*out);
+      DetJob j;
+      j.mx = reinterpret_cast<unsigned int*>(w);
+      j.acc = reinterpret_cast<unsigned long long*>(w + 256);
+      j.bound = static_cast<double>(a.nvox);
+      j.tmax = mode == ppk::K_PP ? *src : *trg;  // what is pushed: pulled src (K_PP) or trgt
+      j.out = *out;
+      const int64_t V = out->sizes[2] * out->sizes[3] * out->sizes[4];
+      a.det_acc = j.acc;
+      a.det_max = j.mx;
+      a.det_bound = j.bound;
+      a.out = nullptr;
+      a.out_sN = a.C * V;
+      a.out_sC = V;
+      a.out_s[0] = out->sizes[3] * out->sizes[4];
+      a.out_s[1] = out->sizes[4];
+      a.out_s[2] = 1;
+      fills.push_back({w, det_bytes(*out)});
+      dets.push_back(j);
+    } else if (CP) {
       // vector reductions into this entry's interleaved accumulator, stored
       // to `out` after the launches
       const int64_t V = out->sizes[2] * out->sizes[3] * out->sizes[4];
@@ -327,6 +373,9 @@ int pp_batch_plan(const pp_batch_entry* items, int32_t nvol, int32_t mode, int32
   VecStore* ps = reinterpret_cast<VecStore*>(pf + nvol);
   for (size_t i = 0; i < stores.size(); ++i) ps[i] = stores[i];
   h->nstore = static_cast<int32_t>(stores.size());
+  DetJob* pd = reinterpret_cast<DetJob*>(ps + nvol);
+  for (size_t i = 0; i < dets.size(); ++i) pd[i] = dets[i];
+  h->ndet = static_cast<int32_t>(dets.size());
   return PP_OK;
 }
 
@@ -339,10 +388,14 @@ int pp_batch_run(const void* plan, void* stream) {
   const int64_t* pn = reinterpret_cast<const int64_t*>(pa + h->nvol);
   const Fill* pf = reinterpret_cast<const Fill*>(pn + h->nvol);
   const VecStore* ps = reinterpret_cast<const VecStore*>(pf + h->nvol);
+  const DetJob* pd = reinterpret_cast<const DetJob*>(ps + h->nvol);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc;
   for (int f = 0; f < h->nfill; ++f)
     if ((rc = cuda_check(cudaMemsetAsync(pf[f].ptr, 0, pf[f].bytes, st), "batch zero fill"))) return rc;
+  // deterministic entries: the scale of each fixed-point accumulator
+  for (int d = 0; d < h->ndet; ++d)
+    if ((rc = det_absmax_of(&pd[d].tmax, pd[d].mx, st))) return rc;
   static thread_local BatchLaunch L;  // 32 KB: not on the stack
   for (int g = 0; g < h->ngroups; ++g) {
     for (int c0 = 0; c0 < h->gcount[g]; c0 += kMaxEntries) {
@@ -374,6 +427,8 @@ int pp_batch_run(const void* plan, void* stream) {
     count_launch();
     if ((rc = cuda_check(cudaGetLastError(), "batched interleaved store"))) return rc;
   }
+  for (int d = 0; d < h->ndet; ++d)
+    if ((rc = det_finalize_to(pd[d].acc, &pd[d].out, pd[d].mx, pd[d].bound, st))) return rc;
   return PP_OK;
 }
 

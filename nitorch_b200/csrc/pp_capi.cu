@@ -373,10 +373,12 @@ __global__ void det_absmax(const S* t, Strided s, unsigned int* out) {
 
 __global__ void det_set_one(unsigned int* out) { *out = __float_as_uint(1.0f); }
 
-// int64 fixed point -> strided output
+// int64 fixed point (plus, when `self` is set, a term per element in the
+// accumulation type laid out like acc) -> strided output
 template <class S>
 __global__ void det_finalize(const unsigned long long* acc, S* dst, Strided s, const unsigned int* mx,
-                             double bound) {
+                             double bound, const typename ppk::Acc<S>::type* self) {
+  using A = typename ppk::Acc<S>::type;
   const float m = __uint_as_float(*mx);
   const double b = static_cast<double>(m) * bound;
   double inv = 1.0;
@@ -389,9 +391,15 @@ __global__ void det_finalize(const unsigned long long* acc, S* dst, Strided s, c
   const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (; i < s.numel; i += step) {
     const double v = static_cast<double>(static_cast<long long>(acc[i])) * inv;
-    dst[strided_offset(s, i)] = ppk::from_acc<S>(static_cast<typename ppk::Acc<S>::type>(v));
+    A r = static_cast<A>(v);
+    if (self) r += self[i];
+    dst[strided_offset(s, i)] = ppk::from_acc<S>(r);
   }
 }
+
+}  // namespace
+
+namespace ppc {
 
 int det_absmax_of(const pp_tensor* t, unsigned int* out, cudaStream_t st) {
   const int64_t n = numel(t);
@@ -409,22 +417,34 @@ int det_absmax_of(const pp_tensor* t, unsigned int* out, cudaStream_t st) {
 }
 
 int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const unsigned int* mx, double bound,
-                    cudaStream_t st) {
+                    cudaStream_t st, const void* self) {
   const int64_t n = numel(out);
   if (n == 0) return PP_OK;
   Strided s = make_strided(out);
   const int nb = grid_blocks(n);
   switch (out->dtype) {
-    case PP_FLOAT32: det_finalize<float><<<nb, 256, 0, st>>>(acc, static_cast<float*>(out->data), s, mx, bound); break;
-    case PP_FLOAT64: det_finalize<double><<<nb, 256, 0, st>>>(acc, static_cast<double*>(out->data), s, mx, bound); break;
-    case PP_BFLOAT16: det_finalize<__nv_bfloat16><<<nb, 256, 0, st>>>(acc, static_cast<__nv_bfloat16*>(out->data), s, mx, bound); break;
-    default: det_finalize<__half><<<nb, 256, 0, st>>>(acc, static_cast<__half*>(out->data), s, mx, bound); break;
+    case PP_FLOAT32:
+      det_finalize<float><<<nb, 256, 0, st>>>(acc, static_cast<float*>(out->data), s, mx, bound,
+                                              static_cast<const float*>(self));
+      break;
+    case PP_FLOAT64:
+      det_finalize<double><<<nb, 256, 0, st>>>(acc, static_cast<double*>(out->data), s, mx, bound,
+                                               static_cast<const double*>(self));
+      break;
+    case PP_BFLOAT16:
+      det_finalize<__nv_bfloat16><<<nb, 256, 0, st>>>(acc, static_cast<__nv_bfloat16*>(out->data), s, mx, bound,
+                                                      static_cast<const float*>(self));
+      break;
+    default:
+      det_finalize<__half><<<nb, 256, 0, st>>>(acc, static_cast<__half*>(out->data), s, mx, bound,
+                                               static_cast<const float*>(self));
+      break;
   }
   count_launch();
   return cuda_check(cudaGetLastError(), "deterministic finalize");
 }
 
-}  // namespace
+}  // namespace ppc
 
 extern "C" {
 
@@ -880,10 +900,19 @@ int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_options
 // Its backward: grad_disp = g + push(g, id + u) + sum_c g_c grad(u_c)(id + u),
 // the gradient of <g, u + pull(u, id + u)> with respect to u, in one pass
 // (the push and the point's own terms accumulate atomically).
-size_t pp_svf_workspace_bytes(const pp_tensor* disp) {
-  if (!disp || disp->ndim != 5 || disp->sizes[4] != 3 || disp->dtype != PP_FLOAT32) return 0;
-  const int64_t vox = numel(disp) / 3;
-  return ((static_cast<size_t>(vox) * 16 + 255) / 256) * 256;
+static size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+size_t pp_svf_workspace_bytes(const pp_tensor* disp, int32_t flags) {
+  if (!disp || disp->ndim < 3 || disp->ndim > 5 || disp->sizes[disp->ndim - 1] != disp->ndim - 2) return 0;
+  const int64_t n = numel(disp);
+  if (flags & PP_DETERMINISTIC) {
+    // max |grad| (256 B), the push part as int64 fixed point, the identity
+    // and grid-gradient terms of every voxel in the accumulation type
+    if (disp->dtype != PP_FLOAT32 && disp->dtype != PP_FLOAT64) return 0;
+    return 256 + round256(static_cast<size_t>(n) * 8) + round256(static_cast<size_t>(n) * (disp->dtype == PP_FLOAT64 ? 8 : 4));
+  }
+  if (disp->ndim != 5 || disp->dtype != PP_FLOAT32) return 0;
+  return round256(static_cast<size_t>(n / 3) * 16);
 }
 
 int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const pp_tensor* grad_disp,
@@ -891,8 +920,7 @@ int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const 
   Call k;
   int rc = prepare(k, disp, opt);
   if (rc) return rc;
-  if (opt->flags & PP_DETERMINISTIC)
-    return fail(PP_ERR_UNSUPPORTED, "(): the self-composition backward has no deterministic mode");
+  const bool det = (opt->flags & PP_DETERMINISTIC) != 0;
   if ((rc = check_tensor(grad, "grad"))) return rc;
   if ((rc = check_same_sizes(grad, disp->sizes, disp->ndim, "grad"))) return rc;
   if ((rc = check_tensor(grad_disp, "grad_disp"))) return rc;
@@ -915,7 +943,43 @@ int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const bool wide = need_wide(k, {disp, grad, grad_disp});
   const int iso = iso_order(k.D, k.order);
-  const size_t need = pp_svf_workspace_bytes(disp);
+  if (det) {
+    // Deterministic: the push of grad into int64 fixed point (order-free
+    // integer atomics), the identity and grid-gradient terms of each voxel
+    // stored by the voxel's own point into a separate buffer, the two added
+    // by the finalize pass.
+    const size_t dneed = pp_svf_workspace_bytes(disp, PP_DETERMINISTIC);
+    if (!dneed) return fail(PP_ERR_DTYPE, "(): the deterministic self-composition backward needs float32/64 fields");
+    if (!workspace || workspace_bytes < dneed || reinterpret_cast<uintptr_t>(workspace) % 16 != 0)
+      return fail(PP_ERR_WORKSPACE, "(): the deterministic mode needs %zu bytes of 16-byte aligned workspace", dneed);
+    const int64_t n = numel(disp);
+    unsigned char* w = static_cast<unsigned char*>(workspace);
+    unsigned int* mx = reinterpret_cast<unsigned int*>(w);
+    unsigned long long* acc = reinterpret_cast<unsigned long long*>(w + 256);
+    void* self = w + 256 + round256(static_cast<size_t>(n) * 8);
+    if ((rc = cuda_check(cudaMemsetAsync(w, 0, 256 + static_cast<size_t>(n) * 8, st), "workspace clear"))) return rc;
+    if ((rc = det_absmax_of(grad, mx, st))) return rc;
+    // accumulators in the field's own (N, *spatial, D) order
+    int64_t per_item = 1;
+    for (int a = 0; a < k.D; ++a) per_item *= disp->sizes[1 + a];
+    k.a.det_acc = acc;
+    k.a.det_max = mx;
+    k.a.det_bound = static_cast<double>(per_item);
+    k.a.aux = self;
+    k.a.out = nullptr;
+    k.a.out_sN = per_item * k.D;
+    k.a.out_sC = 1;
+    {
+      int64_t s = k.D;
+      for (int a = 2; a >= 0; --a) {
+        k.a.out_s[a] = a < k.D ? s : 0;
+        if (a < k.D) s *= disp->sizes[1 + a];
+      }
+    }
+    if ((rc = run(k, ppk::K_PUSHGRAD, wide, st))) return rc;
+    return det_finalize_to(acc, grad_disp, mx, k.a.det_bound, st, self);
+  }
+  const size_t need = pp_svf_workspace_bytes(disp, 0);
   if (need && workspace && workspace_bytes >= need && reinterpret_cast<uintptr_t>(workspace) % 16 == 0 &&
       (iso == 1 || iso == 3) && !wide && ppk::lanes_enabled() && grad_disp->dtype == PP_FLOAT32 &&
       fits32(numel(disp) / 3 * 4)) {

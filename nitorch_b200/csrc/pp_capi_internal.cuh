@@ -163,4 +163,12 @@ void set_image(const pp_tensor* t, int D, int64_t& sN, int64_t& sC, int64_t s[3]
 void set_grid(const pp_tensor* t, int D, int64_t& sN, int64_t s[3], int64_t& sD);
 bool fits32(int64_t v);
 
+// Deterministic scatters (pp_capi.cu): max |t| of a tensor as float bits
+// into *out (which starts at zero), and the int64 fixed-point accumulator
+// (contiguous in out's logical order, scale from *mx times bound) -> out,
+// plus `self` (accumulation-type values laid out like acc) where given.
+int det_absmax_of(const pp_tensor* t, unsigned int* out, cudaStream_t st);
+int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const unsigned int* mx, double bound,
+                    cudaStream_t st, const void* self = nullptr);
+
 }  // namespace ppc

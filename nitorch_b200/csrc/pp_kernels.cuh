@@ -256,8 +256,13 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
         }
         if (MODE == K_PUSHGRAD) {
           const S* tp = static_cast<const S*>(a.trgt) + tvox;
-          T* op = static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN + oo;
-          for (int64_t c = 0; c < a.C; ++c) atomic_acc(op + c * a.out_sC, ldg_acc(tp + c * a.trgt_sC));
+          if (a.det_acc != nullptr) {  // deterministic: this point alone writes its terms (aux)
+            T* sp = static_cast<T*>(a.aux) + static_cast<int64_t>(n) * a.out_sN + oo;
+            for (int64_t c = 0; c < a.C; ++c) sp[c * a.out_sC] = ldg_acc(tp + c * a.trgt_sC);
+          } else {
+            T* op = static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN + oo;
+            for (int64_t c = 0; c < a.C; ++c) atomic_acc(op + c * a.out_sC, ldg_acc(tp + c * a.trgt_sC));
+          }
         }
         return;
       }
@@ -620,10 +625,19 @@ __device__ __forceinline__ void pp_point(const PPArgs& a, const I (&sub)[3], con
       int64_t oo = 0;
 #pragma unroll
       for (int d = 0; d < D; ++d) oo += static_cast<int64_t>(sub[d]) * a.out_s[d];
-      T* op = static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN + oo;
       const T og[3] = {og0, og1, og2};
+      if (a.det_acc != nullptr) {
+        // deterministic mode: the terms of this voxel have no other writer;
+        // stored apart (aux, laid out like the fixed-point accumulator) and
+        // added to the push by the finalize pass
+        T* sp = static_cast<T*>(a.aux) + static_cast<int64_t>(n) * a.out_sN + oo;
 #pragma unroll
-      for (int d = 0; d < D; ++d) atomic_acc(op + d * a.out_sC, og[d] + ldg_acc(trg_v + d * a.trgt_sC));
+        for (int d = 0; d < D; ++d) sp[d * a.out_sC] = og[d] + ldg_acc(trg_v + d * a.trgt_sC);
+      } else {
+        T* op = static_cast<T*>(a.out) + static_cast<int64_t>(n) * a.out_sN + oo;
+#pragma unroll
+        for (int d = 0; d < D; ++d) atomic_acc(op + d * a.out_sC, og[d] + ldg_acc(trg_v + d * a.trgt_sC));
+      }
     } else if (do_grad) {
       T* g = static_cast<T*>(a.gg) + gvox;
       g[0] = og0;

@@ -23,16 +23,16 @@ import torch
 
 from . import _lib
 from .grid import bound_to_nitorch, inter_to_nitorch
-from .spatial import _On, _require_cuda
+from .spatial import _On, _require_cuda, get_deterministic
 
 __all__ = ["exp", "compose", "compose_backward"]
 
 
-def _options(interpolation, bound, extrapolate=True):
+def _options(interpolation, bound, extrapolate=True, flags=0):
     b = bound_to_nitorch(bound if isinstance(bound, (list, tuple)) else [bound], as_type="enum")
     o = inter_to_nitorch(interpolation if isinstance(interpolation, (list, tuple)) else [interpolation],
                          as_type="enum")
-    return _lib.options([int(x) for x in b], [int(x) for x in o], int(extrapolate))
+    return _lib.options([int(x) for x in b], [int(x) for x in o], int(extrapolate), flags)
 
 
 def _batched(field):
@@ -55,17 +55,23 @@ def compose(disp, interpolation="linear", bound="dft", extrapolate=True):
     return out[0] if unbatched else out.reshape(disp.shape)
 
 
-def compose_backward(grad, disp, interpolation="linear", bound="dft", extrapolate=True):
-    """Gradient of <grad, compose(disp)> with respect to disp."""
+def compose_backward(grad, disp, interpolation="linear", bound="dft", extrapolate=True, deterministic=None):
+    """Gradient of <grad, compose(disp)> with respect to disp.  With
+    `deterministic` (default: the library's deterministic switch,
+    ``set_deterministic``) the result is bit-identical from run to run."""
     _require_cuda(disp)
     L = _lib.load()
     u, unbatched = _batched(disp)
     g = grad.reshape(u.shape)
     out = torch.empty(u.shape, dtype=u.dtype, device=u.device)
-    opt = _options(interpolation, bound, extrapolate)
+    det = get_deterministic() if deterministic is None else bool(deterministic)
+    flags = _lib.PP_DETERMINISTIC if det else 0
+    opt = _options(interpolation, bound, extrapolate, flags)
     du = _lib.desc(u)
-    nws = L.pp_svf_workspace_bytes(ctypes.byref(du))
-    ws = torch.empty(nws, dtype=torch.uint8, device=u.device) if nws else None  # the vector-reduction accumulator
+    nws = L.pp_svf_workspace_bytes(ctypes.byref(du), flags)
+    # the vector-reduction accumulator, or the fixed-point accumulator and the
+    # per-voxel terms of the deterministic mode
+    ws = torch.empty(nws, dtype=torch.uint8, device=u.device) if nws else None
     with _On(u):
         _lib.check(L.pp_svf_compose_backward(ctypes.byref(_lib.desc(g)), ctypes.byref(du),
                                              ctypes.byref(_lib.desc(out)), ctypes.byref(opt), _lib.stream_of(u),

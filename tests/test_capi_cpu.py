@@ -94,6 +94,20 @@ def test_workspace_query():
     assert L.pp_push_workspace_bytes(ctypes.byref(d), 0) == 0
 
 
+def test_svf_workspace_query():
+    L = _lib.load()
+    u = _lib.desc(torch.zeros((1, 4, 5, 6, 3), dtype=torch.float32))
+    n = 4 * 5 * 6 * 3
+    r = lambda b: (b + 255) // 256 * 256  # noqa: E731
+    assert L.pp_svf_workspace_bytes(ctypes.byref(u), 0) == r(n // 3 * 16)
+    assert L.pp_svf_workspace_bytes(ctypes.byref(u), _lib.PP_DETERMINISTIC) == 256 + r(n * 8) + r(n * 4)
+    u2 = _lib.desc(torch.zeros((2, 7, 9, 2), dtype=torch.float64))
+    assert L.pp_svf_workspace_bytes(ctypes.byref(u2), 0) == 0  # 2-D: scalar reductions, no workspace
+    assert L.pp_svf_workspace_bytes(ctypes.byref(u2), _lib.PP_DETERMINISTIC) == 256 + r(2 * 7 * 9 * 2 * 8) * 2
+    bad = _lib.desc(torch.zeros((1, 4, 5, 6, 2), dtype=torch.float32))  # 3-D field with 2 components
+    assert L.pp_svf_workspace_bytes(ctypes.byref(bad), _lib.PP_DETERMINISTIC) == 0
+
+
 def test_batch_plan_validation_on_host():
     """pp_batch_plan validates and plans on the host only (no CUDA call)."""
     from nitorch_b200.batch import _entry
@@ -121,7 +135,11 @@ def test_batch_plan_validation_on_host():
     high = _entry(src=x, grid=g, out=z, opt=_lib.options([2], [5], 0))
     assert plan(_lib.PP_BATCH_PULL_PUSH, [high]) == _lib.PP_ERR_UNSUPPORTED
     det = _entry(src=x, grid=g, out=z, opt=_lib.options([2], [1], 0, flags=_lib.PP_DETERMINISTIC))
-    assert plan(_lib.PP_BATCH_PULL_PUSH, [det]) == _lib.PP_ERR_UNSUPPORTED
+    assert plan(_lib.PP_BATCH_PULL_PUSH, [det]) == _lib.PP_ERR_WORKSPACE  # the fixed-point scratch is required
+    arr = (_lib.PPBatchEntry * 2)(det, ok)
+    # header + int64 per output element, plus the interleaved accumulator of `ok`
+    assert L.pp_batch_scratch_bytes(arr, 2, _lib.PP_BATCH_PULL_PUSH) == \
+        256 + 2 * 6 * 5 * 4 * 8 // 256 * 256 + 256 + 6 * 5 * 4 * 2 * 4 // 256 * 256 + 256
     small = _entry(src=x, grid=g, out=torch.zeros(1, 2, 6, 5, 3), opt=_lib.options([2], [1], 0))
     assert plan(_lib.PP_BATCH_PULL_PUSH, [small]) == _lib.PP_ERR_ARG
     half = _entry(src=x, grid=g, out=z.bfloat16(), opt=_lib.options([2], [1], 0))

@@ -71,7 +71,7 @@ def test_compose_backward_float32_paths(order, bound):
         assert relerr(svf.compose_backward(g32, u32, order, bound, ex).double().cpu().numpy(), gref) < 1e-5
         opt = svf._options(order, bound, ex)
         du, dg = _lib.desc(u32), _lib.desc(g32)
-        nws = L.pp_svf_workspace_bytes(ctypes.byref(du))
+        nws = L.pp_svf_workspace_bytes(ctypes.byref(du), 0)
         assert nws >= u32.numel() // 3 * 16
         ws = torch.empty(nws, dtype=torch.uint8, device="cuda")
         outs = {
