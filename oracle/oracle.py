@@ -616,3 +616,264 @@ def solver_restrict(x, shape=None, bound=2, order=1):
     grid = _edge_grid(shape, sp, x.shape[0])
     y = grid_push(np.moveaxis(x, -1, 1), grid, shape, [bound], [order], 1)
     return np.moveaxis(y, 1, -1) * (np.prod(shape) / np.prod(sp))
+
+
+# ---------------------------------------------------------------------------
+# Field and grid regularisers (nitorch._C.solve.c_regulariser /
+# c_regulariser_grid; kernels nitorch/_C/src/impl/regulariser_common.cpp and
+# regulariser_grid_common.cpp).  Every mode of the reference is a linear
+# stencil: differences to the centre along +-1 and +-2 steps of an axis and
+# along the diagonals of an axis pair, plus (grids) the Lame cross terms and
+# (both) the Hessian product at the voxel.  Neighbours are read with the
+# boundary index and sign of every axis they step along; a difference is
+# sign * value(neighbour) - value(centre), as the reference forms it.
+# ---------------------------------------------------------------------------
+
+def _unfold3(v, default):
+    """VEC_UNFOLD (regulariser_common.cpp:30-36): three entries, the last
+    given one repeated, `default` when empty."""
+    v = [float(x) for x in v] if v is not None else []
+    if not v:
+        return [default] * 3
+    return [v[min(i, len(v) - 1)] for i in range(3)]
+
+
+def _per_channel(v, C):
+    """set_factors (regulariser_common.cpp:263-280): C entries, the last given
+    one repeated, 0 when empty."""
+    v = [float(x) for x in v] if v is not None else []
+    if not v:
+        return [0.0] * C
+    return [v[min(c, len(v) - 1)] for c in range(C)]
+
+
+class _Nbr:
+    """Neighbour gather for the regularisers: value(x + o) of an (N, K,
+    *spatial) array for an offset vector o, with boundary index and sign."""
+
+    def __init__(self, shape, bounds):
+        self.shape = shape
+        self.bounds = bounds
+        self.cache = {}
+
+    def axis(self, a, o):
+        key = (a, o)
+        if key not in self.cache:
+            n = self.shape[a]
+            # zero bound: out-of-axis nodes carry sign 0 (index clipped for the read)
+            idx = np.array([min(max(_bound_index(self.bounds[a], i + o, n), 0), n - 1) for i in range(n)])
+            sgn = np.array([_bound_sign(self.bounds[a], i + o, n) for i in range(n)], dtype=np.float64)
+            self.cache[key] = (idx, sgn)
+        return self.cache[key]
+
+    def get(self, arr, offs):
+        """sign * arr at the offset neighbour of every voxel (arr: (..., *spatial))."""
+        dim = len(self.shape)
+        out = arr
+        sign = np.ones(self.shape)
+        for a in range(dim):
+            if offs[a] == 0:
+                continue
+            idx, sgn = self.axis(a, offs[a])
+            out = np.take(out, idx, axis=arr.ndim - dim + a)
+            shp = [1] * dim
+            shp[a] = self.shape[a]
+            sign = sign * sgn.reshape(shp)
+        return out * sign
+
+
+def _step(dim, a, s):
+    o = [0] * dim
+    o[a] = s
+    return o
+
+
+def _diag(dim, a, b, sa, sb):
+    o = [0] * dim
+    o[a] = sa
+    o[b] = sb
+    return o
+
+
+def _hessian_field(h, u, C):
+    """matvec_eye / _diag / _estatics / _sym (regulariser_common.cpp:592-672)
+    of an (N, CC, *spatial) Hessian and an (N, C, *spatial) field."""
+    CC = h.shape[1]
+    out = np.zeros_like(u)
+    if CC == 1:
+        return h[:, :1] * u
+    if CC == C:
+        return h * u
+    if CC == 2 * C - 1:
+        r = h[:, C - 1]
+        s = u[:, C - 1]
+        acc = s * r
+        for c in range(C - 1):
+            out[:, c] += h[:, c] * u[:, c] + h[:, C + c] * s
+            acc = acc + h[:, C + c] * u[:, c]
+        out[:, C - 1] += acc
+        return out
+    k = C
+    for c in range(C):
+        out[:, c] += h[:, c] * u[:, c]
+    for c in range(C):
+        for cc in range(c + 1, C):
+            out[:, cc] += h[:, k] * u[:, c]
+            out[:, c] += h[:, k] * u[:, cc]
+            k += 1
+    return out
+
+
+def regulariser(x, weight=None, hessian=None, absolute=(), membrane=(), bending=(), voxel_size=(1.0,),
+                bound=(2,)):
+    """(H + L) x for an (N, C, *spatial) field, 1-3-D
+    (regulariser_common.cpp: set_kernel :285-299, vel2mom3d_bending :752-804,
+    _membrane :808-839, _absolute :843-856, _rls_membrane :860-903,
+    _rls_absolute :907-925, and their 2-D / 1-D forms).  weight (N, C|1,
+    *spatial) weights the absolute and membrane energies (bending with a
+    weight is an error, as there); hessian (N, CC, *spatial), CC in {1, C,
+    2C-1, C(C+1)/2}.  Weights are read per batch item."""
+    x = np.asarray(x, np.float64)
+    N, C = x.shape[:2]
+    shape = x.shape[2:]
+    dim = len(shape)
+    a = _per_channel(absolute, C)
+    m = _per_channel(membrane, C)
+    b = _per_channel(bending, C)
+    vs = _unfold3(voxel_size, 1.0)
+    vx = [1.0 / (v * v) for v in vs]
+    vx = [vx[i] if i < dim else 0.0 for i in range(3)]
+    bnd = [int(v) for v in _unfold3(bound, 0.0)]
+    nb = _Nbr(shape, bnd)
+    svx = sum(vx)
+    m1 = [-vx[i] for i in range(3)]
+    b1 = [-4.0 * vx[i] * svx for i in range(3)]
+    b2 = [vx[i] * vx[i] for i in range(3)]
+    out = np.zeros_like(x)
+    w = None
+    if weight is not None:
+        if any(b):
+            raise ValueError("RLS only implemented for absolute/membrane")
+        w = np.broadcast_to(np.asarray(weight, np.float64), x.shape)
+    for c in range(C):
+        u = x[:, c]
+        if w is not None:
+            wc = w[:, c]
+            acc = a[c] * wc * u
+            if m[c]:
+                sm = np.zeros_like(u)
+                for ax in range(dim):
+                    for s in (-1, 1):
+                        o = _step(dim, ax, s)
+                        sm += m1[ax] * (wc + nb.get(wc, o)) * (nb.get(u, o) - u)
+                acc = acc + m[c] * 0.5 * sm
+            out[:, c] = acc
+            continue
+        acc = a[c] * u
+        for ax in range(dim):
+            w1 = m[c] * m1[ax] + b[c] * b1[ax]
+            acc = acc + w1 * (nb.get(u, _step(dim, ax, -1)) - u + nb.get(u, _step(dim, ax, 1)) - u)
+        if b[c]:
+            bb = np.zeros_like(u)
+            for ax in range(dim):
+                bb += b2[ax] * (nb.get(u, _step(dim, ax, -2)) - u + nb.get(u, _step(dim, ax, 2)) - u)
+            for i in range(dim):
+                for j in range(i + 1, dim):
+                    wp = 2.0 * vx[i] * vx[j]
+                    for si in (-1, 1):
+                        for sj in (-1, 1):
+                            bb += wp * (nb.get(u, _diag(dim, i, j, si, sj)) - u)
+            acc = acc + b[c] * bb
+        out[:, c] = acc
+    if hessian is not None:
+        h = np.broadcast_to(np.asarray(hessian, np.float64), (N, np.asarray(hessian).shape[1]) + shape)
+        out = out + _hessian_field(h, x, C)
+    return out
+
+
+def regulariser_grid(x, weight=None, hessian=None, absolute=0.0, membrane=0.0, bending=0.0, shear=0.0, div=0.0,
+                     voxel_size=(1.0,), bound=(5,)):
+    """(H + L) x for an (N, D, *spatial) displacement field (components
+    second, as the native front-end takes it), 1-3-D
+    (regulariser_grid_common.cpp: set_kernel :265-298; vel2mom3d_lame
+    :927-1084, _all, _bending, _membrane :1088-1144, _absolute :1147-1166,
+    _rls_membrane, _rls_absolute, and their 2-D / 1-D forms).  Component d
+    is scaled by the squared voxel size of its axis; the Lame terms (shear
+    mu, divergence lambda) couple the components.  weight (N, *spatial)
+    weights absolute and membrane (an error with bending or Lame, as
+    there); hessian (N, DD, *spatial), DD in {1, D, D(D+1)/2}."""
+    x = np.asarray(x, np.float64)
+    N, D = x.shape[:2]
+    shape = x.shape[2:]
+    dim = len(shape)
+    vs = _unfold3(voxel_size, 1.0)
+    vx = [1.0 / (v * v) for v in vs]
+    vx = [vx[i] if i < dim else 0.0 for i in range(3)]
+    bnd = [int(v) for v in _unfold3(bound, 0.0)]
+    nb = _Nbr(shape, bnd)
+    lam0, lam1, lam2, mu, lam = float(absolute), float(membrane), float(bending), float(shear), float(div)
+    svx = sum(vx)
+    w1 = [lam2 * (-4.0 * vx[i] * svx) - lam1 * vx[i] for i in range(3)]
+    w2 = [lam2 * vx[i] * vx[i] for i in range(3)]
+    wc2 = 0.25 * mu + 0.25 * lam
+    out = np.zeros_like(x)
+    if weight is not None:
+        if lam2 or mu or lam:
+            raise ValueError("RLS only implemented for absolute/membrane")
+        wg = np.broadcast_to(np.asarray(weight, np.float64).reshape((-1,) + shape), (N,) + shape)
+        for d in range(D):
+            u = x[:, d]
+            acc = lam0 * wg * u
+            if lam1:
+                sm = np.zeros_like(u)
+                for ax in range(dim):
+                    for s in (-1, 1):
+                        o = _step(dim, ax, s)
+                        sm += w1[ax] * (wg + nb.get(wg, o)) * (nb.get(u, o) - u)
+                acc = acc + sm * 0.5
+            out[:, d] = acc / vx[d]
+    else:
+        for d in range(D):
+            u = x[:, d]
+            acc = lam0 * u
+            for ax in range(dim):
+                acc = acc + w1[ax] * (nb.get(u, _step(dim, ax, -1)) - u + nb.get(u, _step(dim, ax, 1)) - u)
+            if lam2:
+                for ax in range(dim):
+                    acc = acc + w2[ax] * (nb.get(u, _step(dim, ax, -2)) - u + nb.get(u, _step(dim, ax, 2)) - u)
+                for i in range(dim):
+                    for j in range(i + 1, dim):
+                        wp = lam2 * 2.0 * vx[i] * vx[j]
+                        for si in (-1, 1):
+                            for sj in (-1, 1):
+                                acc = acc + wp * (nb.get(u, _diag(dim, i, j, si, sj)) - u)
+            res = acc / vx[d]
+            if mu or lam:
+                for ax in range(dim):
+                    lw = (-2.0 * mu - lam) if ax == d else (-mu * vx[ax] / vx[d])
+                    res = res + lw * (nb.get(u, _step(dim, ax, -1)) - u + nb.get(u, _step(dim, ax, 1)) - u)
+                for e in range(D):
+                    if e == d:
+                        continue
+                    for sd in (-1, 1):
+                        for se in (-1, 1):
+                            res = res - wc2 * sd * se * nb.get(x[:, e], _diag(dim, d, e, sd, se))
+            out[:, d] = res
+    if hessian is not None:
+        h = np.asarray(hessian, np.float64)
+        h = np.broadcast_to(h, (N, h.shape[1]) + shape)
+        DD = h.shape[1]
+        if DD == 1:
+            out = out + h[:, :1] * x
+        elif DD == D:
+            out = out + h * x
+        else:
+            k = D
+            hx = h[:, :D] * x
+            for i in range(D):
+                for j in range(i + 1, D):
+                    hx[:, i] += h[:, k] * x[:, j]
+                    hx[:, j] += h[:, k] * x[:, i]
+                    k += 1
+            out = out + hx
+    return out

@@ -27,6 +27,10 @@ Writes
                         gradient) on seeded float64 inputs.
                         (`python tests/golden/make_golden.py spatial` writes
                         this file alone.)
+  regulariser_golden.npz : outputs of the reference's field and grid
+                        regularisers (nitorch/_C/solve.py) on seeded float64
+                        inputs (`python tests/golden/make_golden.py
+                        regulariser`).
 
 Reference defects are handled as in tests/test_oracle_vs_reference.py: the
 grid_grad_backward target is laid out with a last-dimension stride > 1 (D2),
@@ -270,7 +274,89 @@ def multires(ref, S):
     return {k: np.asarray(v) for k, v in out.items()}
 
 
+REG_FIELD = [  # (absolute, membrane, bending, factor)
+    ([0.1], [0.0], [0.0], [1.0]),
+    ([0.1], [1.0, 2.0], [0.0], [1.0, 0.5]),
+    ([0.05], [0.3], [0.7, 0.2], [1.0]),
+    ([0.0], [0.0], [1.0], [2.0]),
+]
+REG_GRID = [  # (absolute, membrane, bending, (shear, div), factor)
+    (0.1, 0.0, 0.0, (0.0, 0.0), 1.0),
+    (0.1, 1.0, 0.0, (0.0, 0.0), 1.0),
+    (0.05, 0.3, 0.7, (0.0, 0.0), 2.0),
+    (0.02, 0.4, 0.0, (0.6, 0.3), 1.0),
+    (0.01, 0.2, 0.5, (0.7, 0.4), 0.5),
+    (0.0, 0.0, 0.0, (1.0, 0.0), 1.0),
+    (0.0, 0.0, 0.0, (0.0, 1.0), 1.0),
+]
+REG_BOUNDS = ["dct2", "dft", "zero", "dst1", ["dct1", "dst2", "replicate"]]
+REG_SHAPES = {1: (13,), 2: (9, 8), 3: (7, 6, 5)}
+REG_VS = [1.3, 0.8, 1.1]
+
+
+def regulariser(S):
+    """The reference's field and grid regularisers through its own wrappers
+    (nitorch/_C/solve.py c_regulariser / c_regulariser_grid), float64, 1-3-D:
+    every penalty mix of REG_FIELD / REG_GRID under every bound of
+    REG_BOUNDS, weighted absolute / membrane, and each Hessian layout.
+    Not generated, as the reference fails there: a call with every penalty
+    zero (the field kernel's `zeros` never advances its channel loop), a 1-D
+    field Hessian (the front-end expands it to 3-D), weighted field inputs
+    with N > 1 (the kernel reads batch item 0's weights for every item) and
+    grid Hessians with N > 1 (offset by the input's batch stride)."""
+    import nitorch._C.solve as CS
+    out = {}
+    g = torch.Generator().manual_seed(123)
+    for dim, shape in REG_SHAPES.items():
+        vs = REG_VS[:dim]
+        x = torch.randn((2, 2) + shape, generator=g, dtype=torch.float64)
+        out[f"f{dim}_x"] = x.numpy()
+        for kb, bnd in enumerate(REG_BOUNDS):
+            bnd = bnd if isinstance(bnd, str) else bnd[:dim]
+            for kp, (a, m, b, f) in enumerate(REG_FIELD):
+                out[f"f{dim}_b{kb}_p{kp}"] = CS.c_regulariser(x, None, None, dim, a, m, b, f, vs, bnd).numpy()
+        for kw, wc in enumerate((1, 2)):
+            w = torch.rand((1, wc) + shape, generator=g, dtype=torch.float64) + 0.5
+            out[f"f{dim}_w{kw}"] = w.numpy()
+            for kp, (a, m) in enumerate((([0.2], [1.0, 0.5]), ([0.3], [0.0]))):
+                out[f"f{dim}_w{kw}_p{kp}"] = CS.c_regulariser(x[:1], w, None, dim, a, m, [0.0], [1.0], vs,
+                                                              "dct2").numpy()
+        if dim > 1:
+            x3 = torch.randn((2, 3) + shape, generator=g, dtype=torch.float64)
+            out[f"f{dim}_x3"] = x3.numpy()
+            for CC in (1, 3, 5, 6):
+                h = torch.rand((2, CC) + shape, generator=g, dtype=torch.float64)
+                out[f"f{dim}_h{CC}"] = h.numpy()
+                out[f"f{dim}_h{CC}_out"] = CS.c_regulariser(x3, None, h, dim, [0.1], [0.5], [0.0], [1.0], vs,
+                                                            "dft").numpy()
+        v = torch.randn((2,) + shape + (dim,), generator=g, dtype=torch.float64)
+        out[f"g{dim}_x"] = v.numpy()
+        for kb, bnd in enumerate(REG_BOUNDS):
+            bnd = bnd if isinstance(bnd, str) else bnd[:dim]
+            for kp, (a, m, b, lame, f) in enumerate(REG_GRID):
+                out[f"g{dim}_b{kb}_p{kp}"] = CS.c_regulariser_grid(v, None, None, a, m, b, lame, f, vs, bnd).numpy()
+        w = torch.rand((2,) + shape, generator=g, dtype=torch.float64) + 0.5
+        out[f"g{dim}_w"] = w.numpy()
+        for kp, (a, m) in enumerate(((0.2, 1.0), (0.3, 0.0))):
+            out[f"g{dim}_w_p{kp}"] = CS.c_regulariser_grid(v, w, None, a, m, 0.0, 0.0, 1.0, vs, "dft").numpy()
+        if dim > 1:
+            for DD in sorted({1, dim, dim * (dim + 1) // 2}):
+                h = torch.rand((1,) + shape + (DD,), generator=g, dtype=torch.float64)
+                out[f"g{dim}_h{DD}"] = h.numpy()
+                out[f"g{dim}_h{DD}_out"] = CS.c_regulariser_grid(v[:1], None, h, 0.1, 0.5, 0.0, 0.0, 1.0, vs,
+                                                                 "dct2").numpy()
+    return {k: np.asarray(v) for k, v in out.items()}
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "regulariser":
+        S = R.load_spatial()
+        if S is None:
+            raise SystemExit("reference tree / compiled backend not found")
+        torch.set_num_threads(1)
+        np.savez_compressed(os.path.join(HERE, "regulariser_golden.npz"), **regulariser(S))
+        print("regulariser_golden.npz", os.path.getsize(os.path.join(HERE, "regulariser_golden.npz")))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "multires":
         S = R.load_spatial()
         ref = R.load_compiled()
