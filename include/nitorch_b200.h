@@ -284,6 +284,36 @@ PP_API int pp_resize_status(uint32_t* status);
 PP_API int pp_fmg_prolongation(const pp_tensor* input, const pp_tensor* out, const pp_options* opt, void* stream);
 PP_API int pp_fmg_restriction(const pp_tensor* input, const pp_tensor* out, const pp_options* opt, void* stream);
 
+/* ---- Regularisers: out = (H + L) x ------------------------------------
+ * nitorch._C.solve.c_regulariser / c_regulariser_grid (nitorch/_C/solve.py:
+ * 21-142; native nitorch/_C/src/regulariser.cpp:19-64, regulariser_grid.cpp;
+ * kernels nitorch/_C/src/impl/regulariser_common.cpp,
+ * regulariser_grid_common.cpp).  L is the matrix of the absolute, membrane
+ * and bending energies (and, for displacement grids, the Lame shear and
+ * divergence energies) with the boundary conditions `bound` per axis and
+ * voxel sizes `voxel_size` per axis (three entries each, unfolded by the
+ * caller: the last given entry repeated); H a voxel-wise Hessian.  float32
+ * or float64; weights, Hessian and output have the input's dtype; the
+ * output must not overlap the inputs.  A weight map scales the absolute and
+ * membrane energies (PP_ERR_UNSUPPORTED with bending or Lame terms). */
+/* Field: input / out (N, C, *spatial), 1-3-D, C <= 64; absolute / membrane /
+ * bending: C entries each (already times the caller's factor); weight
+ * (N, C, *spatial) or NULL (broadcast by strides); hessian (N, CC, *spatial),
+ * CC in {1, C, 2C-1, C(C+1)/2} (identity, diagonal, the (diag, last row)
+ * layout of regulariser_common.cpp:630-648, or the symmetric diagonal-then-
+ * upper-triangle layout), or NULL. */
+PP_API int pp_regulariser(const pp_tensor* input, const pp_tensor* weight, const pp_tensor* hessian,
+                          const pp_tensor* out, const double* absolute, const double* membrane,
+                          const double* bending, const double* voxel_size, const int32_t* bound, void* stream);
+/* Grid: input / out (N, *spatial, D) displacements, components last, D = the
+ * spatial dimension; component d is scaled by voxel_size[d]^2 as in the
+ * reference; weight (N, *spatial) or NULL; hessian (N, *spatial, DD), DD in
+ * {1, D, D(D+1)/2}, or NULL. */
+PP_API int pp_regulariser_grid(const pp_tensor* input, const pp_tensor* weight, const pp_tensor* hessian,
+                               const pp_tensor* out, double absolute, double membrane, double bending,
+                               double shear, double div, const double* voxel_size, const int32_t* bound,
+                               void* stream);
+
 /* ---- Jacobians of transformation / displacement fields ----------------
  * nitorch.spatial.grid_jacobian / grid_jacdet (nitorch/spatial/_grid.py:
  * 917-1013) without `sample`: central finite differences of the

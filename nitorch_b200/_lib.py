@@ -77,6 +77,7 @@ EXPORTS = (
     "pp_affine_grad_workspace_bytes", "pp_affine_grad_matrix", "pp_resize", "pp_resize_status",
     "pp_fmg_prolongation", "pp_fmg_restriction",
     "pp_grid_jacobian", "pp_grid_jacobian_backward", "pp_jacobian_det",
+    "pp_regulariser", "pp_regulariser_grid",
 )
 
 PP_BATCH_PULL, PP_BATCH_PUSH, PP_BATCH_PUSH_BACKWARD = 0, 2, 4
@@ -111,6 +112,10 @@ def _declare(L):
     L.pp_grid_jacobian.argtypes = [T, T, T, i32, DP, i32, i32, vp]
     L.pp_grid_jacobian_backward.argtypes = [T, T, T, T, i32, DP, i32, i32, vp]
     L.pp_jacobian_det.argtypes = [T, T, T, T, vp]
+    IP = ctypes.POINTER(ctypes.c_int32)
+    L.pp_regulariser.argtypes = [T, T, T, T, DP, DP, DP, DP, IP, vp]
+    d = ctypes.c_double
+    L.pp_regulariser_grid.argtypes = [T, T, T, T, d, d, d, d, d, DP, IP, vp]
     L.pp_svf_compose.argtypes = [T, T, O, vp]
     L.pp_svf_compose_backward.argtypes = [T, T, T, O, vp, vp, sz]
     L.pp_svf_workspace_bytes.argtypes = [T, ctypes.c_int32]

@@ -94,6 +94,40 @@ def test_workspace_query():
     assert L.pp_push_workspace_bytes(ctypes.byref(d), 0) == 0
 
 
+def test_regulariser_validation_on_host():
+    """pp_regulariser / pp_regulariser_grid reject bad arguments before any
+    CUDA call."""
+    L = _lib.load()
+    D3 = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    B3 = (ctypes.c_int32 * 3)(2, 2, 2)
+
+    def field(x, out, w=None, h=None, bend=0.0):
+        C = x.shape[1] if x.dim() > 1 else 1
+        a = (ctypes.c_double * max(C, 1))(*([0.1] * max(C, 1)))
+        b = (ctypes.c_double * max(C, 1))(*([bend] * max(C, 1)))
+        return L.pp_regulariser(ctypes.byref(_lib.desc(x)), None if w is None else ctypes.byref(_lib.desc(w)),
+                                None if h is None else ctypes.byref(_lib.desc(h)), ctypes.byref(_lib.desc(out)),
+                                a, a, b, D3, B3, None)
+
+    x = torch.zeros(1, 3, 4, 5, 6)
+    assert field(torch.zeros(3, 4), torch.zeros(3, 4)) == _lib.PP_ERR_ARG  # no spatial dimension
+    assert field(x.bfloat16(), x.bfloat16()) == _lib.PP_ERR_DTYPE  # float32 / float64 only
+    assert field(torch.zeros(1, 65, 2, 2, 2), torch.zeros(1, 65, 2, 2, 2)) == _lib.PP_ERR_UNSUPPORTED
+    assert field(x, torch.zeros(1, 3, 4, 5, 5)) == _lib.PP_ERR_ARG  # output shape
+    assert field(x, x) == _lib.PP_ERR_ARG  # output overlaps the input
+    assert field(x, torch.zeros_like(x), w=torch.ones_like(x), bend=1.0) == _lib.PP_ERR_UNSUPPORTED
+    assert field(x, torch.zeros_like(x), h=torch.zeros(1, 4, 4, 5, 6)) == _lib.PP_ERR_ARG  # CC not 1/3/5/6
+    g = torch.zeros(1, 4, 5, 6, 3)
+
+    def grid(v, out, w=None, shear=0.0):
+        return L.pp_regulariser_grid(ctypes.byref(_lib.desc(v)), None if w is None else ctypes.byref(_lib.desc(w)),
+                                     None, ctypes.byref(_lib.desc(out)), 0.1, 1.0, 0.0, shear, 0.0, D3, B3, None)
+
+    assert grid(torch.zeros(1, 4, 5, 6, 2), torch.zeros(1, 4, 5, 6, 2)) == _lib.PP_ERR_ARG  # D != dim
+    assert grid(g, torch.zeros_like(g), w=torch.ones(1, 4, 5, 6), shear=1.0) == _lib.PP_ERR_UNSUPPORTED
+    assert grid(g, torch.zeros_like(g), w=torch.ones(1, 4, 5, 7)) == _lib.PP_ERR_ARG
+
+
 def test_svf_workspace_query():
     L = _lib.load()
     u = _lib.desc(torch.zeros((1, 4, 5, 6, 3), dtype=torch.float32))
