@@ -697,6 +697,72 @@ def run_resize(args, rank, world, device):
             "max_rel_diff_vs_per_point": diff, "resize_status": affine.resize_status()}
 
 
+def run_regulariser(args, rank, world, device):
+    """The native solvers' regularisers (nitorch._C.solve): the grid
+    regulariser of a 1x192^3x3 float32 displacement field with nitorch's
+    registration penalties (absolute 1e-4, membrane 1e-3, bending 0.2, Lame
+    (0.05, 0.2), dft; every term of the stencil) and the field regulariser
+    of a 1x3x192^3 image (membrane, dct2).  Roofline: the field read once and
+    the output written once (algorithmic bytes).  Beside it, the reference's
+    own CPU regulariser on the same input (one call, all host threads)."""
+    from nitorch_b200 import _lib, solve
+    n = 192
+    g = torch.Generator(device=device).manual_seed(61)
+    v = torch.randn((1, n, n, n, 3), generator=g, device=device)
+    x = torch.randn((1, 3, n, n, n), generator=g, device=device)
+    ov, ox = torch.empty_like(v), torch.empty_like(x)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    pen = dict(absolute=1e-4, membrane=1e-3, bending=0.2, lame=(0.05, 0.2))
+
+    def timeit(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    l0 = _lib.kernel_launches()
+    grid_ms = timeit(lambda: solve.c_regulariser_grid(v, **pen, bound="dft", output=ov), args.steps)
+    field_ms = timeit(lambda: solve.c_regulariser(x, None, None, 3, 0.0, 1.0, 0.0, bound="dct2", output=ox),
+                      args.steps)
+    launches = _lib.kernel_launches() - l0
+    hbm, src = peaks()
+    algo = 2 * v.numel() * 4
+    out = {}
+    for name, ms in (("grid", grid_ms), ("field", field_ms)):
+        achieved = algo / (ms * 1e-3) / 1e9
+        out[name] = {"ms": round(ms, 4), "value": round(n ** 3 / (ms * 1e-3) / 1e9, 3), "unit": "Gvox/s",
+                     "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                                  "frac": round(achieved / hbm, 4), "peak_source": src,
+                                  "algorithmic_bytes_per_launch": algo}}
+    res = {"workload": f"regulariser_grid 1x{n}^3x3 float32 (absolute 1e-4, membrane 1e-3, bending 0.2, "
+                       f"lame (0.05, 0.2), dft); regulariser 1x3x{n}^3 (membrane 1, dct2)",
+           "gpu_launches": launches, **out}
+    if not args.no_cpu_baseline:
+        from oracle import reference as R
+        ref = R.load_compiled()
+        if ref is not None:
+            vc = v.cpu().movedim(-1, 1).contiguous()
+            E = torch.Tensor()
+            dft = ref.BoundType.dft
+            ref.regulariser_grid(vc, E, E, E, 1e-4, 1e-3, 0.2, 0.05, 0.2, [1.0], [dft])  # warm-up
+            t0 = time.perf_counter()
+            r = ref.regulariser_grid(vc, E, E, E, 1e-4, 1e-3, 0.2, 0.05, 0.2, [1.0], [dft])
+            cpu_ms = (time.perf_counter() - t0) * 1e3
+            ours = solve.c_regulariser_grid(v, **pen, bound="dft").cpu().movedim(-1, 1)
+            res["reference_cpu"] = {"ms": round(cpu_ms, 1), "threads": torch.get_num_threads(),
+                                    "kind": "reference", "max_rel_diff": float((ours - r).abs().max() / r.abs().max())}
+    return res
+
+
 def run_all(args, rank, world, device):
     import gc
     if args.only_resize:
@@ -704,6 +770,9 @@ def run_all(args, rank, world, device):
     if args.only_svf:
         r = run_svf(args, rank, world, device)
         return {"svf": r} if rank == 0 else None
+    if args.only_regulariser:
+        r = run_regulariser(args, rank, world, device)
+        return {"regulariser": r} if rank == 0 else None
     line = run_b200(args, rank, world, device)
     gc.collect()
     torch.cuda.empty_cache()
@@ -726,6 +795,12 @@ def run_all(args, rank, world, device):
         r = run_resize(args, rank, world, device)
         if line is not None:
             line["resize"] = r
+    if not args.no_regulariser:
+        gc.collect()
+        torch.cuda.empty_cache()
+        r = run_regulariser(args, rank, world, device)
+        if line is not None:
+            line["regulariser"] = r
     return line
 
 
@@ -921,6 +996,8 @@ def main():
     ap.add_argument("--no-fused", action="store_true", help="skip the fused pull_push leg")
     ap.add_argument("--only-resize", action="store_true", help="run the resize leg alone")
     ap.add_argument("--only-svf", action="store_true", help="run the config-5 leg alone")
+    ap.add_argument("--only-regulariser", action="store_true", help="run the regulariser leg alone")
+    ap.add_argument("--no-regulariser", action="store_true", help="skip the regulariser leg")
     ap.add_argument("--no-resize", action="store_true")
     ap.add_argument("--svf-steps", type=int, default=5)
     ap.add_argument("--traffic", type=float, default=None,
