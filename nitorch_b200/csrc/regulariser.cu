@@ -24,7 +24,10 @@
 // regulariser_grid_common.cpp:265-298); the kernel is compiled per
 // (dimension, stencil radius, weighted, Lame), so every neighbour offset
 // and sign lives in registers.  Differences and their group sums are formed
-// in the storage type and accumulated in float64, in the reference's order.
+// in the storage type as in the reference; the group terms are accumulated
+// in the storage type too (the reference accumulates them in float64, which
+// moves a float32 result by a few ulps at most).  Voxels at least R from
+// every edge take a path without boundary signs.
 // A thread per voxel, the last axis fastest (coalesced rows; the
 // neighbours come from L1 / L2): HBM-bound, each input element read once
 // from DRAM and each output element written once.
@@ -57,7 +60,8 @@ template <class T> struct Coef {
 };
 
 struct RegArgs {
-  int32_t C, hess, CC, pad;
+  int32_t C, hess, CC;
+  int32_t narrow;  // every neighbour offset fits 32 bits: int32 offset arithmetic
   int32_t bound[3];
   int32_t size[3];
   int64_t nvox;
@@ -90,14 +94,15 @@ __device__ __forceinline__ int sym_index(int i, int j, int C) { return C + i * C
 
 // sign * x[off] (sign 0: outside the volume, nothing read) -- bound::get.
 // INNER: every neighbour lies inside the volume (sign 1).
-template <bool INNER, class S>
-__device__ __forceinline__ S nbr(const S* x, int64_t off, int s) {
+template <bool INNER, class S, class I>
+__device__ __forceinline__ S nbr(const S* x, I off, int s) {
   if constexpr (INNER) return x[off];
   else return s == 0 ? S(0) : (s > 0 ? x[off] : -x[off]);
 }
 
-struct Nbrs {
-  int64_t im[3][2], ip[3][2], wm[3], wp[3];
+// I: int32 when every neighbour offset of every tensor fits, else int64.
+template <class I> struct Nbrs {
+  I im[3][2], ip[3][2], wm[3], wp[3];
   int sm[3][2], sp[3][2];
 };
 
@@ -109,8 +114,8 @@ struct Nbrs {
 template <class V>
 __device__ __forceinline__ V sel3(int c, V v0, V v1, V v2) { return c == 0 ? v0 : (c == 1 ? v1 : v2); }
 
-template <class S, int DIM, int R, bool W, bool LAME, bool G, bool INNER>
-__device__ __forceinline__ void voxel(const RegArgs& A, const S* x, S* out, const S* w, int64_t ho, const Nbrs& N) {
+template <class S, class I, int DIM, int R, bool W, bool LAME, bool G, bool INNER>
+__device__ __forceinline__ void voxel(const RegArgs& A, const S* x, S* out, const S* w, int64_t ho, const Nbrs<I>& N) {
   using T = S;
 #pragma unroll 1
   for (int c = 0; c < (G ? DIM : A.C); ++c) {
@@ -151,8 +156,8 @@ __device__ __forceinline__ void voxel(const RegArgs& A, const S* x, S* out, cons
       if constexpr (LAME) {
         // component c against each other component e on the diagonals of
         // (axis c, axis e): + (c+, e-) - (c+, e+) + (c-, e+) - (c-, e-)
-        const int64_t cp = sel3(c, N.ip[0][0], N.ip[DIM > 1 ? 1 : 0][0], N.ip[DIM > 2 ? 2 : 0][0]);
-        const int64_t cm = sel3(c, N.im[0][0], N.im[DIM > 1 ? 1 : 0][0], N.im[DIM > 2 ? 2 : 0][0]);
+        const I cp = sel3(c, N.ip[0][0], N.ip[DIM > 1 ? 1 : 0][0], N.ip[DIM > 2 ? 2 : 0][0]);
+        const I cm = sel3(c, N.im[0][0], N.im[DIM > 1 ? 1 : 0][0], N.im[DIM > 2 ? 2 : 0][0]);
         const int scp = sel3(c, N.sp[0][0], N.sp[DIM > 1 ? 1 : 0][0], N.sp[DIM > 2 ? 2 : 0][0]);
         const int scm = sel3(c, N.sm[0][0], N.sm[DIM > 1 ? 1 : 0][0], N.sm[DIM > 2 ? 2 : 0][0]);
         S s = S(0);
@@ -196,8 +201,15 @@ __device__ __forceinline__ void voxel(const RegArgs& A, const S* x, S* out, cons
 
 // G: displacement grid (C = DIM components, channel loop unrolled so that the
 // Lame terms index the per-axis registers at compile time).
-template <class S, int DIM, int R, bool W, bool LAME, bool G>
-__global__ void __launch_bounds__(256) regulariser_kernel(const __grid_constant__ RegArgs A) {
+// Resident blocks the register budget is set for (radius 1 without weights:
+// at most 64 registers a thread, otherwise 85, float64 radius 2: 128):
+// latency hiding needs the warps more than the registers.
+template <class S, int R, bool W> struct RegBlocks {
+  static constexpr int value = (R == 1 && !W) ? 4 : (sizeof(S) == 8 && R == 2 ? 2 : 3);
+};
+
+template <class S, class I, int DIM, int R, bool W, bool LAME, bool G>
+__global__ void __launch_bounds__(256, RegBlocks<S, R, W>::value) regulariser_kernel(const __grid_constant__ RegArgs A) {
   static_assert(G || !LAME, "Lame terms are for grids");
   const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < A.nvox; i += step) {
@@ -221,19 +233,19 @@ __global__ void __launch_bounds__(256) regulariser_kernel(const __grid_constant_
       n = r;
     }
     // +-1 and +-2 neighbours per axis: element offsets (input, weights) and signs
-    Nbrs N;
+    Nbrs<I> N;
     bool inner = true;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
       if (sub[a] >= R && sub[a] < A.size[a] - R) {  // interior along this axis: plain steps
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-          N.im[a][k] = -(k + 1) * A.is[a];
-          N.ip[a][k] = (k + 1) * A.is[a];
+          N.im[a][k] = static_cast<I>(-(k + 1) * A.is[a]);
+          N.ip[a][k] = static_cast<I>((k + 1) * A.is[a]);
           N.sm[a][k] = N.sp[a][k] = 1;
           if (W && k == 0) {
-            N.wm[a] = -A.ws[a];
-            N.wp[a] = A.ws[a];
+            N.wm[a] = static_cast<I>(-A.ws[a]);
+            N.wp[a] = static_cast<I>(A.ws[a]);
           }
         }
         continue;
@@ -245,13 +257,13 @@ __global__ void __launch_bounds__(256) regulariser_kernel(const __grid_constant_
         const int slo = ppk::bound_sign<int>(A.bound[a], lo, nn), shi = ppk::bound_sign<int>(A.bound[a], hi, nn);
         const int ilo = slo ? ppk::bound_index<int>(A.bound[a], lo, nn) : sub[a];
         const int ihi = shi ? ppk::bound_index<int>(A.bound[a], hi, nn) : sub[a];
-        N.im[a][k] = static_cast<int64_t>(ilo - sub[a]) * A.is[a];
-        N.ip[a][k] = static_cast<int64_t>(ihi - sub[a]) * A.is[a];
+        N.im[a][k] = static_cast<I>(static_cast<int64_t>(ilo - sub[a]) * A.is[a]);
+        N.ip[a][k] = static_cast<I>(static_cast<int64_t>(ihi - sub[a]) * A.is[a]);
         N.sm[a][k] = slo;
         N.sp[a][k] = shi;
         if (W && k == 0) {
-          N.wm[a] = static_cast<int64_t>(ilo - sub[a]) * A.ws[a];
-          N.wp[a] = static_cast<int64_t>(ihi - sub[a]) * A.ws[a];
+          N.wm[a] = static_cast<I>(static_cast<int64_t>(ilo - sub[a]) * A.ws[a]);
+          N.wp[a] = static_cast<I>(static_cast<int64_t>(ihi - sub[a]) * A.ws[a]);
         }
       }
     }
@@ -267,9 +279,9 @@ __global__ void __launch_bounds__(256) regulariser_kernel(const __grid_constant_
     S* out = static_cast<S*>(A.out) + oo;
     const S* w = W ? static_cast<const S*>(A.wgt) + wo : nullptr;
     if (inner)
-      voxel<S, DIM, R, W, LAME, G, true>(A, x, out, w, ho, N);
+      voxel<S, I, DIM, R, W, LAME, G, true>(A, x, out, w, ho, N);
     else
-      voxel<S, DIM, R, W, LAME, G, false>(A, x, out, w, ho, N);
+      voxel<S, I, DIM, R, W, LAME, G, false>(A, x, out, w, ho, N);
   }
 }
 
@@ -308,7 +320,10 @@ template <class S, int DIM, int R, bool W, bool LAME, bool G>
 void launch_one(const RegArgs& A, cudaStream_t st) {
   const int64_t want = (A.nvox + 255) / 256;
   const unsigned nb = static_cast<unsigned>(want < 148 * 32 ? want : 148 * 32);
-  regulariser_kernel<S, DIM, R, W, LAME, G><<<nb, 256, 0, st>>>(A);
+  if (A.narrow)
+    regulariser_kernel<S, int32_t, DIM, R, W, LAME, G><<<nb, 256, 0, st>>>(A);
+  else
+    regulariser_kernel<S, int64_t, DIM, R, W, LAME, G><<<nb, 256, 0, st>>>(A);
 }
 
 template <class S, int DIM>
@@ -323,7 +338,10 @@ void launch_dim(const RegArgs& A, bool grid, int R, bool W, bool lame, cudaStrea
   return launch_one<S, DIM, 1, false, false, false>(A, st);
 }
 
-int launch(const RegArgs& A, int dtype, int dim, bool grid, int R, bool W, bool lame, cudaStream_t st) {
+// Neighbour offsets (at most two steps along each axis) of a tensor fit 32 bits.
+bool narrow_ok(const pp_tensor* t) { return !t || 4 * ppc::max_offset(t, 1) < (int64_t(1) << 31); }
+
+int launch(RegArgs& A, int dtype, int dim, bool grid, int R, bool W, bool lame, cudaStream_t st) {
   if (A.nvox == 0) return PP_OK;
   if (dtype == PP_FLOAT32) {
     if (dim == 1) launch_dim<float, 1>(A, grid, R, W, lame, st);
@@ -442,6 +460,7 @@ int pp_regulariser(const pp_tensor* input, const pp_tensor* weight, const pp_ten
     }
   }
   float_coefs(A, C);
+  A.narrow = narrow_ok(input) && narrow_ok(weight);
   return launch(A, input->dtype, dim, false, has_b ? 2 : 1, weight != nullptr, false,
                 static_cast<cudaStream_t>(stream));
 }
@@ -525,6 +544,7 @@ int pp_regulariser_grid(const pp_tensor* input, const pp_tensor* weight, const p
     }
   }
   float_coefs(A, D);
+  A.narrow = narrow_ok(input) && narrow_ok(weight);
   return launch(A, input->dtype, D, true, lam2 != 0.0 ? 2 : 1, weight != nullptr, A.w2 != 0.0,
                 static_cast<cudaStream_t>(stream));
 }
