@@ -894,6 +894,11 @@ int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_options
   k.a.out = out->data;
   field_as_image(out, k.D, k.a.out_sN, k.a.out_sC, k.a.out_s);
   k.a.flags = ppk::F_IDGRID | ppk::F_ADDSELF;
+  if (k.D == 3 && iso_order(k.D, k.order) == 1 && ppk::lanes_enabled()) {
+    // 3-D linear float32: the dedicated composition kernel (svf_compose.cu)
+    rc = svf_compose_linear3(disp, out, k.a.bound, k.a.extrapolate, static_cast<cudaStream_t>(stream));
+    if (rc != PP_ERR_UNSUPPORTED) return rc;
+  }
   return run(k, ppk::K_PULL, need_wide(k, {disp, out}), static_cast<cudaStream_t>(stream));
 }
 

@@ -168,6 +168,10 @@ bool fits32(int64_t v);
 // (contiguous in out's logical order, scale from *mx times bound) -> out,
 // plus `self` (accumulation-type values laid out like acc) where given.
 int det_absmax_of(const pp_tensor* t, unsigned int* out, cudaStream_t st);
+// The 3-D linear float32 displacement self-composition (svf_compose.cu), or
+// PP_ERR_UNSUPPORTED (nothing launched) for any other field.
+int svf_compose_linear3(const pp_tensor* disp, const pp_tensor* out, const int32_t bound[3], int32_t extrapolate,
+                        cudaStream_t st);
 int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const unsigned int* mx, double bound,
                     cudaStream_t st, const void* self = nullptr);
 

@@ -54,6 +54,22 @@ def test_compose_float32_and_channel_strides():
     assert relerr(svf.compose(uc).double().cpu().numpy(), ref) < 1e-5
 
 
+@pytest.mark.parametrize("bound", list(BOUNDS))
+def test_compose_float32_linear_kernel(bound):
+    """3-D linear float32 self-composition on its dedicated kernel
+    (svf_compose_lin3): every bound, with and without extrapolation, on a
+    field large enough to leave the volume, and a components-first view."""
+    from nitorch_b200 import _lib
+    u = _vel((23, 21, 19), seed=31, scale=3.0)
+    for ex in (True, False):
+        ref = O.svf_compose(u.cpu().numpy(), BOUNDS[bound], 1, int(ex))
+        out = svf.compose(u.float(), 1, bound, ex)
+        assert _lib.last_kernel().startswith("svf_compose_lin3")
+        assert relerr(out.double().cpu().numpy(), ref) < 1e-5, ex
+        uc = u.float().movedim(-1, 1).contiguous().movedim(1, -1)
+        assert relerr(svf.compose(uc, 1, bound, ex).double().cpu().numpy(), ref) < 1e-5, ex
+
+
 @pytest.mark.parametrize("order", [1, 3])
 @pytest.mark.parametrize("bound", ["dft", "dct2"])
 def test_compose_backward_float32_paths(order, bound):
