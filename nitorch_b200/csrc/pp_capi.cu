@@ -1000,7 +1000,10 @@ int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const 
     k.a.out_s[1] = disp->sizes[3] * 4;
     k.a.out_s[0] = disp->sizes[2] * disp->sizes[3] * 4;
     k.a.flags |= ppk::F_VEC;
-    if ((rc = run(k, ppk::K_PUSHGRAD, wide, st))) return rc;
+    // 3-D linear: the dedicated kernel (svf_compose.cu), else the lane-split one
+    rc = iso == 1 ? svf_compose_backward_linear3(grad, disp, acc, k.a.bound, k.a.extrapolate, st) : PP_ERR_UNSUPPORTED;
+    if (rc == PP_ERR_UNSUPPORTED) rc = run(k, ppk::K_PUSHGRAD, wide, st);
+    if (rc) return rc;
     return store_field_from4(acc, grad_disp, st);
   }
   if ((rc = zero_fill(grad_disp, st))) return rc;

@@ -172,6 +172,10 @@ int det_absmax_of(const pp_tensor* t, unsigned int* out, cudaStream_t st);
 // PP_ERR_UNSUPPORTED (nothing launched) for any other field.
 int svf_compose_linear3(const pp_tensor* disp, const pp_tensor* out, const int32_t bound[3], int32_t extrapolate,
                         cudaStream_t st);
+// Its backward into a zeroed four-slot channel-interleaved accumulator, or
+// PP_ERR_UNSUPPORTED (nothing launched).
+int svf_compose_backward_linear3(const pp_tensor* grad, const pp_tensor* disp, float* acc, const int32_t bound[3],
+                                 int32_t extrapolate, cudaStream_t st);
 int det_finalize_to(const unsigned long long* acc, const pp_tensor* out, const unsigned int* mx, double bound,
                     cudaStream_t st, const void* self = nullptr);
 

@@ -68,6 +68,14 @@ def test_compose_float32_linear_kernel(bound):
         assert relerr(out.double().cpu().numpy(), ref) < 1e-5, ex
         uc = u.float().movedim(-1, 1).contiguous().movedim(1, -1)
         assert relerr(svf.compose(uc, 1, bound, ex).double().cpu().numpy(), ref) < 1e-5, ex
+        # the backward: the push with neighbouring lanes' corners merged
+        g = _vel((23, 21, 19), seed=32, scale=1.0)
+        gref = O.svf_compose_backward(g.cpu().numpy(), u.cpu().numpy(), BOUNDS[bound], 1, int(ex))
+        gd = svf.compose_backward(g.float(), u.float(), 1, bound, ex)
+        assert _lib.last_kernel().startswith("svf_compose_backward_lin3")
+        assert relerr(gd.double().cpu().numpy(), gref) < 1e-5, ex
+        gd = svf.compose_backward(g.float(), uc, 1, bound, ex)
+        assert relerr(gd.double().cpu().numpy(), gref) < 1e-5, ex
 
 
 @pytest.mark.parametrize("order", [1, 3])
