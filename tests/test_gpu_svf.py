@@ -78,6 +78,25 @@ def test_compose_float32_linear_kernel(bound):
         assert relerr(gd.double().cpu().numpy(), gref) < 1e-5, ex
 
 
+def test_compose_linear_kernels_batch_of_two():
+    """Two batch items in one call (the backward's corner merge never crosses
+    an item: a warp holds the last voxels of item 0 and the first of item 1
+    when Z does not divide 32), with a gradient given as a strided view."""
+    from nitorch_b200 import _lib
+    shape = (13, 11, 7)
+    u = torch.cat([_vel(shape, seed=41, scale=2.5), _vel(shape, seed=42, scale=2.5)])
+    g = torch.cat([_vel(shape, seed=43, scale=1.0), _vel(shape, seed=44, scale=1.0)])
+    gs = g.float().movedim(-1, 1).contiguous().movedim(1, -1)
+    for ex in (True, False):
+        out = svf.compose(u.float(), 1, "dft", ex)
+        gd = svf.compose_backward(gs, u.float(), 1, "dft", ex)
+        assert _lib.last_kernel().startswith("svf_compose_backward_lin3")
+        for n in range(2):
+            un, gn = u[n:n + 1].cpu().numpy(), g[n:n + 1].cpu().numpy()
+            assert relerr(out[n:n + 1].double().cpu().numpy(), O.svf_compose(un, 5, 1, int(ex))) < 1e-5
+            assert relerr(gd[n:n + 1].double().cpu().numpy(), O.svf_compose_backward(gn, un, 5, 1, int(ex))) < 1e-5
+
+
 @pytest.mark.parametrize("order", [1, 3])
 @pytest.mark.parametrize("bound", ["dft", "dct2"])
 def test_compose_backward_float32_paths(order, bound):
