@@ -31,7 +31,7 @@ struct ComposeArgs {
   float* out;
 };
 
-__global__ void __launch_bounds__(256, 4) svf_compose_lin3(const ComposeArgs A) {
+__global__ void __launch_bounds__(256, 5) svf_compose_lin3(const ComposeArgs A) {
   const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < A.nvox; i += step) {
     int sub[3];
@@ -128,7 +128,7 @@ struct ComposeBwdArgs {
   float* acc;
 };
 
-__global__ void __launch_bounds__(256, 4) svf_compose_backward_lin3(const ComposeBwdArgs A) {
+__global__ void __launch_bounds__(256, 5) svf_compose_backward_lin3(const ComposeBwdArgs A) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const bool live = i < A.nvox;
