@@ -222,7 +222,9 @@ PP_API int pp_svf_compose(const pp_tensor* disp, const pp_tensor* out, const pp_
  *    four-slot channel-interleaved accumulator with one vector reduction
  *    per tap and is copied to grad_disp afterwards; with NULL / too small a
  *    workspace (or other fields), one reduction per component and tap
- *    straight into grad_disp. */
+ *    straight into grad_disp.  grad_disp may be the first three slots of
+ *    the workspace itself (data = workspace, strides (V*4, Y*Z*4, Z*4, 4,
+ *    1)): the result is then left there, with no copy. */
 PP_API size_t pp_svf_workspace_bytes(const pp_tensor* disp, int32_t flags);
 PP_API int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp,
                                    const pp_tensor* grad_disp, const pp_options* opt, void* stream,

@@ -1004,7 +1004,13 @@ int pp_svf_compose_backward(const pp_tensor* grad, const pp_tensor* disp, const 
     rc = iso == 1 ? svf_compose_backward_linear3(grad, disp, acc, k.a.bound, k.a.extrapolate, st) : PP_ERR_UNSUPPORTED;
     if (rc == PP_ERR_UNSUPPORTED) rc = run(k, ppk::K_PUSHGRAD, wide, st);
     if (rc) return rc;
-    return store_field_from4(acc, grad_disp, st);
+    // grad_disp given as the first three slots of the workspace itself: done
+    bool in_place = grad_disp->data == workspace;
+    {
+      const int64_t want[5] = {V * 4, disp->sizes[2] * disp->sizes[3] * 4, disp->sizes[3] * 4, 4, 1};
+      for (int i = 0; i < 5 && in_place; ++i) in_place = grad_disp->sizes[i] == 1 || grad_disp->strides[i] == want[i];
+    }
+    return in_place ? PP_OK : store_field_from4(acc, grad_disp, st);
   }
   if ((rc = zero_fill(grad_disp, st))) return rc;
   return run(k, ppk::K_PUSHGRAD, wide, st);

@@ -63,7 +63,6 @@ def compose_backward(grad, disp, interpolation="linear", bound="dft", extrapolat
     L = _lib.load()
     u, unbatched = _batched(disp)
     g = grad.reshape(u.shape)
-    out = torch.empty(u.shape, dtype=u.dtype, device=u.device)
     det = get_deterministic() if deterministic is None else bool(deterministic)
     flags = _lib.PP_DETERMINISTIC if det else 0
     opt = _options(interpolation, bound, extrapolate, flags)
@@ -72,6 +71,11 @@ def compose_backward(grad, disp, interpolation="linear", bound="dft", extrapolat
     # the vector-reduction accumulator, or the fixed-point accumulator and the
     # per-voxel terms of the deterministic mode
     ws = torch.empty(nws, dtype=torch.uint8, device=u.device) if nws else None
+    if ws is not None and not det:
+        # the result is the accumulator's first three slots (no copy)
+        out = ws[:u.numel() // 3 * 16].view(torch.float32).view(*u.shape[:-1], 4)[..., :3]
+    else:
+        out = torch.empty(u.shape, dtype=u.dtype, device=u.device)
     with _On(u):
         _lib.check(L.pp_svf_compose_backward(ctypes.byref(_lib.desc(g)), ctypes.byref(du),
                                              ctypes.byref(_lib.desc(out)), ctypes.byref(opt), _lib.stream_of(u),
