@@ -31,7 +31,21 @@ struct ComposeArgs {
   float* out;
 };
 
-__global__ void __launch_bounds__(256, 5) svf_compose_lin3(const ComposeArgs A) {
+// UV4 / OV4: the field / the output is the first three slots of a four-slot
+// buffer (strides (., 4YZ, 4Z, 4, 1), 16-byte aligned): one 16-byte access
+// per voxel or corner instead of three.
+template <bool UV4>
+__device__ __forceinline__ void load3(const float* p, int fC, float (&v)[3]) {
+  if constexpr (UV4) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z;
+  } else {
+    v[0] = __ldg(p); v[1] = __ldg(p + fC); v[2] = __ldg(p + 2 * fC);
+  }
+}
+
+template <bool UV4, bool OV4>
+__global__ void __launch_bounds__(256, UV4 ? 4 : 5) svf_compose_lin3(const ComposeArgs A) {
   const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < A.nvox; i += step) {
     int sub[3];
@@ -46,62 +60,69 @@ __global__ void __launch_bounds__(256, 5) svf_compose_lin3(const ComposeArgs A) 
     const float* un = A.u + n * A.fN;
     const int base = sub[0] * A.fs[0] + sub[1] * A.fs[1] + sub[2] * A.fs[2];
     float self[3], x[3];
+    load3<UV4>(un + base, A.fC, self);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      self[d] = __ldg(un + base + d * A.fC);
-      x[d] = static_cast<float>(sub[d]) + self[d];
-    }
+    for (int d = 0; d < 3; ++d) x[d] = static_cast<float>(sub[d]) + self[d];
     float* o = A.out + n * A.oN + sub[0] * A.os[0] + sub[1] * A.os[1] + sub[2] * A.os[2];
     const float tol = (A.extrapolate & 2) ? 0.55f : 0.05f;
     bool inb = true;
 #pragma unroll
     for (int d = 0; d < 3; ++d) inb = inb && ppk::in_fov<float>(x[d], A.size[d], tol);
+    float res[3];
     if (!((A.extrapolate & 1) || inb)) {  // outside the field of view: the identity term alone
 #pragma unroll
-      for (int d = 0; d < 3; ++d) o[d * A.oC] = self[d];
-      continue;
-    }
-    // per axis: the two nodes' offsets and weights (boundary sign folded in)
-    int off[3][2];
-    float w[3][2];
+      for (int d = 0; d < 3; ++d) res[d] = self[d];
+    } else {
+      // per axis: the two nodes' offsets and weights (boundary sign folded in)
+      int off[3][2];
+      float w[3][2];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float xc = fminf(fmaxf(x[d], -1073741824.f), 1073741824.f);
-      const float f = floorf(xc);
-      const int i0 = static_cast<int>(f);
-      const float t = xc - f;
-      const int nn = A.size[d];
-      if (i0 >= 0 && i0 + 1 < nn) {
-        off[d][0] = i0 * A.fs[d];
-        off[d][1] = off[d][0] + A.fs[d];
-        w[d][0] = 1.f - t;
-        w[d][1] = t;
-      } else {
+      for (int d = 0; d < 3; ++d) {
+        const float xc = fminf(fmaxf(x[d], -1073741824.f), 1073741824.f);
+        const float f = floorf(xc);
+        const int i0 = static_cast<int>(f);
+        const float t = xc - f;
+        const int nn = A.size[d];
+        if (i0 >= 0 && i0 + 1 < nn) {
+          off[d][0] = i0 * A.fs[d];
+          off[d][1] = off[d][0] + A.fs[d];
+          w[d][0] = 1.f - t;
+          w[d][1] = t;
+        } else {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int s = ppk::bound_sign<int>(A.bound[d], i0 + k, nn);
-          const int idx = s ? ppk::bound_index<int>(A.bound[d], i0 + k, nn) : 0;
-          off[d][k] = idx * A.fs[d];
-          w[d][k] = static_cast<float>(s) * (k ? t : 1.f - t);
+          for (int k = 0; k < 2; ++k) {
+            const int s = ppk::bound_sign<int>(A.bound[d], i0 + k, nn);
+            const int idx = s ? ppk::bound_index<int>(A.bound[d], i0 + k, nn) : 0;
+            off[d][k] = idx * A.fs[d];
+            w[d][k] = static_cast<float>(s) * (k ? t : 1.f - t);
+          }
         }
       }
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float* uc = un + c * A.fC;
-      float acc = 0.f;
+      // separable partial sums, x innermost, the three components together
+      float acc[3] = {0.f, 0.f, 0.f};
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
-        float accy = 0.f;
+        float accy[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
           const int oyz = off[1][j] + off[2][k];
-          const float accx = fmaf(w[0][1], __ldg(uc + off[0][1] + oyz), w[0][0] * __ldg(uc + off[0][0] + oyz));
-          accy = fmaf(w[1][j], accx, accy);
+          float c0[3], c1[3];
+          load3<UV4>(un + off[0][0] + oyz, A.fC, c0);
+          load3<UV4>(un + off[0][1] + oyz, A.fC, c1);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) accy[c] = fmaf(w[1][j], fmaf(w[0][1], c1[c], w[0][0] * c0[c]), accy[c]);
         }
-        acc = fmaf(w[2][k], accy, acc);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] = fmaf(w[2][k], accy[c], acc[c]);
       }
-      o[c * A.oC] = acc + self[c];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) res[c] = acc[c] + self[c];
+    }
+    if constexpr (OV4) {
+      *reinterpret_cast<float4*>(o) = make_float4(res[0], res[1], res[2], 0.f);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o[c * A.oC] = res[c];
     }
   }
 }
@@ -128,6 +149,7 @@ struct ComposeBwdArgs {
   float* acc;
 };
 
+template <bool UV4>
 __global__ void __launch_bounds__(256, 5) svf_compose_backward_lin3(const ComposeBwdArgs A) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -147,9 +169,11 @@ __global__ void __launch_bounds__(256, 5) svf_compose_backward_lin3(const Compos
   if (live) {
     const int fb = sub[0] * A.fs[0] + sub[1] * A.fs[1] + sub[2] * A.fs[2];
     const float* gp = A.g + n * A.gN + sub[0] * A.gs[0] + sub[1] * A.gs[1] + sub[2] * A.gs[2];
+    float uu[3];
+    load3<UV4>(un + fb, A.fC, uu);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      x[d] = static_cast<float>(sub[d]) + __ldg(un + fb + d * A.fC);
+      x[d] = static_cast<float>(sub[d]) + uu[d];
       gv[d] = __ldg(gp + d * A.gC);
     }
     const float tol = (A.extrapolate & 2) ? 0.55f : 0.05f;
@@ -196,8 +220,9 @@ __global__ void __launch_bounds__(256, 5) svf_compose_backward_lin3(const Compos
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           if (ao[0][q] < 0 || ao[1][j] < 0 || ao[2][k] < 0) continue;  // a node outside: no tap
-          const float* up = un + fo[0][q] + fo[1][j] + fo[2][k];
-          const float dot = gv[0] * __ldg(up) + gv[1] * __ldg(up + A.fC) + gv[2] * __ldg(up + 2 * A.fC);
+          float cu[3];
+          load3<UV4>(un + fo[0][q] + fo[1][j] + fo[2][k], A.fC, cu);
+          const float dot = gv[0] * cu[0] + gv[1] * cu[1] + gv[2] * cu[2];
           sx = fmaf(w[0][q], dot, sx);
           dx = fmaf(dw[0][q], dot, dx);
         }
@@ -249,6 +274,16 @@ __global__ void __launch_bounds__(256, 5) svf_compose_backward_lin3(const Compos
 
 bool fits_int(int64_t v) { return v < (int64_t(1) << 31) - 1; }
 
+// The first three slots of a 16-byte aligned four-slot (N, X, Y, Z, 4) buffer.
+bool padded4(const pp_tensor* t) {
+  if (t->ndim != 5 || t->sizes[4] != 3 || reinterpret_cast<uintptr_t>(t->data) % 16 != 0) return false;
+  const int64_t want[5] = {t->strides[0], t->sizes[2] * t->sizes[3] * 4, t->sizes[3] * 4, 4, 1};
+  if (t->strides[0] % 4 != 0) return false;
+  for (int i = 1; i < 5; ++i)
+    if (t->sizes[i] > 1 && t->strides[i] != want[i]) return false;
+  return true;
+}
+
 }  // namespace
 
 namespace ppc {
@@ -283,7 +318,11 @@ int svf_compose_linear3(const pp_tensor* disp, const pp_tensor* out, const int32
   const int64_t want = (A.nvox + 255) / 256;
   const unsigned nb = static_cast<unsigned>(want < 148 * 32 ? want : 148 * 32);
   ppk::note_kernel("svf_compose_lin3", ppk::K_PULL, 1, 3);
-  svf_compose_lin3<<<nb, 256, 0, st>>>(A);
+  const bool uv4 = padded4(disp), ov4 = padded4(out);
+  if (uv4 && ov4) svf_compose_lin3<true, true><<<nb, 256, 0, st>>>(A);
+  else if (uv4) svf_compose_lin3<true, false><<<nb, 256, 0, st>>>(A);
+  else if (ov4) svf_compose_lin3<false, true><<<nb, 256, 0, st>>>(A);
+  else svf_compose_lin3<false, false><<<nb, 256, 0, st>>>(A);
   count_launch();
   return cuda_check(cudaGetLastError(), "svf compose launch");
 }
@@ -324,7 +363,10 @@ int svf_compose_backward_linear3(const pp_tensor* grad, const pp_tensor* disp, f
   const int64_t nb = (A.nvox + 255) / 256;  // a thread per voxel: whole warps of consecutive voxels
   if (nb > 0x7fffffffLL) return PP_ERR_UNSUPPORTED;
   ppk::note_kernel("svf_compose_backward_lin3", ppk::K_PUSHGRAD, 1, 3);
-  svf_compose_backward_lin3<<<static_cast<unsigned>(nb), 256, 0, st>>>(A);
+  if (padded4(disp))
+    svf_compose_backward_lin3<true><<<static_cast<unsigned>(nb), 256, 0, st>>>(A);
+  else
+    svf_compose_backward_lin3<false><<<static_cast<unsigned>(nb), 256, 0, st>>>(A);
   count_launch();
   return cuda_check(cudaGetLastError(), "svf compose backward launch");
 }

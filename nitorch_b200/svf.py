@@ -42,12 +42,21 @@ def _batched(field):
     return field.reshape(-1, *field.shape[-dim - 1:]), False
 
 
+def _field_like(u):
+    """An empty field shaped like u ([batch], *spatial, dim).  3-D float32
+    fields are the first three slots of a four-slot buffer: 16-byte voxels,
+    one load or store each in the composition kernels."""
+    if u.dtype == torch.float32 and u.shape[-1] == 3 and u.dim() in (4, 5):
+        return torch.empty(*u.shape[:-1], 4, dtype=u.dtype, device=u.device)[..., :3]
+    return torch.empty(u.shape, dtype=u.dtype, device=u.device)
+
+
 def compose(disp, interpolation="linear", bound="dft", extrapolate=True):
     """u + pull(u, id + u) for a displacement field u ([batch], *spatial, dim)."""
     _require_cuda(disp)
     L = _lib.load()
     u, unbatched = _batched(disp)
-    out = torch.empty(u.shape, dtype=u.dtype, device=u.device)
+    out = _field_like(u)
     opt = _options(interpolation, bound, extrapolate)
     with _On(u):
         _lib.check(L.pp_svf_compose(ctypes.byref(_lib.desc(u)), ctypes.byref(_lib.desc(out)), ctypes.byref(opt),
@@ -93,6 +102,8 @@ class _Exp(torch.autograd.Function):
     @staticmethod
     def forward(ctx, vel, inverse, steps, interpolation, bound, displacement):
         u = (-vel if inverse else vel) / (2 ** steps)
+        if steps:
+            u = _field_like(u).copy_(u)  # the compositions' layout
         states = []
         for _ in range(steps):
             states.append(u)

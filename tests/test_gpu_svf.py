@@ -76,6 +76,12 @@ def test_compose_float32_linear_kernel(bound):
         assert relerr(gd.double().cpu().numpy(), gref) < 1e-5, ex
         gd = svf.compose_backward(g.float(), uc, 1, bound, ex)
         assert relerr(gd.double().cpu().numpy(), gref) < 1e-5, ex
+        # a field held as the first three slots of a four-slot buffer (16-byte loads)
+        up = svf._field_like(u.float()).copy_(u.float())
+        assert up.stride()[-2] == 4
+        assert relerr(svf.compose(up, 1, bound, ex).double().cpu().numpy(), ref) < 1e-5, ex
+        gd = svf.compose_backward(g.float(), up, 1, bound, ex)
+        assert relerr(gd.double().cpu().numpy(), gref) < 1e-5, ex
 
 
 def test_compose_linear_kernels_batch_of_two():
