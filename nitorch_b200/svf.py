@@ -92,18 +92,32 @@ def compose_backward(grad, disp, interpolation="linear", bound="dft", extrapolat
     return out[0] if unbatched else out.reshape(disp.shape)
 
 
+_IDENTITY = {}
+
+
 def _identity(shape, dtype, device):
-    mesh = torch.meshgrid(*[torch.arange(s, dtype=dtype, device=device) for s in shape], indexing="ij")
-    return torch.stack(mesh, dim=-1)
+    """The identity grid (*shape, dim), built once per (shape, dtype, device)
+    and kept (read only) for later calls."""
+    key = (tuple(shape), dtype, str(device))
+    ident = _IDENTITY.get(key)
+    if ident is None:
+        mesh = torch.meshgrid(*[torch.arange(s, dtype=dtype, device=device) for s in shape], indexing="ij")
+        ident = torch.stack(mesh, dim=-1)
+        if len(_IDENTITY) >= 8:
+            _IDENTITY.clear()
+        _IDENTITY[key] = ident
+    return ident
 
 
 class _Exp(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, vel, inverse, steps, interpolation, bound, displacement):
-        u = (-vel if inverse else vel) / (2 ** steps)
+        scale = (-1.0 if inverse else 1.0) / (2 ** steps)
         if steps:
-            u = _field_like(u).copy_(u)  # the compositions' layout
+            u = torch.mul(vel, scale, out=_field_like(vel))  # in the compositions' layout
+        else:
+            u = vel * scale
         states = []
         for _ in range(steps):
             states.append(u)
