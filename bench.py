@@ -634,11 +634,47 @@ def run_svf(args, rank, world, device):
         iteration()
     torch.cuda.synchronize()
     total_ms, launches, _ = timed_steps(iteration, args, world, device, flush, steps=args.svf_steps)
+
+    # the two kernels of every squaring, alone on a field of this size in the
+    # iteration's layout: composition (field in, field out: 2 x 12 B per voxel
+    # algorithmic) and its backward (field and gradient in, accumulator out:
+    # 12 + 12 + 16 B per voxel)
+    def kernel_ms(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    from nitorch_b200 import _lib
+    u = torch.mul(v, 1.0 / 256, out=svf._field_like(v))
+    g = torch.randn_like(v)
+    fwd_ms = kernel_ms(lambda: svf.compose(u))
+    fwd_kernel = _lib.last_kernel()
+    bwd_ms = kernel_ms(lambda: svf.compose_backward(g, u))
+    bwd_kernel = _lib.last_kernel()
+    hbm, src = peaks()
+    kernels = {}
+    for name, ms, per_vox, kern in (("compose", fwd_ms, 24, fwd_kernel), ("compose_backward", bwd_ms, 40, bwd_kernel)):
+        algo = per_vox * nvox
+        achieved = algo / (ms * 1e-3) / 1e9
+        kernels[name] = {"kernel": kern, "ms": round(ms, 4),
+                         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                                      "frac": round(achieved / hbm, 4), "peak_source": src,
+                                      "algorithmic_bytes_per_launch": algo}}
     return {"workload": "cfg5: exp(v) by 8 squarings (linear, dft) -> pull moving (cubic, dct2) -> MSE -> "
                         "backward -> step; 1x160x192x160",
             "ms_per_iteration": round(total_ms / args.svf_steps, 3),
             "value": round(world * nvox * args.svf_steps / (total_ms * 1e-3) / 1e9, 4), "unit": "Gvox/s",
-            "gpu_launches_per_iteration": round(launches / args.svf_steps, 1)}
+            "gpu_launches_per_iteration": round(launches / args.svf_steps, 1), "kernels": kernels}
 
 
 # ---------------------------------------------------------------------- #
