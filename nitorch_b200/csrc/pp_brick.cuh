@@ -90,7 +90,11 @@ template <int CP> struct BrickGatherSmem {
   static constexpr size_t bytes = size_t(GatherWin::NV) * CP * 4;
 };
 // Resident CTAs per SM the gather kernels are built for (register caps).
-template <int MODE> struct GatherBlocks { static constexpr int value = MODE == K_PULL ? 6 : 4; };
+// (single-channel grid gradients: five, 96 registers without spills; more
+// channels spill there and keep four)
+template <int MODE, int CB> struct GatherBlocks {
+  static constexpr int value = MODE == K_PULL ? 6 : (CB == 1 ? 5 : 4);
+};
 
 template <int CP> __device__ __forceinline__ void vload(const float* p, float (&v)[CP]) {
   if constexpr (CP == 4) { const float4 q = *reinterpret_cast<const float4*>(p); v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w; }
@@ -516,7 +520,7 @@ __global__ void __launch_bounds__(32 * BRK_SCATTER_WARPS) pp_brick_scatter_kerne
 //               t the incoming gradient at the point
 // ===========================================================================
 template <int MODE, int CB, int CP, class S>
-__global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE>::value)
+__global__ void __launch_bounds__(BRK_GATHER_THREADS, GatherBlocks<MODE, CB>::value)
     pp_brick_gather_kernel(const PPArgs a) {
   using G = GatherWin;
   static_assert(MODE == K_PULL || MODE == K_PUSHGRAD, "gather modes");
