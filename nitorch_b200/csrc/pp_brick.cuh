@@ -90,10 +90,11 @@ template <int CP> struct BrickGatherSmem {
   static constexpr size_t bytes = size_t(GatherWin::NV) * CP * 4;
 };
 // Resident CTAs per SM the gather kernels are built for (register caps).
-// (single-channel grid gradients: five, 96 registers without spills; more
-// channels spill there and keep four)
+// (single-channel pulls: eight, 64 registers; single-channel grid
+// gradients: five, 96 registers; both without spills, where more channels
+// spill and keep six and four)
 template <int MODE, int CB> struct GatherBlocks {
-  static constexpr int value = MODE == K_PULL ? 6 : (CB == 1 ? 5 : 4);
+  static constexpr int value = MODE == K_PULL ? (CB == 1 ? 8 : 6) : (CB == 1 ? 5 : 4);
 };
 
 template <int CP> __device__ __forceinline__ void vload(const float* p, float (&v)[CP]) {
