@@ -464,8 +464,10 @@ __device__ __forceinline__ void load_target(const PPArgs& a, const BrickPoint& q
 // the per-point fallback body (= C for C <= 4); CP: channel slots per window
 // voxel (1 for C = 1, 2 for C = 2, 4 for C = 3-4).
 // ===========================================================================
+// Six CTAs per SM (at most 85 registers; no spills): the shared-memory
+// budget of 3-channel windows holds six.
 template <int MODE, int CB, int CP, class S>
-__global__ void __launch_bounds__(32 * BRK_SCATTER_WARPS) pp_brick_scatter_kernel(const PPArgs a) {
+__global__ void __launch_bounds__(32 * BRK_SCATTER_WARPS, 6) pp_brick_scatter_kernel(const PPArgs a) {
   using W = BrickWin;
   using SM = BrickScatterSmem<CP>;
   static_assert(MODE == K_PUSH || MODE == K_COUNT, "scatter modes");
