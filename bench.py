@@ -289,10 +289,10 @@ SCATTER_OPS = ("push_fwd", "pull_bwd", "pp_fwd", "pp_bwd")
 # channel-interleaved accumulator into the output (store_interleaved_vox).
 # A kernel not listed here reports traffic null.
 MEASURED_TRAFFIC = {
-    "pp_brick_gather_kernel mode=0 order=3 cb=3": 281_256_704,
-    "pp_brick_scatter_kernel mode=2 order=3 cb=3": 413_061_632 + 152_020_224,
-    "pp_kernel mode=4 order=3 cb=3": 486_608_384,
-    "pp_brick_pullbwd_kernel mode=5 order=3 cb=3": 584_656_640 + 149_855_488,
+    "pp_brick_gather_kernel mode=0 order=3 cb=3": 291_602_176,
+    "pp_brick_scatter_kernel mode=2 order=3 cb=3": 413_647_360 + 152_769_792,
+    "pp_kernel mode=4 order=3 cb=3": 492_331_520,
+    "pp_brick_pullbwd_kernel mode=5 order=3 cb=3": 583_946_240 + 151_942_400,
     # resize 1x3x256^3 -> 320^3, cubic, dct2
     "resize_sep_kernel tma mode=0 order=3 cb=1": 566_675_200,
 }
