@@ -78,3 +78,24 @@ def test_wide_offsets_vs_oracle(wide_buffer, order, bound):
     pushed = spatial.grid_push(T, G, list(src), b, o, 1)
     assert "order=-1" in _lib.last_kernel(), _lib.last_kernel()
     assert relerr(np64(pushed), O.grid_push(tgt, grid, src, [bound], [order], 1)) < 1e-5
+
+
+@pytest.mark.parametrize("bound", ["dct2", "dft", "zero"])
+def test_wide_regularisers_vs_oracle(wide_buffer, bound):
+    """The regularisers' 64-bit neighbour-offset instances: a field and a
+    displacement grid whose x axis has a stride of 2^30 elements (their ±2
+    steps along x do not fit 32 bits)."""
+    from nitorch_b200 import solve
+    code = {"dct2": 2, "dft": 5, "zero": 7}[bound]
+    vol = np.random.default_rng(5).standard_normal((1, C, 3, 7, 8))
+    V = _wide(wide_buffer, vol)
+    for (a, m, b) in (([0.1], [1.0], [0.0]), ([0.05], [0.3], [0.7])):
+        got = solve.c_regulariser(V, None, None, 3, a, m, b, 1.0, [1.2, 0.9, 1.1], bound)
+        ref = O.regulariser(vol, None, None, a, m, b, [1.2, 0.9, 1.1], [code])
+        assert relerr(got.double().cpu().numpy(), ref) < 1e-5, (a, m, b)
+    fld = np.random.default_rng(6).standard_normal((1, 3, 7, 8, 3))
+    G = wide_buffer.as_strided(fld.shape, (0, XS, 8 * 3, 3, 1))
+    G.copy_(torch.as_tensor(fld, dtype=torch.float32))
+    got = solve.c_regulariser_grid(G, None, None, 0.01, 0.2, 0.5, (0.7, 0.4), 1.0, [1.2, 0.9, 1.1], bound)
+    ref = O.regulariser_grid(np.moveaxis(fld, -1, 1), None, None, 0.01, 0.2, 0.5, 0.7, 0.4, [1.2, 0.9, 1.1], [code])
+    assert relerr(got.double().cpu().numpy(), np.moveaxis(ref, 1, -1)) < 1e-5
